@@ -1,0 +1,419 @@
+#!/usr/bin/env python
+"""Benchmark of the raster-stencil path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+
+Default workload (terrain16k): the full terrain set on a 16384 x 16384
+float32 DEM (1 GiB; seeded diamond-square fBm, H = 0.8, scaled to
+0-3000 m; 2% NoData as random 8x8 blocks in the validity mask; CellSize
+10): Gradient, Slope, Aspect, Hillshade (azimuth 315, altitude 45, z 1),
+profile / plan / mean Curvature, TRI / TPI / roughness, and the fused
+Slope -> Lookup (knots 0,5,10,20,30,40 deg) -> Reclass (5 classes) pass.
+One step runs every op of the set once over the DEM, with the DEM and the
+outputs resident in HBM. The inputs (1 GiB) are larger than L2, so no
+flush is needed between steps.
+
+Other workloads: slope2k (Slope on 2048 x 2048, CellSize 30), focal8k
+(focal ops on 8192 x 8192, r = 1..8).
+
+value: whole-job Mcells/s, output cells of every op per second (an op
+with two outputs counts its cells once). e2e: the same metric through the
+public API with host (page-locked) buffers, the host-to-device copy of
+the DEM and the device-to-host copy of each result inside the timed
+region. roofline: the op with the largest share of the step, its
+algorithmic bytes per launch over its average CUDA-event duration, against
+the measured HBM copy bandwidth. cpu_baseline: the parity oracle (a C
+restatement of the reference's scalar kernels) timed on the host cores on
+a row band of the same DEM.
+
+--impl reference times the reference's CPU implementation of the path:
+the reference (Go) cannot be built here, so it is the oracle port, on all
+host cores, each step a bounded row band of the workload.
+
+Multi-GPU (under torchrun): each rank runs the whole workload on its own
+GPU over its own DEM (independent rasters, no collective on the data
+path); value is the cells of all ranks over the max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+SLOPE_XS, SLOPE_YS = [0, 5, 10, 20, 30, 40], [1, 1.1, 1.3, 1.9, 3, 4.5]
+BREAKS, VALUES = [1.2, 1.6, 2.2, 3], [1, 2, 3, 4, 5]
+
+
+def hbm_peak():
+    try:
+        with open(PEAKS_PATH) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# Workloads: (name, stage-list factory, outputs) per op, and the input.
+
+def terrain_ops(cell_size):
+    from strata_b200 import terrain, transfer
+
+    o = dict(CellSize=cell_size)
+    return [
+        ("gradient", lambda: terrain.gradient_stage(terrain.GradientOptions(**o)), 2),
+        ("slope", lambda: terrain.slope_stage(terrain.SlopeOptions(**o)), 1),
+        ("aspect", lambda: terrain.aspect_stage(terrain.AspectOptions(**o)), 1),
+        ("hillshade", lambda: terrain.hillshade_stage(terrain.HillshadeOptions(Azimuth=315, Altitude=45,
+                                                                               ZFactor=1, **o)), 1),
+        ("curvature_profile", lambda: terrain.curvature_stage(terrain.CurvatureOptions(Type=0, **o)), 1),
+        ("curvature_plan", lambda: terrain.curvature_stage(terrain.CurvatureOptions(Type=1, **o)), 1),
+        ("curvature_mean", lambda: terrain.curvature_stage(terrain.CurvatureOptions(Type=2, **o)), 1),
+        ("tri", lambda: terrain.ruggedness_stage(terrain.RuggednessOptions(Type=0, Radius=1)), 1),
+        ("tpi", lambda: terrain.ruggedness_stage(terrain.RuggednessOptions(Type=2, Radius=1)), 1),
+        ("roughness", lambda: terrain.ruggedness_stage(terrain.RuggednessOptions(Type=3, Radius=1)), 1),
+        ("slope_lookup_reclass", lambda: terrain.slope_stage(terrain.SlopeOptions(**o))
+         .extend(transfer.lookup_stage(SLOPE_XS, SLOPE_YS)).extend(transfer.reclass_stage(BREAKS, VALUES)), 1),
+    ]
+
+
+def focal_ops():
+    from strata_b200 import engine, focal, synth
+
+    ops = []
+    for r in range(1, 9):
+        w = synth.uniform_weights((2 * r + 1) ** 2, 0x5EED0003 + r)
+        ops.append((f"correlate_r{r}", lambda w=w, r=r: focal.weights_stage(focal.WeightsOptions(r, w), False), 1))
+    g = focal.Gaussian(8, 2.5)
+    ops.append(("gaussian_r8", lambda: focal.separable_stage(focal.SeparableOptions(8, g, g)), 1))
+    for r in (3, 8):
+        for name, op in (("mean", engine._lib.OP_MEAN), ("min", engine._lib.OP_MIN), ("max", engine._lib.OP_MAX)):
+            ops.append((f"{name}_r{r}", lambda r=r, op=op: focal.box_stage(focal.BoxOptions(r), op), 1))
+    return ops
+
+
+def workload(name):
+    from strata_b200 import synth
+
+    if name == "terrain16k":
+        n, seed, cs = 16384, 0x5EED0002, 10
+        cells = synth.fbm_dem(n, n, seed)
+        valid = synth.block_mask(n, n, seed, 0.02)
+        return dict(name="terrain set on 16384x16384 f32 DEM", width=n, height=n, cells=cells, valid=valid,
+                    ops=terrain_ops(cs), cell_size=cs, mask="2% NoData in 8x8 blocks")
+    if name == "slope2k":
+        n, seed, cs = 2048, 0x5EED0001, 30
+        from strata_b200 import terrain
+
+        return dict(name="Slope on 2048x2048 f32 DEM", width=n, height=n, cells=synth.fbm_dem(n, n, seed),
+                    valid=synth.block_mask(n, n, seed, 0.02), cell_size=cs, mask="2% NoData in 8x8 blocks",
+                    ops=[("slope", lambda: terrain.slope_stage(terrain.SlopeOptions(CellSize=cs)), 1)])
+    if name == "focal8k":
+        n, seed = 8192, 0x5EED0003
+        return dict(name="focal ops on 8192x8192 f32 raster", width=n, height=n, cells=synth.normal_trend(n, n, seed),
+                    valid=synth.cell_mask(n, n, seed, 0.05), ops=focal_ops(), cell_size=None,
+                    mask="5% random NoData cells")
+    raise SystemExit(f"unknown workload {name}")
+
+
+def alg_bytes(cells, nout, masked):
+    """Algorithmic bytes of one op over `cells` cells: one input read and
+    nout outputs written, 4 B a cell, plus 1/8 B a cell per mask."""
+    b = cells * 4 * (1 + nout)
+    if masked:
+        b += cells * (1 + nout) / 8.0
+    return b
+
+
+# ---------------------------------------------------------------------------
+# Clock sampling during the timed region.
+
+class Clocks:
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self.stop = threading.Event()
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.samples.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+# ---------------------------------------------------------------------------
+# The CPU leg: the oracle on a row band.
+
+def cpu_run(wl, rows, nthreads, reps=1):
+    """Runs every op of the workload with the oracle over the first `rows`
+    rows of the input; returns (cells processed, seconds)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from helpers import host_raster, like, run_oracle
+
+    src = host_raster(np.ascontiguousarray(wl["cells"][:rows]), wl["valid"][:rows])
+    outs = [like(src), like(src)]
+    total, t0 = 0, time.perf_counter()
+    for _ in range(reps):
+        for _name, mk, nout in wl["ops"]:
+            run_oracle(mk(), src, outs[:nout], nthreads=nthreads)
+            total += src.width * src.height
+    return total, time.perf_counter() - t0
+
+
+def cpu_baseline(wl, target_s=10.0):
+    threads = os.cpu_count() or 1
+    rows = min(wl["height"], max(64, (1 << 22) // wl["width"]))
+    cells, secs = cpu_run(wl, rows, threads)
+    reps = max(1, int(target_s / max(secs, 1e-3)))
+    cells, secs = cpu_run(wl, rows, threads, reps)
+    return {"value": cells / secs / 1e6, "unit": "Mcells/s", "cores": threads, "kind": "port",
+            "sample": f"{rows} rows x {wl['width']} cells, every op of the set, {reps} pass(es), {secs:.1f} s"}
+
+
+# ---------------------------------------------------------------------------
+# Our arm.
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+
+    from strata_b200 import engine
+    from strata_b200.raster import Float32Raster, mask_from_bool
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    wl = workload(args.workload)
+    W, H = wl["width"], wl["height"]
+    n = W * H
+    masked = wl["valid"] is not None
+    host_cells = torch.from_numpy(wl["cells"].reshape(-1)).pin_memory()
+    host_mask = torch.from_numpy(mask_from_bool(wl["valid"]).view(np.int64)).pin_memory()
+    src = Float32Raster(host_cells.to(dev), W, H, W, host_mask.to(dev), 0)
+    words = (n + 63) // 64
+    outs = [Float32Raster(torch.empty(n, dtype=torch.float32, device=dev), W, H, W,
+                          torch.empty(words, dtype=torch.int64, device=dev), 0) for _ in range(2)]
+    stream = torch.cuda.Stream(dev)
+    opts = engine.Options(Stream=stream, Async=True, Device=local_rank)
+    ops = [(name, mk(), nout) for name, mk, nout in wl["ops"]]
+
+    def step(events=None):
+        for i, (name, stages, nout) in enumerate(ops):
+            if events is not None:
+                events[i][0].record(stream)
+            err = engine.process(stages, outs[:nout], [src], opts)
+            assert err is None
+            if events is not None:
+                events[i][1].record(stream)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+    torch.cuda.synchronize()
+
+    import torch.distributed as dist
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    per_op = [[torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)] for _ in ops]
+    op_ms = [0.0] * len(ops)
+    # Per-op durations, from a separate pass of K steps with events between ops.
+    with torch.cuda.stream(stream):
+        for _ in range(args.steps):
+            step(per_op)
+            torch.cuda.synchronize()
+            for i in range(len(ops)):
+                op_ms[i] += per_op[i][0].elapsed_time(per_op[i][1]) / args.steps
+
+    barrier()
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local_rank) as clk:
+        with torch.cuda.stream(stream):
+            start.record(stream)
+            for _ in range(args.steps):
+                step()
+            end.record(stream)
+        torch.cuda.synchronize()
+    ms = start.elapsed_time(end) / args.steps
+    barrier()
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+
+    cells_per_step = n * len(ops)
+    value = world * cells_per_step / (ms / 1e3) / 1e6
+    peak, peak_kind = hbm_peak()
+    per = []
+    for i, (name, _st, nout) in enumerate(ops):
+        b = alg_bytes(n, nout, masked)
+        gbs = b / (op_ms[i] / 1e3) / 1e9
+        per.append({"op": name, "ms": round(op_ms[i], 4), "mcells_s": round(n / (op_ms[i] / 1e3) / 1e6, 1),
+                    "gbs": round(gbs, 1), "frac_hbm": round(gbs / peak, 4)})
+    top = max(range(len(ops)), key=lambda i: op_ms[i])
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get(args.workload, {}).get(ops[top][0])
+        except Exception:
+            traffic = None
+    top_bytes = alg_bytes(n, ops[top][2], masked)
+    achieved = top_bytes / (op_ms[top] / 1e3) / 1e9
+    roofline = {"bound": "hbm", "kernel": ops[top][0], "achieved": round(achieved, 1), "peak": peak,
+                "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
+                "alg_bytes_per_launch": int(top_bytes)}
+
+    # e2e: the public API with host buffers, copies inside the timed region.
+    host_src = Float32Raster(host_cells.numpy(), W, H, W, host_mask.numpy().view(np.uint64), 0)
+    host_outs = [Float32Raster(torch.empty(n, dtype=torch.float32).pin_memory().numpy(), W, H, W,
+                               np.zeros(words, np.uint64), 0) for _ in range(2)]
+    e2e_opts = engine.Options(Device=local_rank)
+
+    def e2e_step():
+        for name, stages, nout in ops:
+            assert engine.process(stages, host_outs[:nout], [host_src], e2e_opts) is None
+
+    e2e_step()
+    barrier()
+    t0 = time.perf_counter()
+    e2e_steps = max(1, min(args.steps, 3))
+    for _ in range(e2e_steps):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    barrier()
+    if world > 1:
+        t = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    h2d = sum(n * 4 + words * 8 for _ in ops)
+    d2h = sum(nout * (n * 4 + words * 8) for _n, _s, nout in ops)
+    e2e = {"value": round(world * cells_per_step / e2e_s / 1e6, 1), "unit": "Mcells/s",
+           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": round(e2e_s * 1e3, 2),
+           "api": "engine.process with host rasters (strata_process, on_device=0)"}
+
+    launches_per_step = sum(1 + (nout if masked else 0) for _n, _s, nout in ops)
+    line = {
+        "metric": "Mcells/s (output cells of every op in the set per second)", "value": round(value, 1),
+        "unit": "Mcells/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": wl["name"], "width": W, "height": H, "cell_size": wl["cell_size"],
+                   "ops": [o[0] for o in ops], "mask": wl["mask"], "l2": "inputs larger than L2 (no flush)",
+                   "parallelism": f"independent rasters x{world}"},
+        "roofline": roofline, "e2e": e2e, "gpu_launches": launches_per_step * args.steps,
+        "clocks": clk.summary(), "per_op": per,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(wl)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def run_reference(args):
+    wl = workload(args.workload)
+    threads = os.cpu_count() or 1
+    rows = min(wl["height"], max(64, (1 << 22) // wl["width"]))
+    for _ in range(args.warmup):
+        cpu_run(wl, rows, threads)
+    cells, secs = 0, 0.0
+    for _ in range(args.steps):
+        c, s = cpu_run(wl, rows, threads)
+        cells += c
+        secs += s
+    value = cells / secs / 1e6
+    line = {
+        "impl": "reference", "metric": "Mcells/s (output cells of every op in the set per second)",
+        "value": round(value, 1), "unit": "Mcells/s", "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(secs / args.steps * 1e3, 2), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": wl["name"], "width": wl["width"], "height": wl["height"],
+                   "ops": [o[0] for o in wl["ops"]], "mask": wl["mask"]},
+        "cpu_baseline": {"value": round(value, 1), "unit": "Mcells/s", "cores": threads, "kind": "port",
+                         "sample": f"{rows} rows x {wl['width']} cells of the workload, every op, per step"},
+        "e2e": {"value": round(value, 1), "unit": "Mcells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="terrain16k", choices=["terrain16k", "slope2k", "focal8k"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference(args)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,275 @@
+/*
+ * strata_cuda.h - C ABI of libstrata_cuda, the B200 (sm_100a) backend for
+ * strata's raster-stencil path.
+ *
+ * Every entry point is plain C: pointers, sizes and status codes, no C++
+ * types and no exceptions across the boundary. A Go cgo shim, a ctypes
+ * binding or a C program binds it the same way.
+ *
+ * The path it replaces, in the strata sources:
+ *   - internal/exec/process.go:28-35   exec.ProcessN        -> strata_process
+ *   - internal/exec/chunked.go:33-40   exec.ProcessChunked  -> strata_process_chunked
+ *   - internal/exec/pipeline.go:187    exec.NewPipeline (a stencil stage
+ *                                      followed by pointwise stages)
+ *                                      -> strata_process with nstages > 1
+ *   - the kernels the terrain, focal and transfer packages build
+ *     (terrain/slope.go:76-82, aspect.go, hillshade.go, gradient.go,
+ *     curvature.go, ruggedness.go; focal/correlate.go:72-88,
+ *     separable.go:78-89, box.go:77-80; transfer/transfer.go:184-223)
+ *                                      -> the strata_stage_* builders
+ *
+ * Status codes: STRATA_OK (0) or a negative STRATA_E* value. The message
+ * of the last failure on the calling thread is strata_last_error().
+ * Argument errors that the reference reports with a panic return
+ * STRATA_EINVAL with the reference's message text and prefix ("terrain:",
+ * "focal:", "transfer.Lookup:", "engine:").
+ */
+#ifndef STRATA_CUDA_H
+#define STRATA_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define STRATA_ABI_VERSION 1
+
+/* Status codes. */
+#define STRATA_OK 0
+#define STRATA_EINVAL (-1)    /* an argument the reference panics on */
+#define STRATA_ECUDA (-2)     /* a CUDA runtime or launch error */
+#define STRATA_ENOMEM (-3)    /* device or pinned host memory exhausted */
+#define STRATA_ECANCELED (-4) /* the cancel flag was set; see strata_exec_opts */
+#define STRATA_ETIMEDOUT (-5) /* a bounded device-side wait ran out */
+#define STRATA_EIO (-6)       /* a source or sink callback failed */
+#define STRATA_ENOTSUP (-8)   /* valid for the reference, not on this backend (the caller falls back to the CPU) */
+
+/* Ops: the kernels of the terrain, focal and transfer packages. */
+enum {
+    STRATA_OP_GRADIENT = 1,   /* terrain.Gradient: 2 outputs (dx, dy), radius 1 */
+    STRATA_OP_SLOPE = 2,      /* terrain.Slope, radius 1 */
+    STRATA_OP_ASPECT = 3,     /* terrain.Aspect, radius 1 */
+    STRATA_OP_HILLSHADE = 4,  /* terrain.Hillshade, radius 1 */
+    STRATA_OP_CURVATURE = 5,  /* terrain.Curvature (Zevenbergen-Thorne), radius 1 */
+    STRATA_OP_RUGGEDNESS = 6, /* terrain.Ruggedness, radius 1..8 */
+    STRATA_OP_CORRELATE = 7,  /* focal.Correlate / Convolve, radius 1..8 */
+    STRATA_OP_SEPARABLE = 8,  /* focal.CorrelateSeparable, radius 1..8 */
+    STRATA_OP_MEAN = 9,       /* focal.Mean, radius 1..8 */
+    STRATA_OP_MIN = 10,       /* focal.Min, radius 1..8 */
+    STRATA_OP_MAX = 11,       /* focal.Max, radius 1..8 */
+    STRATA_OP_LOOKUP = 12,    /* transfer.Lookup, pointwise */
+    STRATA_OP_RECLASS = 13    /* transfer.Reclass, pointwise */
+};
+
+/* strata_stage.kind for STRATA_OP_CURVATURE (stencil.CurvatureKind). */
+enum { STRATA_CURV_PROFILE = 0, STRATA_CURV_PLAN = 1, STRATA_CURV_MEAN = 2 };
+/* strata_stage.kind for STRATA_OP_RUGGEDNESS (stencil.RuggednessKind). */
+enum { STRATA_RUG_TRI_RILEY = 0, STRATA_RUG_TRI_WILSON = 1, STRATA_RUG_TPI = 2, STRATA_RUG_ROUGHNESS = 3 };
+
+/* strata_stage.flags. */
+#define STRATA_STAGE_ROTATE180 1 /* correlate with the weights rotated by 180 degrees (Convolve) */
+
+/* Largest tables a stage may carry. */
+#define STRATA_MAX_RADIUS 8
+#define STRATA_MAX_KNOTS 64
+
+/*
+ * A raster view: strata's raster.Float32Raster (raster/raster.go:41-54).
+ * Cell (x, y) is data[y * stride + x]; its validity is bit
+ * valid_offset + y * stride + x of valid (LSB first in each 64-bit word),
+ * set = valid. valid == NULL means every cell is valid. on_device != 0
+ * says data and valid are device pointers on the context's device;
+ * otherwise they are host pointers and the call copies through device
+ * memory (page-locked host memory copies fastest).
+ */
+typedef struct {
+    float *data;
+    int64_t width, height, stride;
+    uint64_t *valid;
+    int64_t valid_offset;
+    int32_t on_device;
+    int32_t reserved;
+} strata_raster;
+
+/*
+ * One stage: an op and its resolved constants, as the reference's kernel
+ * value holds them after its option checks.
+ *   GRADIENT   k[0]=kx k[1]=ky
+ *   SLOPE      k[0]=kx k[1]=ky k[2]=scale, kind=1 takes Atan32 first
+ *   ASPECT     k[0]=kx k[1]=ky k[2]=flat, kind=1 trigonometric
+ *   HILLSHADE  k[0]=kx k[1]=ky k[2]=c k[3]=bx k[4]=by
+ *   CURVATURE  k[0..4]=kp kq kr kt ks, kind=STRATA_CURV_*
+ *   RUGGEDNESS radius, kind=STRATA_RUG_*
+ *   CORRELATE  radius, table[0]=(2r+1)^2 weights row-major, flags
+ *   SEPARABLE  radius, table[0]=row taps, table[1]=column taps (2r+1 each)
+ *   MEAN/MIN/MAX radius
+ *   LOOKUP     table[0]=xs table[1]=ys (table_len[0] knots)
+ *   RECLASS    table[0]=breaks (table_len[0]) table[1]=values (table_len[0]+1)
+ * Tables are host memory, read during the call only.
+ */
+typedef struct {
+    uint32_t op;
+    int32_t radius;
+    int32_t kind;
+    int32_t flags;
+    float k[16];
+    const float *table[4];
+    int32_t table_len[4];
+} strata_stage;
+
+/*
+ * Execution options: engine.Options (engine/engine.go:7-28) plus what a
+ * device call needs. tile_width / tile_height choose the chunked tiles
+ * (0 = whole raster, as the reference) and must not be negative; workers
+ * is accepted for parity and must not be negative. stream is a
+ * cudaStream_t (NULL = the context's stream). cancel, when not NULL, is
+ * polled between row strips (plain) or tiles (chunked): a non-zero value
+ * stops the call with STRATA_ECANCELED after a plan-order prefix.
+ * flags: STRATA_EXEC_ASYNC returns without synchronising when every
+ * operand is on the device.
+ */
+typedef struct {
+    int64_t tile_width, tile_height;
+    int32_t workers;
+    int32_t flags;
+    void *stream;
+    const volatile int32_t *cancel;
+} strata_exec_opts;
+
+#define STRATA_EXEC_ASYNC 1
+
+/*
+ * engine.Stats (engine/stats.go:77-168), counted for the device's own
+ * tiling: bands are thread-block tiles, kernel_read counts each tile's
+ * window including its halo, kernel_written each output cell once.
+ * A call adds to the struct it is given.
+ */
+typedef struct {
+    int64_t cells, ideal, tiles, bands;
+    int64_t source_read, sink_written, kernel_read, kernel_written;
+} strata_stats;
+
+typedef struct strata_ctx strata_ctx;
+
+/* Library and context. */
+int strata_abi_version(void);
+const char *strata_last_error(void);
+int strata_ctx_create(int device, strata_ctx **out);
+void strata_ctx_destroy(strata_ctx *ctx);
+int strata_ctx_device(const strata_ctx *ctx);
+int strata_ctx_synchronize(strata_ctx *ctx);
+
+/* Device memory owned by the context's device (for resident rasters). */
+int strata_alloc(strata_ctx *ctx, size_t bytes, void **dev);
+int strata_free(strata_ctx *ctx, void *dev);
+int strata_upload(strata_ctx *ctx, void *dev, const void *host, size_t bytes);
+int strata_download(strata_ctx *ctx, void *host, const void *dev, size_t bytes);
+
+/*
+ * exec.ProcessN (internal/exec/process.go:28) for one kernel or a
+ * pipeline: stages[0] is any op, stages[1..nstages-1] pointwise ops
+ * (LOOKUP / RECLASS) applied to its result in order, as exec.Pipeline
+ * runs Slope -> Lookup -> Reclass (graph/run.go:390-486). src holds nsrc
+ * = 1 raster; dst holds 2 rasters for GRADIENT, else 1. Edge cells (within
+ * the radius of the raster's border) get NaN and invalid; interior
+ * validity is the AND of the input's validity over the window
+ * (internal/exec/halo.go:21-229). stats may be NULL.
+ */
+int strata_process(strata_ctx *ctx, const strata_stage *stages, int nstages,
+                   const strata_raster *src, int nsrc, const strata_raster *dst, int ndst,
+                   const strata_exec_opts *opts, strata_stats *stats);
+
+/*
+ * engine.RasterSource / RasterSink (engine/source.go:19-70) as callbacks.
+ * read fills buf (a host raster of buf->width x buf->height cells, with a
+ * validity mask iff masked) from the window at (x, y); write takes buf
+ * for the window at (x, y). Each returns 0, or non-zero to fail the call
+ * with STRATA_EIO.
+ */
+typedef struct {
+    int64_t width, height;
+    int32_t masked;
+    int32_t reserved;
+    void *user;
+    int (*read)(void *user, const strata_raster *buf, int64_t x, int64_t y);
+} strata_source;
+
+typedef struct {
+    int64_t width, height;
+    int32_t masked;
+    int32_t reserved;
+    void *user;
+    int (*write)(void *user, const strata_raster *buf, int64_t x, int64_t y);
+} strata_sink;
+
+/*
+ * exec.ProcessChunked (internal/exec/chunked.go:33): reads tiles of the
+ * source with their halo, computes them on the device and hands each
+ * tile to the sinks, in plan order, with bounded memory (two pinned
+ * buffer sets). The sinks receive the bits strata_process would write.
+ */
+int strata_process_chunked(strata_ctx *ctx, const strata_stage *stages, int nstages,
+                           const strata_source *src, int nsrc, const strata_sink *dst, int ndst,
+                           const strata_exec_opts *opts, strata_stats *stats);
+
+/* ---------------------------------------------------------------------- */
+/* Stage builders: option resolution and checks of the typed entry points. */
+
+typedef struct { double cell_size, cell_size_y, z_factor; int32_t fit_radius; int32_t reserved; } strata_gradient_options;
+/* units: 0 degrees, 1 percent, 2 radians (terrain.SlopeUnits) */
+typedef struct { double cell_size, cell_size_y, z_factor; int32_t fit_radius; int32_t units; } strata_slope_options;
+typedef struct {
+    double cell_size, cell_size_y, z_factor;
+    int32_t fit_radius;
+    int32_t zero_for_flat;
+    int32_t trigonometric;
+    int32_t reserved;
+} strata_aspect_options;
+typedef struct {
+    double cell_size, cell_size_y, z_factor;
+    int32_t fit_radius;
+    int32_t reserved;
+    double azimuth, altitude;
+} strata_hillshade_options;
+/* type: 0 profile, 1 plan, 2 mean (terrain.CurvatureType) */
+typedef struct { double cell_size, cell_size_y, z_factor; int32_t fit_radius; int32_t type; } strata_curvature_options;
+/* type: 0 TRI (Riley), 1 TRIWilson, 2 TPI, 3 Roughness; radius 0 means 1 */
+typedef struct { int32_t type; int32_t radius; } strata_ruggedness_options;
+typedef struct { int32_t radius; int32_t nweights; const float *weights; } strata_weights_options;
+typedef struct { int32_t radius; int32_t nrow; const float *row; int32_t ncol; int32_t reserved; const float *col; } strata_separable_options;
+typedef struct { int32_t radius; } strata_box_options;
+
+/* terrain.newGradientKernel (terrain/gradient.go:70-73). */
+int strata_stage_gradient(const strata_gradient_options *o, strata_stage *out);
+/* terrain.newSlopeKernel / slopeScale (terrain/slope.go:76-95). */
+int strata_stage_slope(const strata_slope_options *o, strata_stage *out);
+/* terrain.newAspectKernel (terrain/aspect.go:90-102). */
+int strata_stage_aspect(const strata_aspect_options *o, strata_stage *out);
+/* terrain.newHillshadeKernel / hillshadeLight (terrain/hillshade.go:84-117). */
+int strata_stage_hillshade(const strata_hillshade_options *o, strata_stage *out);
+/* terrain.newCurvatureKernel (terrain/curvature.go:113-140). */
+int strata_stage_curvature(const strata_curvature_options *o, strata_stage *out);
+/* terrain.newRuggednessKernel (terrain/ruggedness.go:119-141). */
+int strata_stage_ruggedness(const strata_ruggedness_options *o, strata_stage *out);
+/* focal.newWeightsKernel (focal/correlate.go:72-88); convolve != 0 for Convolve.
+ * The stage keeps the caller's weights pointer. */
+int strata_stage_correlate(const strata_weights_options *o, int convolve, strata_stage *out);
+/* focal.newSeparableKernel (focal/separable.go:78-89). */
+int strata_stage_separable(const strata_separable_options *o, strata_stage *out);
+/* focal.newBox (focal/box.go:77-80); op is STRATA_OP_MEAN, _MIN or _MAX. */
+int strata_stage_box(const strata_box_options *o, uint32_t op, strata_stage *out);
+/* transfer.newLookupKernel (transfer/transfer.go:197-212). */
+int strata_stage_lookup(const float *xs, const float *ys, int32_t n, strata_stage *out);
+/* transfer.newReclassKernel (transfer/transfer.go:187-195). */
+int strata_stage_reclass(const float *breaks, int32_t nbreaks, const float *values, int32_t nvalues,
+                         strata_stage *out);
+/* focal.Gaussian (focal/separable.go:59-76): 2*radius+1 taps into taps. */
+int strata_focal_gaussian(int32_t radius, double sigma, float *taps);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,186 @@
+"""Python binding of the parity oracle - TEST INFRASTRUCTURE ONLY.
+
+Loads oracle/liboracle.so (the C restatement of strata's scalar kernels in
+strata_oracle.c) through ctypes. Only tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline legs import this module; the product never does.
+
+Rasters are described by plain numpy arrays: ``data`` is a 1-D float32
+array holding (height-1)*stride + width cells, ``valid`` an optional 1-D
+uint64 array of LSB-first validity bits starting at bit ``valid_offset``
+(strata's raster.Float32Raster layout, raster/raster.go:41-54).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+
+GRADIENT, SLOPE, ASPECT, HILLSHADE, CURVATURE, RUGGEDNESS = 1, 2, 3, 4, 5, 6
+CORRELATE, SEPARABLE, MEAN, MIN, MAX, LOOKUP, RECLASS = 7, 8, 9, 10, 11, 12, 13
+
+
+class Stage(ctypes.Structure):
+    _fields_ = [
+        ("op", ctypes.c_uint32),
+        ("radius", ctypes.c_int32),
+        ("kind", ctypes.c_int32),
+        ("flags", ctypes.c_int32),
+        ("k", ctypes.c_float * 16),
+        ("table", ctypes.c_void_p * 4),
+        ("table_len", ctypes.c_int32 * 4),
+    ]
+
+
+class Raster(ctypes.Structure):
+    _fields_ = [
+        ("data", ctypes.c_void_p),
+        ("width", ctypes.c_int64),
+        ("height", ctypes.c_int64),
+        ("stride", ctypes.c_int64),
+        ("valid", ctypes.c_void_p),
+        ("valid_offset", ctypes.c_int64),
+    ]
+
+
+def build() -> str:
+    """Compiles liboracle.so from strata_oracle.c (make, in this folder)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        src = os.path.join(HERE, "strata_oracle.c")
+        if not os.path.exists(LIB_PATH) or (
+            os.path.exists(src) and os.path.getmtime(src) > os.path.getmtime(LIB_PATH)
+        ):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        f, d, i64, p = ctypes.c_float, ctypes.c_double, ctypes.c_int64, ctypes.c_void_p
+        L.orc_atan32.restype = f
+        L.orc_atan32.argtypes = [f]
+        L.orc_atan2f32.restype = f
+        L.orc_atan2f32.argtypes = [f, f]
+        L.orc_go_min.restype = f
+        L.orc_go_min.argtypes = [f, f]
+        L.orc_go_max.restype = f
+        L.orc_go_max.argtypes = [f, f]
+        L.orc_atan32_array.argtypes = [p, p, i64]
+        L.orc_atan2f32_array.argtypes = [p, p, p, i64]
+        L.orc_horn_scales.argtypes = [d, d, d, ctypes.POINTER(f), ctypes.POINTER(f)]
+        L.orc_zt_scales.argtypes = [d, d, d, ctypes.POINTER(f)]
+        L.orc_hillshade_light.argtypes = [d, d, ctypes.POINTER(f)]
+        L.orc_gaussian.argtypes = [ctypes.c_int, d, ctypes.POINTER(f)]
+        L.orc_process.restype = ctypes.c_int
+        L.orc_process.argtypes = [ctypes.POINTER(Stage), ctypes.c_int, ctypes.POINTER(Raster),
+                                  ctypes.POINTER(Raster), ctypes.c_int, ctypes.c_int]
+        _lib = L
+    return _lib
+
+
+# ---------------------------------------------------------------------------
+# Scalar helpers.
+
+def atan32(x: float) -> np.float32:
+    return np.float32(lib().orc_atan32(np.float32(x)))
+
+
+def atan2f32(y: float, x: float) -> np.float32:
+    return np.float32(lib().orc_atan2f32(np.float32(y), np.float32(x)))
+
+
+def atan32_array(x: np.ndarray) -> np.ndarray:
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    out = np.empty_like(x)
+    lib().orc_atan32_array(x.ctypes.data, out.ctypes.data, x.size)
+    return out
+
+
+def atan2f32_array(y: np.ndarray, x: np.ndarray) -> np.ndarray:
+    y = np.ascontiguousarray(y, dtype=np.float32)
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    out = np.empty_like(y)
+    lib().orc_atan2f32_array(y.ctypes.data, x.ctypes.data, out.ctypes.data, y.size)
+    return out
+
+
+def go_min(a, b):
+    return np.float32(lib().orc_go_min(np.float32(a), np.float32(b)))
+
+
+def go_max(a, b):
+    return np.float32(lib().orc_go_max(np.float32(a), np.float32(b)))
+
+
+def horn_scales(cx, cy, z):
+    kx, ky = ctypes.c_float(), ctypes.c_float()
+    lib().orc_horn_scales(cx, cy, z, ctypes.byref(kx), ctypes.byref(ky))
+    return np.float32(kx.value), np.float32(ky.value)
+
+
+def zt_scales(cx, cy, z):
+    out = (ctypes.c_float * 5)()
+    lib().orc_zt_scales(cx, cy, z, out)
+    return [np.float32(v) for v in out]
+
+
+def hillshade_light(azimuth, altitude):
+    out = (ctypes.c_float * 3)()
+    lib().orc_hillshade_light(azimuth, altitude, out)
+    return [np.float32(v) for v in out]
+
+
+def gaussian(radius, sigma):
+    out = (ctypes.c_float * (2 * radius + 1))()
+    lib().orc_gaussian(radius, sigma, out)
+    return np.array(list(out), dtype=np.float32)
+
+
+# ---------------------------------------------------------------------------
+# Whole-raster calls.
+
+def stage(op, radius=0, kind=0, k=(), tables=()):
+    """Builds a Stage; returns (stage, keepalive) so table arrays outlive it."""
+    st = Stage()
+    st.op, st.radius, st.kind = op, radius, kind
+    for i, v in enumerate(k):
+        st.k[i] = float(v)
+    keep = []
+    for i, t in enumerate(tables):
+        a = np.ascontiguousarray(t, dtype=np.float32)
+        keep.append(a)
+        st.table[i] = a.ctypes.data
+        st.table_len[i] = a.size
+    return st, keep
+
+
+def _raster(data, width, height, stride, valid=None, valid_offset=0):
+    r = Raster()
+    r.data = data.ctypes.data
+    r.width, r.height, r.stride = width, height, stride
+    r.valid = valid.ctypes.data if valid is not None else None
+    r.valid_offset = valid_offset
+    return r
+
+
+def process(stages, src, dsts, nthreads=1):
+    """Runs stages over src into dsts.
+
+    stages: list of (Stage, keepalive) from stage().
+    src, dsts[i]: dicts with keys data, width, height, stride, valid, valid_offset.
+    """
+    st_arr = (Stage * len(stages))(*[s for s, _ in stages])
+    s = _raster(**src)
+    d_arr = (Raster * len(dsts))(*[_raster(**d) for d in dsts])
+    rc = lib().orc_process(st_arr, len(stages), ctypes.byref(s), d_arr, len(dsts), nthreads)
+    if rc != 0:
+        raise ValueError(f"oracle: invalid call (rc={rc})")

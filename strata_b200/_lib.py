@@ -1,0 +1,176 @@
+"""ctypes binding of libstrata_cuda (include/strata_cuda.h).
+
+The library is built in-tree (strata_b200/libstrata_cuda.so) by
+strata_b200/build.py. Loading fails loudly when it is missing: the device
+backend has no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libstrata_cuda.so")
+
+OK, EINVAL, ECUDA, ENOMEM, ECANCELED, ETIMEDOUT, EIO, ENOTSUP = 0, -1, -2, -3, -4, -5, -6, -8
+
+OP_GRADIENT, OP_SLOPE, OP_ASPECT, OP_HILLSHADE, OP_CURVATURE, OP_RUGGEDNESS = 1, 2, 3, 4, 5, 6
+OP_CORRELATE, OP_SEPARABLE, OP_MEAN, OP_MIN, OP_MAX, OP_LOOKUP, OP_RECLASS = 7, 8, 9, 10, 11, 12, 13
+STAGE_ROTATE180 = 1
+EXEC_ASYNC = 1
+MAX_RADIUS = 8
+MAX_KNOTS = 64
+
+c_i32, c_i64, c_f32, c_f64, c_p = ctypes.c_int32, ctypes.c_int64, ctypes.c_float, ctypes.c_double, ctypes.c_void_p
+
+
+class Raster(ctypes.Structure):
+    _fields_ = [("data", c_p), ("width", c_i64), ("height", c_i64), ("stride", c_i64),
+                ("valid", c_p), ("valid_offset", c_i64), ("on_device", c_i32), ("reserved", c_i32)]
+
+
+class Stage(ctypes.Structure):
+    _fields_ = [("op", ctypes.c_uint32), ("radius", c_i32), ("kind", c_i32), ("flags", c_i32),
+                ("k", c_f32 * 16), ("table", c_p * 4), ("table_len", c_i32 * 4)]
+
+
+class ExecOpts(ctypes.Structure):
+    _fields_ = [("tile_width", c_i64), ("tile_height", c_i64), ("workers", c_i32), ("flags", c_i32),
+                ("stream", c_p), ("cancel", ctypes.POINTER(c_i32))]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("cells", c_i64), ("ideal", c_i64), ("tiles", c_i64), ("bands", c_i64),
+                ("source_read", c_i64), ("sink_written", c_i64), ("kernel_read", c_i64),
+                ("kernel_written", c_i64)]
+
+
+READ_FN = ctypes.CFUNCTYPE(ctypes.c_int, c_p, ctypes.POINTER(Raster), c_i64, c_i64)
+WRITE_FN = ctypes.CFUNCTYPE(ctypes.c_int, c_p, ctypes.POINTER(Raster), c_i64, c_i64)
+
+
+class Source(ctypes.Structure):
+    _fields_ = [("width", c_i64), ("height", c_i64), ("masked", c_i32), ("reserved", c_i32),
+                ("user", c_p), ("read", READ_FN)]
+
+
+class Sink(ctypes.Structure):
+    _fields_ = [("width", c_i64), ("height", c_i64), ("masked", c_i32), ("reserved", c_i32),
+                ("user", c_p), ("write", WRITE_FN)]
+
+
+class GradientOptions(ctypes.Structure):
+    _fields_ = [("cell_size", c_f64), ("cell_size_y", c_f64), ("z_factor", c_f64),
+                ("fit_radius", c_i32), ("reserved", c_i32)]
+
+
+class SlopeOptions(ctypes.Structure):
+    _fields_ = [("cell_size", c_f64), ("cell_size_y", c_f64), ("z_factor", c_f64),
+                ("fit_radius", c_i32), ("units", c_i32)]
+
+
+class AspectOptions(ctypes.Structure):
+    _fields_ = [("cell_size", c_f64), ("cell_size_y", c_f64), ("z_factor", c_f64),
+                ("fit_radius", c_i32), ("zero_for_flat", c_i32), ("trigonometric", c_i32), ("reserved", c_i32)]
+
+
+class HillshadeOptions(ctypes.Structure):
+    _fields_ = [("cell_size", c_f64), ("cell_size_y", c_f64), ("z_factor", c_f64),
+                ("fit_radius", c_i32), ("reserved", c_i32), ("azimuth", c_f64), ("altitude", c_f64)]
+
+
+class CurvatureOptions(ctypes.Structure):
+    _fields_ = [("cell_size", c_f64), ("cell_size_y", c_f64), ("z_factor", c_f64),
+                ("fit_radius", c_i32), ("type", c_i32)]
+
+
+class RuggednessOptions(ctypes.Structure):
+    _fields_ = [("type", c_i32), ("radius", c_i32)]
+
+
+class WeightsOptions(ctypes.Structure):
+    _fields_ = [("radius", c_i32), ("nweights", c_i32), ("weights", c_p)]
+
+
+class SeparableOptions(ctypes.Structure):
+    _fields_ = [("radius", c_i32), ("nrow", c_i32), ("row", c_p), ("ncol", c_i32), ("reserved", c_i32),
+                ("col", c_p)]
+
+
+class BoxOptions(ctypes.Structure):
+    _fields_ = [("radius", c_i32)]
+
+
+# (name, restype, argtypes) of every entry point include/strata_cuda.h declares.
+SIGNATURES = [
+    ("strata_abi_version", ctypes.c_int, []),
+    ("strata_last_error", ctypes.c_char_p, []),
+    ("strata_ctx_create", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(c_p)]),
+    ("strata_ctx_destroy", None, [c_p]),
+    ("strata_ctx_device", ctypes.c_int, [c_p]),
+    ("strata_ctx_synchronize", ctypes.c_int, [c_p]),
+    ("strata_alloc", ctypes.c_int, [c_p, ctypes.c_size_t, ctypes.POINTER(c_p)]),
+    ("strata_free", ctypes.c_int, [c_p, c_p]),
+    ("strata_upload", ctypes.c_int, [c_p, c_p, c_p, ctypes.c_size_t]),
+    ("strata_download", ctypes.c_int, [c_p, c_p, c_p, ctypes.c_size_t]),
+    ("strata_process", ctypes.c_int, [c_p, ctypes.POINTER(Stage), ctypes.c_int, ctypes.POINTER(Raster),
+                                      ctypes.c_int, ctypes.POINTER(Raster), ctypes.c_int,
+                                      ctypes.POINTER(ExecOpts), ctypes.POINTER(Stats)]),
+    ("strata_process_chunked", ctypes.c_int, [c_p, ctypes.POINTER(Stage), ctypes.c_int, ctypes.POINTER(Source),
+                                              ctypes.c_int, ctypes.POINTER(Sink), ctypes.c_int,
+                                              ctypes.POINTER(ExecOpts), ctypes.POINTER(Stats)]),
+    ("strata_stage_gradient", ctypes.c_int, [ctypes.POINTER(GradientOptions), ctypes.POINTER(Stage)]),
+    ("strata_stage_slope", ctypes.c_int, [ctypes.POINTER(SlopeOptions), ctypes.POINTER(Stage)]),
+    ("strata_stage_aspect", ctypes.c_int, [ctypes.POINTER(AspectOptions), ctypes.POINTER(Stage)]),
+    ("strata_stage_hillshade", ctypes.c_int, [ctypes.POINTER(HillshadeOptions), ctypes.POINTER(Stage)]),
+    ("strata_stage_curvature", ctypes.c_int, [ctypes.POINTER(CurvatureOptions), ctypes.POINTER(Stage)]),
+    ("strata_stage_ruggedness", ctypes.c_int, [ctypes.POINTER(RuggednessOptions), ctypes.POINTER(Stage)]),
+    ("strata_stage_correlate", ctypes.c_int, [ctypes.POINTER(WeightsOptions), ctypes.c_int, ctypes.POINTER(Stage)]),
+    ("strata_stage_separable", ctypes.c_int, [ctypes.POINTER(SeparableOptions), ctypes.POINTER(Stage)]),
+    ("strata_stage_box", ctypes.c_int, [ctypes.POINTER(BoxOptions), ctypes.c_uint32, ctypes.POINTER(Stage)]),
+    ("strata_stage_lookup", ctypes.c_int, [c_p, c_p, c_i32, ctypes.POINTER(Stage)]),
+    ("strata_stage_reclass", ctypes.c_int, [c_p, c_i32, c_p, c_i32, ctypes.POINTER(Stage)]),
+    ("strata_focal_gaussian", ctypes.c_int, [c_i32, c_f64, ctypes.POINTER(c_f32)]),
+]
+
+_lib = None
+_lock = threading.Lock()
+
+
+def lib():
+    """The loaded library; raises if libstrata_cuda.so has not been built."""
+    global _lib
+    if _lib is None:
+        with _lock:
+            if _lib is None:
+                if not os.path.exists(LIB_PATH):
+                    raise RuntimeError(
+                        f"libstrata_cuda.so is not built ({LIB_PATH}); run python -m strata_b200.build")
+                L = ctypes.CDLL(LIB_PATH)
+                for name, res, args in SIGNATURES:
+                    f = getattr(L, name)
+                    f.restype = res
+                    f.argtypes = args
+                _lib = L
+    return _lib
+
+
+def last_error() -> str:
+    return lib().strata_last_error().decode("utf-8", "replace")
+
+
+def check(rc: int) -> None:
+    """Raises the Python form of a status code: StrataPanic for EINVAL,
+    NotSupported for ENOTSUP, RuntimeError for device failures. ECANCELED
+    and EIO are returned as errors by the Tiled/Chunked functions instead."""
+    from .raster import NotSupported, StrataPanic
+
+    if rc == OK:
+        return
+    msg = last_error()
+    if rc == EINVAL:
+        raise StrataPanic(msg)
+    if rc == ENOTSUP:
+        raise NotSupported(msg)
+    raise RuntimeError(f"strata_cuda error {rc}: {msg}")

@@ -1,0 +1,1263 @@
+// api.cu - the C ABI of libstrata_cuda (include/strata_cuda.h).
+//
+// The host side of the device backend: the checks exec.ProcessN makes
+// before it runs (internal/exec/process.go:37-135), staging of host
+// rasters through device memory, the launches, Stats, and the stage
+// builders that resolve the typed options as the terrain, focal and
+// transfer packages do.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "launch.h"
+
+using strata::EpiStage;
+using strata::LaunchParams;
+using strata::ValidityParams;
+
+// ---------------------------------------------------------------------------
+// Errors.
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+    return fail(e == cudaErrorMemoryAllocation ? STRATA_ENOMEM : STRATA_ECUDA, "strata_cuda: %s: %s", what,
+                cudaGetErrorString(e));
+}
+
+// Go's %v for a float64 (fmt: the shortest representation that round
+// trips, %e form when the exponent is < -4 or >= 21), or for a float32
+// with f32 set. Used to reproduce the reference's panic messages.
+std::string fmt_v(double x, bool f32 = false) {
+    if (std::isnan(x)) return "NaN";
+    if (std::isinf(x)) return x > 0 ? "+Inf" : "-Inf";
+    if (x == 0) return std::signbit(x) ? "-0" : "0";
+    char buf[64];
+    int prec = 1;
+    for (; prec <= 17; prec++) {
+        snprintf(buf, sizeof buf, "%.*e", prec - 1, x);
+        double back = strtod(buf, nullptr);
+        if (f32 ? (float)back == (float)x : back == x) break;
+    }
+    snprintf(buf, sizeof buf, "%.*e", prec - 1, x);
+    // buf: d.ddde[+-]XX
+    std::string s(buf);
+    size_t e = s.find('e');
+    int exp = atoi(s.c_str() + e + 1);
+    std::string digits;
+    for (size_t i = 0; i < e; i++)
+        if (isdigit((unsigned char)s[i])) digits += s[i];
+    bool neg = x < 0;
+    std::string out = neg ? "-" : "";
+    if (exp < -4 || exp >= 21) {
+        out += digits.substr(0, 1);
+        if (digits.size() > 1) out += "." + digits.substr(1);
+        char eb[16];
+        snprintf(eb, sizeof eb, "e%c%02d", exp < 0 ? '-' : '+', exp < 0 ? -exp : exp);
+        out += eb;
+        return out;
+    }
+    if (exp < 0) {
+        out += "0." + std::string(-exp - 1, '0') + digits;
+    } else if ((int)digits.size() <= exp + 1) {
+        out += digits + std::string(exp + 1 - digits.size(), '0');
+    } else {
+        out += digits.substr(0, exp + 1) + "." + digits.substr(exp + 1);
+    }
+    return out;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Context.
+
+struct strata_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::mutex mu;
+    // Device buffers for host operands, grown on demand and reused.
+    struct Buf {
+        void* p = nullptr;
+        size_t n = 0;
+    };
+    Buf bufs[8];
+    // Page-locked staging for mask merges.
+    std::vector<uint64_t> host_words;
+};
+
+namespace {
+
+int ensure(strata_ctx* c, int slot, size_t bytes, void** out) {
+    auto& b = c->bufs[slot];
+    if (b.n < bytes) {
+        if (b.p) cudaFree(b.p);
+        b.p = nullptr;
+        b.n = 0;
+        size_t want = bytes + bytes / 8 + 256;
+        cudaError_t e = cudaMalloc(&b.p, want);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return cuda_fail(e, "device buffer");
+        }
+        b.n = want;
+    }
+    *out = b.p;
+    return STRATA_OK;
+}
+
+}  // namespace
+
+extern "C" int strata_abi_version(void) { return STRATA_ABI_VERSION; }
+
+extern "C" const char* strata_last_error(void) { return g_err.c_str(); }
+
+extern "C" int strata_ctx_create(int device, strata_ctx** out) {
+    if (!out) return fail(STRATA_EINVAL, "strata_cuda: nil output pointer");
+    *out = nullptr;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDeviceCount");
+    if (device < 0 || device >= n) return fail(STRATA_EINVAL, "strata_cuda: device %d out of range [0, %d)", device, n);
+    e = cudaSetDevice(device);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+    auto* c = new strata_ctx;
+    c->device = device;
+    e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete c;
+        return cuda_fail(e, "cudaStreamCreate");
+    }
+    *out = c;
+    return STRATA_OK;
+}
+
+extern "C" void strata_ctx_destroy(strata_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    for (auto& b : c->bufs)
+        if (b.p) cudaFree(b.p);
+    cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+extern "C" int strata_ctx_device(const strata_ctx* c) { return c ? c->device : -1; }
+
+extern "C" int strata_ctx_synchronize(strata_ctx* c) {
+    if (!c) return fail(STRATA_EINVAL, "strata_cuda: nil context");
+    cudaSetDevice(c->device);
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamSynchronize");
+    return STRATA_OK;
+}
+
+extern "C" int strata_alloc(strata_ctx* c, size_t bytes, void** dev) {
+    if (!c || !dev) return fail(STRATA_EINVAL, "strata_cuda: nil argument");
+    cudaSetDevice(c->device);
+    cudaError_t e = cudaMalloc(dev, bytes ? bytes : 1);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return cuda_fail(e, "cudaMalloc");
+    }
+    return STRATA_OK;
+}
+
+extern "C" int strata_free(strata_ctx* c, void* dev) {
+    if (!c) return fail(STRATA_EINVAL, "strata_cuda: nil context");
+    cudaSetDevice(c->device);
+    cudaError_t e = cudaFree(dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFree");
+    return STRATA_OK;
+}
+
+extern "C" int strata_upload(strata_ctx* c, void* dev, const void* host, size_t bytes) {
+    if (!c) return fail(STRATA_EINVAL, "strata_cuda: nil context");
+    cudaSetDevice(c->device);
+    cudaError_t e = cudaMemcpyAsync(dev, host, bytes, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "upload");
+    return STRATA_OK;
+}
+
+extern "C" int strata_download(strata_ctx* c, void* host, const void* dev, size_t bytes) {
+    if (!c) return fail(STRATA_EINVAL, "strata_cuda: nil context");
+    cudaSetDevice(c->device);
+    cudaError_t e = cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "download");
+    return STRATA_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Checks of ProcessN (internal/exec/process.go:37-135).
+
+namespace {
+
+int64_t span_cells(const strata_raster& r) { return (r.height - 1) * r.stride + r.width; }
+
+// raster.Float32Raster.Validate (raster/raster.go:174-203), for the
+// fields a C caller passes.
+int validate(const char* name, int i, const strata_raster& r) {
+    if (r.width <= 0 || r.height <= 0)
+        return fail(STRATA_EINVAL, "engine: %s[%d]: raster: dimensions must be positive, got %lld×%lld", name, i,
+                    (long long)r.width, (long long)r.height);
+    if (r.stride < r.width)
+        return fail(STRATA_EINVAL, "engine: %s[%d]: raster: stride %lld is less than width %lld", name, i,
+                    (long long)r.stride, (long long)r.width);
+    if (r.height - 1 > (INT64_MAX - r.width) / r.stride)
+        return fail(STRATA_EINVAL, "engine: %s[%d]: raster: %lld×%lld with stride %lld has more cells than an int holds",
+                    name, i, (long long)r.width, (long long)r.height, (long long)r.stride);
+    if (!r.data) return fail(STRATA_EINVAL, "engine: %s[%d]: raster: nil Data", name, i);
+    if (r.valid && r.valid_offset < 0)
+        return fail(STRATA_EINVAL, "engine: %s[%d]: raster: negative ValidOffset %lld", name, i,
+                    (long long)r.valid_offset);
+    return STRATA_OK;
+}
+
+enum Relation { kDisjoint, kSame, kPartial };
+
+bool spans_meet(int64_t a0, int64_t an, int64_t b0, int64_t bn) { return a0 < b0 + bn && b0 < a0 + an; }
+
+// overlap.relate (internal/overlap/overlap.go).
+Relation relate(int64_t a0, int64_t as, int64_t b0, int64_t bs, int64_t w, int64_t h) {
+    if (!spans_meet(a0, (h - 1) * as + w, b0, (h - 1) * bs + w)) return kDisjoint;
+    if (a0 == b0) return (as == bs || h == 1) ? kSame : kPartial;
+    if (as != bs) return kPartial;
+    int64_t diff = a0 - b0;
+    int64_t dy = diff / as, dx = diff % as;
+    if (dx < 0) {
+        dy -= 1;
+        dx += as;
+    }
+    auto rows_meet = [h](int64_t d) { return d > -h && d < h; };
+    if ((dx < w && rows_meet(dy)) || (dx > as - w && rows_meet(dy + 1))) return kPartial;
+    return kDisjoint;
+}
+
+// Two operands can only share memory when they are in the same address
+// space: both on the device or both on the host.
+bool same_space(const strata_raster& a, const strata_raster& b) { return (a.on_device != 0) == (b.on_device != 0); }
+
+Relation data_rel(const strata_raster& a, const strata_raster& b) {
+    if (!same_space(a, b)) return kDisjoint;
+    int64_t a0 = (int64_t)(uintptr_t)a.data, b0 = (int64_t)(uintptr_t)b.data;
+    if ((a0 - b0) % 4 != 0) return spans_meet(a0, span_cells(a) * 4, b0, span_cells(b) * 4) ? kPartial : kDisjoint;
+    return relate(a0 / 4, a.stride, b0 / 4, b.stride, a.width, a.height);
+}
+
+int64_t bit_addr(const strata_raster& r) { return (int64_t)(uintptr_t)r.valid * 8 + r.valid_offset; }
+
+Relation bits_rel(const strata_raster& a, const strata_raster& b) {
+    if (!a.valid || !b.valid || !same_space(a, b)) return kDisjoint;
+    return relate(bit_addr(a), a.stride, bit_addr(b), b.stride, a.width, a.height);
+}
+
+bool data_spans(const strata_raster& a, const strata_raster& b) {
+    if (!same_space(a, b)) return false;
+    return spans_meet((int64_t)(uintptr_t)a.data, span_cells(a) * 4, (int64_t)(uintptr_t)b.data, span_cells(b) * 4);
+}
+
+bool bit_spans(const strata_raster& a, const strata_raster& b) {
+    if (!a.valid || !b.valid || !same_space(a, b)) return false;
+    return spans_meet(bit_addr(a), span_cells(a), bit_addr(b), span_cells(b));
+}
+
+bool is_pointwise(uint32_t op) { return op == STRATA_OP_LOOKUP || op == STRATA_OP_RECLASS; }
+
+int op_radius(const strata_stage& s) {
+    switch (s.op) {
+    case STRATA_OP_GRADIENT:
+    case STRATA_OP_SLOPE:
+    case STRATA_OP_ASPECT:
+    case STRATA_OP_HILLSHADE:
+    case STRATA_OP_CURVATURE:
+        return 1;
+    case STRATA_OP_LOOKUP:
+    case STRATA_OP_RECLASS:
+        return 0;
+    default:
+        return s.radius;
+    }
+}
+
+bool finite32(float v) { return v - v == 0; }
+
+// A stage's tables into the launch parameters.
+int fill_stage(const strata_stage& s, LaunchParams& p, int epi_index) {
+    if (is_pointwise(s.op)) {
+        if (epi_index >= strata::kMaxEpilogue)
+            return fail(STRATA_ENOTSUP, "engine: a pipeline on the gpu backend takes at most %d pointwise stages",
+                        strata::kMaxEpilogue);
+        EpiStage& e = p.epi[epi_index];
+        e.op = (int)s.op;
+        int n = s.table_len[0];
+        if (n < (s.op == STRATA_OP_LOOKUP ? 1 : 0) || n > STRATA_MAX_KNOTS || !s.table[0] || !s.table[1])
+            return fail(STRATA_EINVAL, "engine: stage table of %d entries (1 to %d)", n, STRATA_MAX_KNOTS);
+        e.n = n;
+        memcpy(e.a, s.table[0], sizeof(float) * n);
+        memcpy(e.b, s.table[1], sizeof(float) * (s.op == STRATA_OP_LOOKUP ? n : n + 1));
+        return STRATA_OK;
+    }
+    p.op = (int)s.op;
+    p.radius = op_radius(s);
+    p.kind = s.kind;
+    memcpy(p.k, s.k, sizeof p.k);
+    int r = p.radius;
+    if (s.op >= STRATA_OP_RUGGEDNESS && s.op <= STRATA_OP_MAX && (r < 1 || r > STRATA_MAX_RADIUS))
+        return fail(STRATA_EINVAL, "engine: stage radius %d outside 1 to %d", r, STRATA_MAX_RADIUS);
+    int d = 2 * r + 1;
+    if (s.op == STRATA_OP_CORRELATE) {
+        if (s.table_len[0] != d * d || !s.table[0])
+            return fail(STRATA_EINVAL, "focal: Radius %d needs %d×%d = %d Weights, got %d", r, d, d, d * d,
+                        s.table_len[0]);
+        for (int i = 0; i < d * d; i++) {
+            int j = (s.flags & STRATA_STAGE_ROTATE180) ? d * d - 1 - i : i;
+            p.w[j] = s.table[0][i];
+        }
+    } else if (s.op == STRATA_OP_SEPARABLE) {
+        if (s.table_len[0] != d || s.table_len[1] != d || !s.table[0] || !s.table[1])
+            return fail(STRATA_EINVAL, "focal: Radius %d needs %d Row and %d Col taps, got %d and %d", r, d, d,
+                        s.table_len[0], s.table_len[1]);
+        for (int i = 0; i < d; i++) {
+            p.w[i] = s.table[0][i];
+            p.w[17 + i] = s.table[1][i];
+        }
+    }
+    if (s.op == STRATA_OP_CURVATURE && (s.kind < 0 || s.kind > 2))
+        return fail(STRATA_EINVAL, "stencil: unknown CurvatureKind %d", s.kind);
+    if (s.op == STRATA_OP_RUGGEDNESS && (s.kind < 0 || s.kind > 3))
+        return fail(STRATA_EINVAL, "stencil: unknown RuggednessKind %d", s.kind);
+    return STRATA_OK;
+}
+
+int check_opts(const strata_exec_opts* o) {
+    if (o && (o->tile_width < 0 || o->tile_height < 0 || o->workers < 0))
+        return fail(STRATA_EINVAL, "engine: negative Options {TileWidth:%lld TileHeight:%lld Workers:%d}",
+                    (long long)o->tile_width, (long long)o->tile_height, o->workers);
+    return STRATA_OK;
+}
+
+// Resolves stages into launch parameters (op, radius, epilogue).
+int plan_stages(const strata_stage* stages, int nstages, LaunchParams& p, int* nout) {
+    if (!stages || nstages < 1) return fail(STRATA_EINVAL, "engine: nil kernel");
+    memset(&p, 0, sizeof p);
+    const strata_stage& s0 = stages[0];
+    if (s0.op < STRATA_OP_GRADIENT || s0.op > STRATA_OP_RECLASS)
+        return fail(STRATA_EINVAL, "engine: unknown op %u", s0.op);
+    int epi = 0;
+    int rc;
+    if (is_pointwise(s0.op)) {
+        p.op = (int)s0.op;
+        p.radius = 0;
+        for (int i = 0; i < nstages; i++) {
+            if (!is_pointwise(stages[i].op))
+                return fail(STRATA_ENOTSUP,
+                            "engine: a pipeline on the gpu backend is one stencil stage followed by pointwise stages");
+            if ((rc = fill_stage(stages[i], p, epi++)) != STRATA_OK) return rc;
+        }
+    } else {
+        if ((rc = fill_stage(s0, p, 0)) != STRATA_OK) return rc;
+        for (int i = 1; i < nstages; i++) {
+            if (!is_pointwise(stages[i].op) || s0.op == STRATA_OP_GRADIENT)
+                return fail(STRATA_ENOTSUP,
+                            "engine: a pipeline on the gpu backend is one stencil stage followed by pointwise stages");
+            if ((rc = fill_stage(stages[i], p, epi++)) != STRATA_OK) return rc;
+        }
+    }
+    p.nepi = epi;
+    *nout = s0.op == STRATA_OP_GRADIENT ? 2 : 1;
+    return STRATA_OK;
+}
+
+int check_operands(const strata_raster* src, int nsrc, const strata_raster* dst, int ndst, int nout, int r) {
+    if (nsrc != 1 || ndst != nout || !src || !dst)
+        return fail(STRATA_EINVAL, "engine: kernel takes 1 inputs and %d outputs, got %d and %d", nout, nsrc, ndst);
+    int rc;
+    for (int i = 0; i < ndst; i++) {
+        if ((rc = validate("dst", i, dst[i])) != STRATA_OK) return rc;
+        if (dst[i].width != dst[0].width || dst[i].height != dst[0].height)
+            return fail(STRATA_EINVAL, "engine: dst[%d] is %lld×%lld, dst[0] is %lld×%lld", i, (long long)dst[i].width,
+                        (long long)dst[i].height, (long long)dst[0].width, (long long)dst[0].height);
+    }
+    if ((rc = validate("src", 0, src[0])) != STRATA_OK) return rc;
+    if (src[0].width != dst[0].width || src[0].height != dst[0].height)
+        return fail(STRATA_EINVAL, "engine: src[0] is %lld×%lld, dst[0] is %lld×%lld", (long long)src[0].width,
+                    (long long)src[0].height, (long long)dst[0].width, (long long)dst[0].height);
+    for (int i = 0; i < ndst; i++)
+        if (src[0].valid && !dst[i].valid)
+            return fail(STRATA_EINVAL,
+                        "engine: an input has a validity mask but dst[%d].Valid is nil; allocate it with "
+                        "raster.NewFloat32Like, or set Valid on its root raster before windowing",
+                        i);
+    for (int i = 0; i < ndst; i++) {
+        for (int j = i + 1; j < ndst; j++) {
+            bool dm = r == 0 ? data_rel(dst[i], dst[j]) != kDisjoint : data_spans(dst[i], dst[j]);
+            if (dm) return fail(STRATA_EINVAL, "engine: dst[%d] and dst[%d] share Data", i, j);
+            bool bm = r == 0 ? bits_rel(dst[i], dst[j]) != kDisjoint : bit_spans(dst[i], dst[j]);
+            if (bm) return fail(STRATA_EINVAL, "engine: dst[%d] and dst[%d] share validity bits", i, j);
+        }
+        const strata_raster& s = src[0];
+        if (r > 0) {
+            if (data_spans(dst[i], s))
+                return fail(STRATA_EINVAL,
+                            "engine: dst[%d] and src[0] share Data; a kernel with radius %d would read neighbours "
+                            "it has already overwritten",
+                            i, r);
+            if (bit_spans(dst[i], s)) return fail(STRATA_EINVAL, "engine: dst[%d] and src[0] share validity bits", i);
+            continue;
+        }
+        Relation d = data_rel(dst[i], s);
+        if (d == kPartial)
+            return fail(STRATA_EINVAL, "engine: dst[%d] overlaps src[0] at a different offset or stride", i);
+        if (d == kSame && nout > 1)
+            return fail(STRATA_EINVAL, "engine: dst[%d] is src[0]; only a kernel with one output runs in place", i);
+        if (bits_rel(dst[i], s) == kPartial)
+            return fail(STRATA_EINVAL,
+                        "engine: dst[%d] validity bits overlap src[0]'s at a different offset or stride", i);
+    }
+    return STRATA_OK;
+}
+
+// A raster resolved to device memory.
+struct DevOperand {
+    float* data = nullptr;
+    int64_t stride = 0;
+    uint32_t* bits = nullptr;  // 32-bit view of the mask words
+    int64_t bit_off = 0;       // bit of cell (0, 0) in bits
+    int64_t lo_word = 0, hi_word = 0;  // 32-bit words holding the raster's bits
+    // Host staging of the mask, for write-back.
+    int64_t host_w0 = 0, nwords64 = 0;
+};
+
+// The 64-bit words [w0, w0 + n) that hold bits [off, off + cells).
+void mask_words(int64_t off, int64_t cells, int64_t* w0, int64_t* n) {
+    *w0 = off >> 6;
+    *n = ((off + cells + 63) >> 6) - *w0;
+}
+
+int stage_in(strata_ctx* c, cudaStream_t st, const strata_raster& r, int slot, bool copy_data, DevOperand* d) {
+    d->stride = r.stride;
+    int64_t cells = span_cells(r);
+    if (r.on_device) {
+        d->data = r.data;
+        if (r.valid) {
+            int64_t w0 = (r.valid_offset >> 6);
+            d->bits = reinterpret_cast<uint32_t*>(r.valid + w0);
+            d->bit_off = r.valid_offset - w0 * 64;
+        }
+    } else {
+        void* p;
+        int rc = ensure(c, slot, (size_t)cells * 4, &p);
+        if (rc) return rc;
+        d->data = (float*)p;
+        if (copy_data) {
+            cudaError_t e = cudaMemcpyAsync(p, r.data, (size_t)cells * 4, cudaMemcpyHostToDevice, st);
+            if (e != cudaSuccess) return cuda_fail(e, "copy to device");
+        }
+        if (r.valid) {
+            int64_t w0, n;
+            mask_words(r.valid_offset, cells, &w0, &n);
+            void* m;
+            if ((rc = ensure(c, slot + 1, (size_t)n * 8, &m))) return rc;
+            cudaError_t e = cudaMemcpyAsync(m, r.valid + w0, (size_t)n * 8, cudaMemcpyHostToDevice, st);
+            if (e != cudaSuccess) return cuda_fail(e, "copy mask to device");
+            d->bits = (uint32_t*)m;
+            d->bit_off = r.valid_offset - w0 * 64;
+            d->host_w0 = w0;
+            d->nwords64 = n;
+        }
+    }
+    if (d->bits) {
+        d->lo_word = d->bit_off >> 5;
+        d->hi_word = (d->bit_off + cells - 1) >> 5;
+    }
+    return STRATA_OK;
+}
+
+// Copies a host destination back: its cells, and its mask bits merged into
+// the caller's words (the first and last words may hold other rasters'
+// bits).
+int stage_out(strata_ctx* c, cudaStream_t st, const strata_raster& r, const DevOperand& d) {
+    if (r.on_device) return STRATA_OK;
+    cudaError_t e = cudaMemcpy2DAsync(r.data, (size_t)r.stride * 4, d.data, (size_t)r.stride * 4, (size_t)r.width * 4,
+                                      (size_t)r.height, cudaMemcpyDeviceToHost, st);
+    if (e != cudaSuccess) return cuda_fail(e, "copy to host");
+    if (r.valid) {
+        c->host_words.resize((size_t)d.nwords64);
+        e = cudaMemcpyAsync(c->host_words.data(), d.bits, (size_t)d.nwords64 * 8, cudaMemcpyDeviceToHost, st);
+        if (e != cudaSuccess) return cuda_fail(e, "copy mask to host");
+        e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return cuda_fail(e, "copy mask to host");
+        int64_t lo = r.valid_offset, hi = r.valid_offset + span_cells(r);  // bits of the raster's span
+        for (int64_t k = 0; k < d.nwords64; k++) {
+            int64_t w = d.host_w0 + k;
+            uint64_t own = ~0ull;
+            if (w * 64 < lo) own &= ~0ull << (lo - w * 64);
+            if ((w + 1) * 64 > hi) own &= (hi - w * 64) >= 64 ? ~0ull : ((1ull << (hi - w * 64)) - 1);
+            r.valid[w] = (r.valid[w] & ~own) | (c->host_words[(size_t)k] & own);
+        }
+    }
+    return STRATA_OK;
+}
+
+void fill_validity(ValidityParams& v, const DevOperand& s, bool src_masked, const DevOperand& d, int64_t dst_cells_span,
+                   int64_t W, int64_t H, int r, int64_t y0, int64_t y1) {
+    memset(&v, 0, sizeof v);
+    if (src_masked) {
+        v.src_bits = s.bits;
+        v.src_off = s.bit_off;
+        v.src_stride = s.stride;
+        v.src_lo_word = s.lo_word;
+        v.src_hi_word = s.hi_word;
+    }
+    v.dst_bits = d.bits;
+    v.dst_off = d.bit_off;
+    v.dst_stride = d.stride;
+    v.out_x0 = 0;
+    v.out_x1 = W;
+    v.out_y0 = y0;
+    v.out_y1 = y1;
+    v.width = W;
+    v.height = H;
+    v.radius = r;
+    // Words holding the region's bits: rows y0 .. y1-1.
+    int64_t b0 = d.bit_off + y0 * d.stride;
+    int64_t b1 = d.bit_off + (y1 - 1) * d.stride + W;  // exclusive
+    (void)dst_cells_span;
+    v.dst_lo_word = b0 >> 5;
+    v.dst_words = ((b1 + 31) >> 5) - v.dst_lo_word;
+}
+
+}  // namespace
+
+extern "C" int strata_process(strata_ctx* c, const strata_stage* stages, int nstages, const strata_raster* src,
+                              int nsrc, const strata_raster* dst, int ndst, const strata_exec_opts* opts,
+                              strata_stats* stats) {
+    if (!c) return fail(STRATA_EINVAL, "engine: nil context");
+    LaunchParams p;
+    int nout = 0;
+    int rc = plan_stages(stages, nstages, p, &nout);
+    if (rc) return rc;
+    if ((rc = check_opts(opts))) return rc;
+    if ((rc = check_operands(src, nsrc, dst, ndst, nout, p.radius))) return rc;
+
+    std::lock_guard<std::mutex> lock(c->mu);
+    cudaSetDevice(c->device);
+    cudaStream_t st = (opts && opts->stream) ? (cudaStream_t)opts->stream : c->stream;
+    const int64_t W = src[0].width, H = src[0].height;
+
+    DevOperand ds, dd[2];
+    if ((rc = stage_in(c, st, src[0], 0, true, &ds))) return rc;
+    for (int i = 0; i < ndst; i++)
+        if ((rc = stage_in(c, st, dst[i], 2 + 2 * i, false, &dd[i]))) return rc;
+
+    p.src = ds.data;
+    p.src_stride = ds.stride;
+    p.src_x0 = p.src_y0 = 0;
+    p.src_w = W;
+    p.src_h = H;
+    p.dst0 = dd[0].data;
+    p.dst0_stride = dd[0].stride;
+    if (ndst > 1) {
+        p.dst1 = dd[1].data;
+        p.dst1_stride = dd[1].stride;
+    }
+    p.dst_x0 = p.dst_y0 = 0;
+    p.width = W;
+    p.height = H;
+    p.out_x0 = 0;
+    p.out_x1 = W;
+
+    // Row strips: the whole raster at once, or strips of about 2^22 cells
+    // with the cancel flag polled between them.
+    const volatile int32_t* cancel = opts ? opts->cancel : nullptr;
+    int64_t strip = H;
+    if (cancel) {
+        strip = ((int64_t)1 << 22) / W;
+        strip = (strip + 31) / 32 * 32;
+        if (strip < 32) strip = 32;
+    }
+    int64_t bands = 0, window = 0, done_rows = 0;
+    bool canceled = false;
+    for (int64_t y0 = 0; y0 < H; y0 += strip) {
+        if (cancel && *cancel) {
+            canceled = true;
+            break;
+        }
+        int64_t y1 = y0 + strip < H ? y0 + strip : H;
+        p.out_y0 = y0;
+        p.out_y1 = y1;
+        int64_t wc = 0;
+        int64_t t = strata::launch_data(p, st, &wc);
+        if (t < 0) return fail(STRATA_ENOTSUP, "engine: op %d at radius %d has no device kernel", p.op, p.radius);
+        bands += t;
+        window += wc;
+        for (int i = 0; i < ndst; i++) {
+            if (!dst[i].valid) continue;
+            ValidityParams v;
+            fill_validity(v, ds, src[0].valid != nullptr, dd[i], span_cells(dst[i]), W, H, p.radius, y0, y1);
+            strata::launch_validity(v, st);
+        }
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
+        if (cancel) {
+            e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) return cuda_fail(e, "kernel");
+        }
+        done_rows = y1;
+    }
+    bool all_device = src[0].on_device && dst[0].on_device && (ndst < 2 || dst[1].on_device);
+    for (int i = 0; i < ndst; i++)
+        if ((rc = stage_out(c, st, dst[i], dd[i]))) return rc;
+    if (!(all_device && opts && (opts->flags & STRATA_EXEC_ASYNC))) {
+        cudaError_t e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return cuda_fail(e, "kernel");
+    }
+    if (stats) {
+        int64_t cells = done_rows * W;
+        stats->cells += cells;
+        stats->ideal += cells * 4 * (1 + nout);
+        stats->bands += bands;
+        stats->kernel_read += window * 4;
+        stats->kernel_written += cells * 4 * nout;
+    }
+    if (canceled) return fail(STRATA_ECANCELED, "context canceled");
+    return STRATA_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Stage builders.
+
+namespace {
+
+void stage_init(strata_stage* s, uint32_t op) {
+    memset(s, 0, sizeof *s);
+    s->op = op;
+}
+
+// terrain.resolveCells (terrain/stencil.go:16-34).
+int resolve_cells(double cs, double csy, double z, double* cx, double* cy, double* zf) {
+    if (!(cs > 0) || std::isinf(cs))
+        return fail(STRATA_EINVAL, "terrain: CellSize must be positive and finite, got %s", fmt_v(cs).c_str());
+    if (csy == 0) csy = cs;
+    if (!(csy > 0) || std::isinf(csy))
+        return fail(STRATA_EINVAL, "terrain: CellSizeY must be positive and finite (or 0 for CellSize), got %s",
+                    fmt_v(csy).c_str());
+    if (z == 0) z = 1;
+    if (std::isnan(z) || std::isinf(z))
+        return fail(STRATA_EINVAL, "terrain: ZFactor must be finite, got %s", fmt_v(z).c_str());
+    *cx = cs;
+    *cy = csy;
+    *zf = z;
+    return STRATA_OK;
+}
+
+bool usable(float k) { return k != 0 && !std::isinf(k); }
+
+// terrain.cellSizes (terrain/stencil.go:37-49) with stencil.HornScales
+// (internal/stencil/horn.go:114-116).
+int horn_scales(double cs, double csy, double z, float* kx, float* ky) {
+    double cx, cy, zf;
+    int rc = resolve_cells(cs, csy, z, &cx, &cy, &zf);
+    if (rc) return rc;
+    *kx = (float)(zf / (8 * cx));
+    *ky = (float)(zf / (8 * cy));
+    if (!usable(*kx) || !usable(*ky))
+        return fail(STRATA_EINVAL,
+                    "terrain: ZFactor/(8·CellSize) and ZFactor/(8·CellSizeY) must be finite and non-zero as float32, "
+                    "got %s and %s for CellSize %s, CellSizeY %s and ZFactor %s",
+                    fmt_v(*kx, true).c_str(), fmt_v(*ky, true).c_str(), fmt_v(cs).c_str(), fmt_v(csy).c_str(),
+                    fmt_v(z).c_str());
+    return STRATA_OK;
+}
+
+// The fit-radius switch of terrain/fit.go:187-226: 0 is Horn's 3x3
+// kernel, 1..8 Wood's fit (checked at terrain/fit.go:37-40).
+int fit_radius(int32_t fr) {
+    if (fr == 0) return STRATA_OK;
+    if (fr < 0 || fr > STRATA_MAX_RADIUS)
+        return fail(STRATA_EINVAL, "terrain: FitRadius must be 0 to %d, got %d", STRATA_MAX_RADIUS, fr);
+    return fail(STRATA_ENOTSUP, "terrain: FitRadius %d (Wood's quadratic fit) is not on the gpu backend", fr);
+}
+
+int check_focal_radius(int r) {
+    if (r < 1 || r > STRATA_MAX_RADIUS)
+        return fail(STRATA_EINVAL, "focal: Radius must be 1 to %d, got %d", STRATA_MAX_RADIUS, r);
+    return STRATA_OK;
+}
+
+int check_finite(const char* what, const float* v, int n) {
+    for (int i = 0; i < n; i++)
+        if (!finite32(v[i]))
+            return fail(STRATA_EINVAL, "focal: %s must be finite, got %s at index %d", what, fmt_v(v[i], true).c_str(),
+                        i);
+    return STRATA_OK;
+}
+
+// transfer.checkIncreasing (transfer/transfer.go:225-239).
+int check_increasing(const char* op, const char* name, const float* xs, int n) {
+    for (int i = 0; i < n; i++)
+        if (xs[i] != xs[i]) return fail(STRATA_EINVAL, "%s: %s must not hold NaN, but %s[%d] is NaN", op, name, name, i);
+    for (int i = 1; i < n; i++)
+        if (!(xs[i - 1] < xs[i]))
+            return fail(STRATA_EINVAL, "%s: %s must be strictly increasing, but %s[%d] = %s is not above %s[%d] = %s", op,
+                        name, name, i, fmt_v(xs[i], true).c_str(), name, i - 1, fmt_v(xs[i - 1], true).c_str());
+    return STRATA_OK;
+}
+
+}  // namespace
+
+extern "C" int strata_stage_gradient(const strata_gradient_options* o, strata_stage* out) {
+    if (!o || !out) return fail(STRATA_EINVAL, "terrain: nil options");
+    int rc = fit_radius(o->fit_radius);
+    if (rc) return rc;
+    float kx, ky;
+    if ((rc = horn_scales(o->cell_size, o->cell_size_y, o->z_factor, &kx, &ky))) return rc;
+    stage_init(out, STRATA_OP_GRADIENT);
+    out->radius = 1;
+    out->k[0] = kx;
+    out->k[1] = ky;
+    return STRATA_OK;
+}
+
+extern "C" int strata_stage_slope(const strata_slope_options* o, strata_stage* out) {
+    if (!o || !out) return fail(STRATA_EINVAL, "terrain: nil options");
+    int rc = fit_radius(o->fit_radius);
+    if (rc) return rc;
+    float kx, ky;
+    if ((rc = horn_scales(o->cell_size, o->cell_size_y, o->z_factor, &kx, &ky))) return rc;
+    // terrain.slopeScale (terrain/slope.go:84-95).
+    float scale;
+    int take_atan;
+    switch (o->units) {
+    case 0: scale = (float)(180 / M_PI); take_atan = 1; break;
+    case 2: scale = 1; take_atan = 1; break;
+    case 1: scale = 100; take_atan = 0; break;
+    default: return fail(STRATA_EINVAL, "terrain: unknown SlopeUnits %d", o->units);
+    }
+    stage_init(out, STRATA_OP_SLOPE);
+    out->radius = 1;
+    out->kind = take_atan;
+    out->k[0] = kx;
+    out->k[1] = ky;
+    out->k[2] = scale;
+    return STRATA_OK;
+}
+
+extern "C" int strata_stage_aspect(const strata_aspect_options* o, strata_stage* out) {
+    if (!o || !out) return fail(STRATA_EINVAL, "terrain: nil options");
+    int rc = fit_radius(o->fit_radius);
+    if (rc) return rc;
+    float kx, ky;
+    if ((rc = horn_scales(o->cell_size, o->cell_size_y, o->z_factor, &kx, &ky))) return rc;
+    stage_init(out, STRATA_OP_ASPECT);
+    out->radius = 1;
+    out->kind = o->trigonometric ? 1 : 0;
+    out->k[0] = kx;
+    out->k[1] = ky;
+    out->k[2] = o->zero_for_flat ? 0.0f : -1.0f;  // terrain.aspectFlat, AspectFlat = -1
+    return STRATA_OK;
+}
+
+extern "C" int strata_stage_hillshade(const strata_hillshade_options* o, strata_stage* out) {
+    if (!o || !out) return fail(STRATA_EINVAL, "terrain: nil options");
+    int rc = fit_radius(o->fit_radius);
+    if (rc) return rc;
+    float kx, ky;
+    if ((rc = horn_scales(o->cell_size, o->cell_size_y, o->z_factor, &kx, &ky))) return rc;
+    // terrain.hillshadeLight (terrain/hillshade.go:94-117).
+    double az = o->azimuth, alt = o->altitude;
+    if (std::isnan(az) || std::isinf(az))
+        return fail(STRATA_EINVAL, "terrain: Azimuth must be finite, got %s", fmt_v(az).c_str());
+    if (az == 0) az = 315;
+    if (alt == 0) alt = 45;
+    if (!(alt > 0 && alt <= 90))
+        return fail(STRATA_EINVAL, "terrain: Altitude must be in (0, 90] (or 0 for 45), got %s",
+                    fmt_v(o->altitude).c_str());
+    az = std::fmod(az, 360);
+    az = az * M_PI / 180;
+    alt = alt * M_PI / 180;
+    stage_init(out, STRATA_OP_HILLSHADE);
+    out->radius = 1;
+    out->k[0] = kx;
+    out->k[1] = ky;
+    out->k[2] = (float)(255 * std::sin(alt));
+    out->k[3] = (float)(-255 * std::cos(alt) * std::sin(az));
+    out->k[4] = (float)(255 * std::cos(alt) * std::cos(az));
+    return STRATA_OK;
+}
+
+extern "C" int strata_stage_curvature(const strata_curvature_options* o, strata_stage* out) {
+    if (!o || !out) return fail(STRATA_EINVAL, "terrain: nil options");
+    int rc = fit_radius(o->fit_radius);
+    if (rc) return rc;
+    double cx, cy, z;
+    if ((rc = resolve_cells(o->cell_size, o->cell_size_y, o->z_factor, &cx, &cy, &z))) return rc;
+    if (o->type < 0 || o->type > 2) return fail(STRATA_EINVAL, "terrain: unknown CurvatureType %d", o->type);
+    // stencil.ZTScales (internal/stencil/curvature.go:29-33).
+    float k[5] = {(float)(z / (2 * cx)), (float)(z / (2 * cy)), (float)(z / (cx * cx)), (float)(z / (cy * cy)),
+                  (float)(z / (4 * cx * cy))};
+    for (float v : k)
+        if (!usable(v))
+            return fail(STRATA_EINVAL,
+                        "terrain: ZFactor/(2·CellSize), ZFactor/CellSize² and ZFactor/(4·CellSize·CellSizeY), and the "
+                        "same for CellSizeY, must be finite and non-zero as float32, got %s, %s, %s, %s and %s for "
+                        "CellSize %s, CellSizeY %s and ZFactor %s",
+                        fmt_v(k[0], true).c_str(), fmt_v(k[1], true).c_str(), fmt_v(k[2], true).c_str(),
+                        fmt_v(k[3], true).c_str(), fmt_v(k[4], true).c_str(), fmt_v(o->cell_size).c_str(),
+                        fmt_v(o->cell_size_y).c_str(), fmt_v(o->z_factor).c_str());
+    stage_init(out, STRATA_OP_CURVATURE);
+    out->radius = 1;
+    out->kind = o->type;
+    for (int i = 0; i < 5; i++) out->k[i] = k[i];
+    return STRATA_OK;
+}
+
+extern "C" int strata_stage_ruggedness(const strata_ruggedness_options* o, strata_stage* out) {
+    if (!o || !out) return fail(STRATA_EINVAL, "terrain: nil options");
+    int r = o->radius == 0 ? 1 : o->radius;
+    if (r < 1 || r > STRATA_MAX_RADIUS)
+        return fail(STRATA_EINVAL, "terrain: RuggednessOptions.Radius must be 0 to %d, got %d", STRATA_MAX_RADIUS,
+                    o->radius);
+    if (o->type < 0 || o->type > 3) return fail(STRATA_EINVAL, "terrain: unknown RuggednessType %d", o->type);
+    stage_init(out, STRATA_OP_RUGGEDNESS);
+    out->radius = r;
+    out->kind = o->type;
+    return STRATA_OK;
+}
+
+extern "C" int strata_stage_correlate(const strata_weights_options* o, int convolve, strata_stage* out) {
+    if (!o || !out) return fail(STRATA_EINVAL, "focal: nil options");
+    int rc = check_focal_radius(o->radius);
+    if (rc) return rc;
+    int d = 2 * o->radius + 1;
+    if (o->nweights != d * d || (!o->weights && o->nweights))
+        return fail(STRATA_EINVAL, "focal: Radius %d needs %d×%d = %d Weights, got %d", o->radius, d, d, d * d,
+                    o->nweights);
+    if ((rc = check_finite("Weights", o->weights, o->nweights))) return rc;
+    stage_init(out, STRATA_OP_CORRELATE);
+    out->radius = o->radius;
+    out->flags = convolve ? STRATA_STAGE_ROTATE180 : 0;
+    out->table[0] = o->weights;
+    out->table_len[0] = o->nweights;
+    return STRATA_OK;
+}
+
+extern "C" int strata_stage_separable(const strata_separable_options* o, strata_stage* out) {
+    if (!o || !out) return fail(STRATA_EINVAL, "focal: nil options");
+    int rc = check_focal_radius(o->radius);
+    if (rc) return rc;
+    int d = 2 * o->radius + 1;
+    if (o->nrow != d || o->ncol != d || !o->row || !o->col)
+        return fail(STRATA_EINVAL, "focal: Radius %d needs %d Row and %d Col taps, got %d and %d", o->radius, d, d,
+                    o->nrow, o->ncol);
+    if ((rc = check_finite("Row taps", o->row, o->nrow))) return rc;
+    if ((rc = check_finite("Col taps", o->col, o->ncol))) return rc;
+    stage_init(out, STRATA_OP_SEPARABLE);
+    out->radius = o->radius;
+    out->table[0] = o->row;
+    out->table_len[0] = o->nrow;
+    out->table[1] = o->col;
+    out->table_len[1] = o->ncol;
+    return STRATA_OK;
+}
+
+extern "C" int strata_stage_box(const strata_box_options* o, uint32_t op, strata_stage* out) {
+    if (!o || !out) return fail(STRATA_EINVAL, "focal: nil options");
+    if (op != STRATA_OP_MEAN && op != STRATA_OP_MIN && op != STRATA_OP_MAX)
+        return fail(STRATA_EINVAL, "focal: op %u is not Mean, Min or Max", op);
+    int rc = check_focal_radius(o->radius);
+    if (rc) return rc;
+    stage_init(out, op);
+    out->radius = o->radius;
+    return STRATA_OK;
+}
+
+extern "C" int strata_stage_lookup(const float* xs, const float* ys, int32_t n, strata_stage* out) {
+    const char* op = "transfer.Lookup";
+    if (!out) return fail(STRATA_EINVAL, "%s: nil stage", op);
+    if (n < 0) return fail(STRATA_EINVAL, "%s: negative table length %d", op, n);
+    if (n == 0) return fail(STRATA_EINVAL, "%s: the table needs at least one knot", op);
+    int rc = check_increasing(op, "xs", xs, n);
+    if (rc) return rc;
+    for (int i = 0; i < n; i++)
+        if (!finite32(xs[i]))
+            return fail(STRATA_EINVAL, "%s: xs must be finite, but xs[%d] = %s", op, i, fmt_v(xs[i], true).c_str());
+    if (n > STRATA_MAX_KNOTS)
+        return fail(STRATA_ENOTSUP, "%s: the gpu backend takes at most %d knots, got %d", op, STRATA_MAX_KNOTS, n);
+    stage_init(out, STRATA_OP_LOOKUP);
+    out->table[0] = xs;
+    out->table[1] = ys;
+    out->table_len[0] = n;
+    out->table_len[1] = n;
+    return STRATA_OK;
+}
+
+extern "C" int strata_stage_reclass(const float* breaks, int32_t nbreaks, const float* values, int32_t nvalues,
+                                    strata_stage* out) {
+    const char* op = "transfer.Reclass";
+    if (!out) return fail(STRATA_EINVAL, "%s: nil stage", op);
+    if (nvalues != nbreaks + 1)
+        return fail(STRATA_EINVAL, "%s: values must hold one more element than breaks, got %d values and %d breaks", op,
+                    nvalues, nbreaks);
+    int rc = check_increasing(op, "breaks", breaks, nbreaks);
+    if (rc) return rc;
+    if (nbreaks > STRATA_MAX_KNOTS)
+        return fail(STRATA_ENOTSUP, "%s: the gpu backend takes at most %d breaks, got %d", op, STRATA_MAX_KNOTS,
+                    nbreaks);
+    stage_init(out, STRATA_OP_RECLASS);
+    out->table[0] = breaks;
+    out->table[1] = values;
+    out->table_len[0] = nbreaks;
+    out->table_len[1] = nvalues;
+    return STRATA_OK;
+}
+
+extern "C" int strata_focal_gaussian(int32_t radius, double sigma, float* taps) {
+    int rc = check_focal_radius(radius);
+    if (rc) return rc;
+    if (!(sigma > 0) || std::isinf(sigma))
+        return fail(STRATA_EINVAL, "focal: Gaussian sigma must be positive and finite, got %s", fmt_v(sigma).c_str());
+    if (!taps) return fail(STRATA_EINVAL, "focal: nil taps");
+    // focal.Gaussian (focal/separable.go:59-76).
+    double g[2 * STRATA_MAX_RADIUS + 1];
+    double sum = 0;
+    for (int i = 0; i < 2 * radius + 1; i++) {
+        double x = (double)(i - radius);
+        g[i] = std::exp(-x * x / (2 * sigma * sigma));
+        sum += g[i];
+    }
+    for (int i = 0; i < 2 * radius + 1; i++) taps[i] = (float)(g[i] / sum);
+    return STRATA_OK;
+}
+
+// ---------------------------------------------------------------------------
+// exec.ProcessChunked (internal/exec/chunked.go:33-464): tiles of the
+// source, grown by the radius and clipped to the raster, are read into
+// page-locked buffers, computed on the device, and handed to the sinks in
+// plan order. Two buffer sets alternate, so tile i computes and copies
+// while the host writes tile i-1 and reads tile i+1.
+
+namespace {
+
+int64_t round_up64(int64_t v) { return (v + 63) / 64 * 64; }
+
+struct PinnedBuf {
+    void* p = nullptr;
+    size_t n = 0;
+    ~PinnedBuf() {
+        if (p) cudaFreeHost(p);
+    }
+    int get(size_t bytes) {
+        if (n >= bytes) return STRATA_OK;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        n = 0;
+        cudaError_t e = cudaHostAlloc(&p, bytes ? bytes : 1, cudaHostAllocDefault);
+        if (e != cudaSuccess) return cuda_fail(e, "page-locked buffer");
+        n = bytes;
+        return STRATA_OK;
+    }
+};
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t n = 0;
+    ~DevBuf() {
+        if (p) cudaFree(p);
+    }
+    int get(size_t bytes) {
+        if (n >= bytes) return STRATA_OK;
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+        cudaError_t e = cudaMalloc(&p, bytes ? bytes : 1);
+        if (e != cudaSuccess) return cuda_fail(e, "device tile buffer");
+        n = bytes;
+        return STRATA_OK;
+    }
+};
+
+// One tile's buffers: the input window and the outputs, host and device.
+struct TileSet {
+    PinnedBuf in_data, in_bits, out_data[2], out_bits[2];
+    DevBuf d_in_data, d_in_bits, d_out_data[2], d_out_bits[2];
+    cudaEvent_t done = nullptr;
+    int64_t x0 = 0, y0 = 0, x1 = 0, y1 = 0;
+    int64_t out_stride[2] = {0, 0};
+    bool pending = false;
+};
+
+}  // namespace
+
+extern "C" int strata_process_chunked(strata_ctx* c, const strata_stage* stages, int nstages,
+                                      const strata_source* src, int nsrc, const strata_sink* dst, int ndst,
+                                      const strata_exec_opts* opts, strata_stats* stats) {
+    if (!c) return fail(STRATA_EINVAL, "engine: nil context");
+    LaunchParams p;
+    int nout = 0;
+    int rc = plan_stages(stages, nstages, p, &nout);
+    if (rc) return rc;
+    if ((rc = check_opts(opts))) return rc;
+    if (nsrc != 1 || ndst != nout || !src || !dst)
+        return fail(STRATA_EINVAL, "engine: kernel takes 1 inputs and %d outputs, got %d and %d", nout, nsrc, ndst);
+    for (int i = 0; i < ndst; i++)
+        if (!dst[i].write) return fail(STRATA_EINVAL, "engine: dst[%d] is a nil sink", i);
+    if (!src[0].read) return fail(STRATA_EINVAL, "engine: src[0] is a nil source");
+    const int64_t W = dst[0].width, H = dst[0].height;
+    if (W <= 0 || H <= 0)
+        return fail(STRATA_EINVAL, "engine: dst[0] is %lld×%lld; sizes must be positive", (long long)W, (long long)H);
+    if (src[0].width != W || src[0].height != H)
+        return fail(STRATA_EINVAL, "engine: src[0] is %lld×%lld, dst[0] is %lld×%lld", (long long)src[0].width,
+                    (long long)src[0].height, (long long)W, (long long)H);
+    for (int i = 0; i < ndst; i++) {
+        if (dst[i].width != W || dst[i].height != H)
+            return fail(STRATA_EINVAL, "engine: dst[%d] is %lld×%lld, dst[0] is %lld×%lld", i, (long long)dst[i].width,
+                        (long long)dst[i].height, (long long)W, (long long)H);
+        if (src[0].masked && !dst[i].masked)
+            return fail(STRATA_EINVAL, "engine: a source is Masked but dst[%d] is not; its validity would be lost", i);
+    }
+
+    const int r = p.radius;
+    const int64_t tw = (opts && opts->tile_width > 0) ? std::min<int64_t>(opts->tile_width, W) : W;
+    const int64_t th = (opts && opts->tile_height > 0) ? std::min<int64_t>(opts->tile_height, H) : H;
+    const int64_t tiles_x = (W + tw - 1) / tw;
+    const int64_t ntiles = tiles_x * ((H + th - 1) / th);
+    const int64_t inW = std::min(W, tw + 2 * r), inH = std::min(H, th + 2 * r);
+    const bool in_masked = src[0].masked != 0;
+    const int64_t in_stride = in_masked ? round_up64(inW) : inW;
+    const int64_t in_cells = (inH - 1) * in_stride + inW;
+
+    std::lock_guard<std::mutex> lock(c->mu);
+    cudaSetDevice(c->device);
+    cudaStream_t st = (opts && opts->stream) ? (cudaStream_t)opts->stream : c->stream;
+
+    TileSet sets[2];
+    for (auto& s : sets) {
+        if ((rc = s.in_data.get((size_t)in_cells * 4)) || (rc = s.d_in_data.get((size_t)in_cells * 4))) return rc;
+        if (in_masked) {
+            size_t words = (size_t)((in_cells + 63) / 64);
+            if ((rc = s.in_bits.get(words * 8)) || (rc = s.d_in_bits.get(words * 8))) return rc;
+        }
+        for (int i = 0; i < ndst; i++) {
+            int64_t os = dst[i].masked ? round_up64(tw) : tw;
+            int64_t oc = (th - 1) * os + tw;
+            s.out_stride[i] = os;
+            if ((rc = s.out_data[i].get((size_t)oc * 4)) || (rc = s.d_out_data[i].get((size_t)oc * 4))) return rc;
+            if (dst[i].masked) {
+                size_t words = (size_t)((oc + 63) / 64);
+                if ((rc = s.out_bits[i].get(words * 8)) || (rc = s.d_out_bits[i].get(words * 8))) return rc;
+            }
+        }
+        if (cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming) != cudaSuccess)
+            return fail(STRATA_ECUDA, "strata_cuda: cudaEventCreate");
+    }
+    struct EventGuard {
+        TileSet* s;
+        ~EventGuard() {
+            for (int i = 0; i < 2; i++)
+                if (s[i].done) cudaEventDestroy(s[i].done);
+        }
+    } guard{sets};
+
+    strata_stats local = {};
+    int status = STRATA_OK;
+    // Hands a finished tile to the sinks.
+    auto flush = [&](TileSet& s) -> int {
+        if (!s.pending) return STRATA_OK;
+        s.pending = false;
+        cudaError_t e = cudaEventSynchronize(s.done);
+        if (e != cudaSuccess) return cuda_fail(e, "tile");
+        for (int i = 0; i < ndst; i++) {
+            strata_raster b = {};
+            b.data = (float*)s.out_data[i].p;
+            b.width = s.x1 - s.x0;
+            b.height = s.y1 - s.y0;
+            b.stride = s.out_stride[i];
+            b.valid = dst[i].masked ? (uint64_t*)s.out_bits[i].p : nullptr;
+            if (dst[i].write(dst[i].user, &b, s.x0, s.y0) != 0)
+                return fail(STRATA_EIO, "engine: writing dst[%d] at (%lld, %lld) failed", i, (long long)s.x0,
+                            (long long)s.y0);
+        }
+        int64_t cells = (s.x1 - s.x0) * (s.y1 - s.y0);
+        local.sink_written += cells * 4 * ndst;
+        local.cells += cells;
+        local.ideal += cells * 4 * (1 + nout);
+        local.kernel_written += cells * 4 * nout;
+        local.tiles++;
+        return STRATA_OK;
+    };
+
+    const volatile int32_t* cancel = opts ? opts->cancel : nullptr;
+    for (int64_t t = 0; t < ntiles && status == STRATA_OK; t++) {
+        TileSet& s = sets[t & 1];
+        // The set's previous tile (t - 2) must be with the sinks before its
+        // buffers are reused; tile t - 1 is written while t computes.
+        if ((status = flush(s))) break;
+        if (cancel && *cancel) {
+            status = STRATA_ECANCELED;
+            break;
+        }
+        const int64_t x0 = (t % tiles_x) * tw, y0 = (t / tiles_x) * th;
+        const int64_t x1 = std::min(x0 + tw, W), y1 = std::min(y0 + th, H);
+        const int64_t rx0 = std::max<int64_t>(0, x0 - r), ry0 = std::max<int64_t>(0, y0 - r);
+        const int64_t rx1 = std::min(W, x1 + r), ry1 = std::min(H, y1 + r);
+        const int64_t ww = rx1 - rx0, wh = ry1 - ry0;
+        const int64_t ws = in_masked ? round_up64(ww) : ww;
+        strata_raster b = {};
+        b.data = (float*)s.in_data.p;
+        b.width = ww;
+        b.height = wh;
+        b.stride = ws;
+        b.valid = in_masked ? (uint64_t*)s.in_bits.p : nullptr;
+        if (in_masked) memset(s.in_bits.p, 0, (size_t)(((wh - 1) * ws + ww + 63) / 64) * 8);
+        if (src[0].read(src[0].user, &b, rx0, ry0) != 0) {
+            status = fail(STRATA_EIO, "engine: reading src[0] at (%lld, %lld) failed", (long long)rx0, (long long)ry0);
+            break;
+        }
+        local.source_read += ww * wh * 4;
+        const int64_t wcells = (wh - 1) * ws + ww;
+        cudaError_t e = cudaMemcpyAsync(s.d_in_data.p, s.in_data.p, (size_t)wcells * 4, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess && in_masked)
+            e = cudaMemcpyAsync(s.d_in_bits.p, s.in_bits.p, (size_t)((wcells + 63) / 64) * 8, cudaMemcpyHostToDevice,
+                                st);
+        for (int i = 0; i < ndst && e == cudaSuccess; i++)
+            if (dst[i].masked) {
+                int64_t oc = (y1 - y0 - 1) * s.out_stride[i] + (x1 - x0);
+                e = cudaMemsetAsync(s.d_out_bits[i].p, 0, (size_t)((oc + 63) / 64) * 8, st);
+            }
+        if (e != cudaSuccess) {
+            status = cuda_fail(e, "tile copy");
+            break;
+        }
+        LaunchParams q = p;
+        q.src = (const float*)s.d_in_data.p;
+        q.src_stride = ws;
+        q.src_x0 = rx0;
+        q.src_y0 = ry0;
+        q.src_w = ww;
+        q.src_h = wh;
+        q.dst0 = (float*)s.d_out_data[0].p;
+        q.dst0_stride = s.out_stride[0];
+        if (ndst > 1) {
+            q.dst1 = (float*)s.d_out_data[1].p;
+            q.dst1_stride = s.out_stride[1];
+        }
+        q.dst_x0 = x0;
+        q.dst_y0 = y0;
+        q.out_x0 = x0;
+        q.out_y0 = y0;
+        q.out_x1 = x1;
+        q.out_y1 = y1;
+        q.width = W;
+        q.height = H;
+        int64_t wc = 0;
+        int64_t nt = strata::launch_data(q, st, &wc);
+        if (nt < 0) {
+            status = fail(STRATA_ENOTSUP, "engine: op %d at radius %d has no device kernel", p.op, p.radius);
+            break;
+        }
+        local.bands += nt;
+        local.kernel_read += wc * 4;
+        for (int i = 0; i < ndst; i++) {
+            if (!dst[i].masked) continue;
+            ValidityParams v;
+            memset(&v, 0, sizeof v);
+            if (in_masked) {
+                v.src_bits = (const uint32_t*)s.d_in_bits.p;
+                v.src_off = 0;
+                v.src_stride = ws;
+                v.src_lo_word = 0;
+                v.src_hi_word = (wcells - 1) >> 5;
+            }
+            v.src_x0 = rx0;
+            v.src_y0 = ry0;
+            v.dst_bits = (uint32_t*)s.d_out_bits[i].p;
+            v.dst_off = 0;
+            v.dst_stride = s.out_stride[i];
+            v.dst_x0 = x0;
+            v.dst_y0 = y0;
+            v.out_x0 = x0;
+            v.out_y0 = y0;
+            v.out_x1 = x1;
+            v.out_y1 = y1;
+            v.width = W;
+            v.height = H;
+            v.radius = r;
+            int64_t oc = (y1 - y0 - 1) * s.out_stride[i] + (x1 - x0);
+            v.dst_lo_word = 0;
+            v.dst_words = (oc + 31) >> 5;
+            strata::launch_validity(v, st);
+        }
+        for (int i = 0; i < ndst && e == cudaSuccess; i++) {
+            int64_t oc = (y1 - y0 - 1) * s.out_stride[i] + (x1 - x0);
+            e = cudaMemcpyAsync(s.out_data[i].p, s.d_out_data[i].p, (size_t)oc * 4, cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess && dst[i].masked)
+                e = cudaMemcpyAsync(s.out_bits[i].p, s.d_out_bits[i].p, (size_t)((oc + 63) / 64) * 8,
+                                    cudaMemcpyDeviceToHost, st);
+        }
+        if (e == cudaSuccess) e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaEventRecord(s.done, st);
+        if (e != cudaSuccess) {
+            status = cuda_fail(e, "tile");
+            break;
+        }
+        s.x0 = x0;
+        s.y0 = y0;
+        s.x1 = x1;
+        s.y1 = y1;
+        s.pending = true;
+        // Write the other set's tile (t - 1) while this one runs.
+        if ((status = flush(sets[(t + 1) & 1]))) break;
+    }
+    // Tiles already computed are written in plan order, after a cancel too;
+    // after a failure nothing more is written.
+    if (status == STRATA_OK || status == STRATA_ECANCELED) {
+        for (int64_t k = 0; k < 2; k++) {
+            // the older pending tile first
+            TileSet* a = &sets[0];
+            TileSet* b2 = &sets[1];
+            TileSet* first = (a->pending && b2->pending) ? ((a->y0 < b2->y0 || (a->y0 == b2->y0 && a->x0 < b2->x0)) ? a : b2)
+                                                          : (a->pending ? a : b2);
+            int frc = flush(*first);
+            if (frc) {
+                status = frc;
+                break;
+            }
+        }
+    } else {
+        cudaStreamSynchronize(st);
+    }
+    if (stats) {
+        stats->cells += local.cells;
+        stats->ideal += local.ideal;
+        stats->tiles += local.tiles;
+        stats->bands += local.bands;
+        stats->source_read += local.source_read;
+        stats->sink_written += local.sink_written;
+        stats->kernel_read += local.kernel_read;
+        stats->kernel_written += local.kernel_written;
+    }
+    if (status == STRATA_ECANCELED) return fail(STRATA_ECANCELED, "context canceled");
+    return status;
+}

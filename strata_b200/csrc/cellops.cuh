@@ -1,0 +1,249 @@
+// cellops.cuh - the per-cell arithmetic of strata's raster-stencil kernels,
+// as device functions.
+//
+// Every float operation is an explicitly rounded intrinsic (__fadd_rn,
+// __fmul_rn, __fdiv_rn, ...), which the compiler never contracts into an
+// FMA, so each result is the reference scalar backend's bits: strata wraps
+// every product in float32(...) for the same reason
+// (internal/stencil/horn.go:12-18, internal/focalrow/focalrow.go:14-33).
+// The operation order of each function follows the reference function
+// cited beside it.
+#pragma once
+
+#include <cstdint>
+
+namespace strata {
+namespace cell {
+
+__device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float div(float a, float b) { return __fdiv_rn(a, b); }
+
+// float32(math.Sqrt(float64(x))): the float64 root of a float32 rounded to
+// float32 equals the correctly rounded float32 root (53 >= 2*24 + 2, so the
+// double rounding is innocuous), which __fsqrt_rn computes directly.
+__device__ __forceinline__ float sqrt64of32(float x) { return __fsqrt_rn(x); }
+
+__device__ __forceinline__ float nanf32() { return __int_as_float(0x7fc00000); }
+__device__ __forceinline__ float abs32(float x) { return __int_as_float(__float_as_int(x) & 0x7fffffff); }
+
+// Go's builtin min and max for float32: NaN wins, -0 orders below +0.
+__device__ __forceinline__ float go_min(float a, float b) {
+    if (a != a) return a;
+    if (b != b) return b;
+    if (a == b) return __int_as_float(__float_as_int(a) | __float_as_int(b));
+    return a < b ? a : b;
+}
+__device__ __forceinline__ float go_max(float a, float b) {
+    if (a != a) return a;
+    if (b != b) return b;
+    if (a == b) return __int_as_float(__float_as_int(a) & __float_as_int(b));
+    return a > b ? a : b;
+}
+
+// Atan32 constants (internal/stencil/horn.go:226-235, aspect.go:10-14),
+// each the correctly rounded float32 of the reference's expression.
+constexpr float kTan3Pi8 = 0x1.3504f4p+1f;
+constexpr float kTanPi8 = 0x1.a8279ap-2f;
+constexpr float kPi2 = 0x1.921fb6p+0f;
+constexpr float kPi4 = 0x1.921fb6p-1f;
+constexpr float kC4 = 0x1.49e1a2p-4f;
+constexpr float kC3 = 0x1.1c370ap-3f;
+constexpr float kC2 = 0x1.9924bep-3f;
+constexpr float kC1 = 0x1.555454p-2f;
+constexpr float kPi = 0x1.921fb6p+1f;
+constexpr float kRadToDeg = 0x1.ca5dc2p+5f;
+
+// Atan32 (internal/stencil/horn.go:249-262): the Cephes float32
+// arctangent with the argument reduced around 0, pi/4 or pi/2.
+__device__ __forceinline__ float atan32(float x) {
+    float num = x, den = 1.0f, y0 = 0.0f;
+    if (x > kTanPi8) {
+        num = sub(x, 1.0f);
+        den = add(x, 1.0f);
+        y0 = kPi4;
+    }
+    if (x > kTan3Pi8) {
+        num = -1.0f;
+        den = x;
+        y0 = kPi2;
+    }
+    float t = div(num, den);
+    float z = mul(t, t);
+    float p = sub(mul(kC4, z), kC3);
+    p = add(mul(p, z), kC2);
+    p = sub(mul(p, z), kC1);
+    return add(y0, add(mul(mul(p, z), t), t));
+}
+
+// Atan2F32 (internal/stencil/aspect.go:33-47).
+__device__ __forceinline__ float atan2f32(float y, float x) {
+    float ax = abs32(x), ay = abs32(y);
+    float a = atan32(div(ay, ax));
+    if (ay == 0.0f && ax == 0.0f) a = 0.0f;
+    if (ay == ax && ay > 0x1.fffffep+127f) a = kPi4;
+    if (__float_as_uint(x) & 0x80000000u) a = sub(kPi, a);
+    return __uint_as_float(__float_as_uint(a) | (__float_as_uint(y) & 0x80000000u));
+}
+
+// hornDX / hornDY (internal/stencil/horn.go:152-160).
+__device__ __forceinline__ float horn_dx(float z1, float z3, float z4, float z6, float z7, float z9) {
+    float d = sub(z6, z4);
+    return add(add(sub(z3, z1), sub(z9, z7)), add(d, d));
+}
+__device__ __forceinline__ float horn_dy(float z1, float z2, float z3, float z7, float z8, float z9) {
+    float d = sub(z8, z2);
+    return add(add(sub(z7, z1), sub(z9, z3)), add(d, d));
+}
+
+// magnitude (internal/stencil/horn.go:220-222).
+__device__ __forceinline__ float magnitude(float gx, float gy) {
+    return sqrt64of32(add(mul(gx, gx), mul(gy, gy)));
+}
+
+// Slope from a gradient (horn.go:193-216, gradrow.go:44-59).
+__device__ __forceinline__ float slope(float gx, float gy, float scale, bool take_atan) {
+    float m = magnitude(gx, gy);
+    return take_atan ? mul(atan32(m), scale) : mul(m, scale);
+}
+
+// aspectArgs + aspectDegrees (internal/stencil/aspect.go:97-121).
+__device__ __forceinline__ float aspect(float gx, float gy, float flat, bool trig) {
+    float y, x;
+    if (trig) {
+        y = gy;
+        x = sub(0.0f, gx);
+    } else {
+        y = sub(0.0f, gx);
+        x = gy;
+    }
+    float d = mul(atan2f32(y, x), kRadToDeg);
+    float off = d < 0.0f ? 360.0f : 0.0f;
+    d = add(d, off);
+    if (d >= 360.0f) d = 0.0f;
+    if (y == 0.0f && x == 0.0f) d = flat;
+    return d;
+}
+
+// shade (internal/stencil/aspect.go:162-173).
+__device__ __forceinline__ float shade(float gx, float gy, float c, float bx, float by) {
+    float num = add(c, add(mul(bx, gx), mul(by, gy)));
+    float den = sqrt64of32(add(1.0f, add(mul(gx, gx), mul(gy, gy))));
+    float v = div(num, den);
+    if (v < 0.0f) v = 0.0f;
+    if (v > 255.0f) v = 255.0f;
+    return v;
+}
+
+// Zevenbergen-Thorne curvature (internal/stencil/curvature.go:79-129):
+// ztDerivs, then the profile (0), plan (1) or mean (2) formula.
+__device__ __forceinline__ float zt_curvature(float z1, float z2, float z3, float z4, float z5, float z6,
+                                              float z7, float z8, float z9, const float* k, int kind) {
+    float P = mul(sub(z6, z4), k[0]);
+    float Q = mul(sub(z8, z2), k[1]);
+    float c = add(z5, z5);
+    float R = mul(sub(add(z4, z6), c), k[2]);
+    float T = mul(sub(add(z2, z8), c), k[3]);
+    float S = mul(sub(add(z1, z9), add(z3, z7)), k[4]);
+    float p2 = mul(P, P), q2 = mul(Q, Q);
+    float pq = mul(P, Q);
+    float pq2 = add(pq, pq);
+    if (kind == 0) {
+        float g = add(p2, q2);
+        float w = add(1.0f, g);
+        float num = add(add(mul(p2, R), mul(pq2, S)), mul(q2, T));
+        float v = sub(0.0f, div(div(num, g), mul(w, sqrt64of32(w))));
+        if (g == 0.0f) v = add(num, 0.0f);
+        return v;
+    }
+    if (kind == 1) {
+        float g = add(p2, q2);
+        float num = add(sub(mul(q2, R), mul(pq2, S)), mul(p2, T));
+        float v = sub(0.0f, div(div(num, g), sqrt64of32(g)));
+        if (g == 0.0f) v = add(num, 0.0f);
+        return v;
+    }
+    float w = add(1.0f, add(p2, q2));
+    float num = add(sub(mul(add(1.0f, q2), R), mul(pq2, S)), mul(add(1.0f, p2), T));
+    float d = mul(w, sqrt64of32(w));
+    return sub(0.0f, div(num, add(d, d)));
+}
+
+__device__ __forceinline__ double sq64(float d) {
+    double x = (double)d;
+    return __dmul_rn(x, x);
+}
+
+// RuggednessRow at radius 1 (internal/stencil/rugged.go:70-103).
+__device__ __forceinline__ float rugged3(float v1, float v2, float v3, float v4, float v5, float v6,
+                                         float v7, float v8, float v9, int kind) {
+    float c = v5;
+    if (kind == 0) {
+        double a = __dadd_rn(sq64(sub(v1, c)), sq64(sub(v2, c)));
+        a = __dadd_rn(a, sq64(sub(v3, c)));
+        a = __dadd_rn(a, sq64(sub(v4, c)));
+        a = __dadd_rn(a, sq64(sub(v6, c)));
+        a = __dadd_rn(a, sq64(sub(v7, c)));
+        a = __dadd_rn(a, sq64(sub(v8, c)));
+        a = __dadd_rn(a, sq64(sub(v9, c)));
+        return __double2float_rn(__dsqrt_rn(a));
+    }
+    if (kind == 1) {
+        float a = add(abs32(sub(v1, c)), abs32(sub(v2, c)));
+        a = add(a, abs32(sub(v3, c)));
+        a = add(a, abs32(sub(v4, c)));
+        a = add(a, abs32(sub(v6, c)));
+        a = add(a, abs32(sub(v7, c)));
+        a = add(a, abs32(sub(v8, c)));
+        a = add(a, abs32(sub(v9, c)));
+        return mul(a, 0.125f);
+    }
+    if (kind == 2) {
+        float a = add(v1, v2);
+        a = add(a, v3);
+        a = add(a, v4);
+        a = add(a, v6);
+        a = add(a, v7);
+        a = add(a, v8);
+        a = add(a, v9);
+        return sub(v5, mul(a, 0.125f));
+    }
+    float hi = go_max(go_max(go_max(go_max(v1, v2), go_max(v3, v4)), go_max(go_max(v5, v6), go_max(v7, v8))), v9);
+    float lo = go_min(go_min(go_min(go_min(v1, v2), go_min(v3, v4)), go_min(go_min(v5, v6), go_min(v7, v8))), v9);
+    return sub(hi, lo);
+}
+
+// scalarLookupFloat32 (internal/curve/scalar.go:84-114).
+__device__ __forceinline__ float lookup(float v, const float* xs, const float* ys, int n) {
+    if (v != v) return v;
+    int k = n;
+    for (int j = 0; j < n; j++) {
+        if (v < xs[j]) {
+            k = j;
+            break;
+        }
+    }
+    if (k == 0) return ys[0];
+    if (k == n) return ys[n - 1];
+    float x0 = xs[k - 1], y0 = ys[k - 1];
+    if (v == x0) return y0;
+    float t = div(sub(v, x0), sub(xs[k], x0));
+    return add(y0, mul(t, sub(ys[k], y0)));
+}
+
+// scalarReclassFloat32 (internal/curve/scalar.go:39-60).
+__device__ __forceinline__ float reclass(float v, const float* breaks, int nb, const float* values) {
+    if (v != v) return v;
+    int k = nb;
+    for (int j = 0; j < nb; j++) {
+        if (v < breaks[j]) {
+            k = j;
+            break;
+        }
+    }
+    return values[k];
+}
+
+}  // namespace cell
+}  // namespace strata

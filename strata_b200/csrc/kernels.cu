@@ -1,0 +1,426 @@
+// kernels.cu - sm_100a kernels of the raster-stencil path.
+//
+// Data kernels: one thread block computes a tile of output cells from a
+// halo tile of the input staged in shared memory; cells within the radius
+// of the raster's border get NaN (internal/exec/halo.go:61-92). Ops whose
+// reference form is separable (ColumnX then RowX,
+// internal/focalrow/focalrow.go:153-315) keep that two-pass order inside
+// the tile, so every cell folds its terms in the reference's order.
+//
+// Validity kernel: one thread owns one 32-bit word of the output mask and
+// writes only the bits of the output's own cells, the AND of the input's
+// bits over each cell's window (internal/stencil/mask.go:43-161), with
+// every other bit of the word preserved.
+#include "cellops.cuh"
+#include "launch.h"
+
+namespace strata {
+namespace {
+
+using namespace cell;
+
+constexpr int kThreadsX = 32;
+constexpr int kThreadsY = 8;
+constexpr int kThreads = kThreadsX * kThreadsY;
+constexpr int kCX = 2;
+constexpr int kCY = 4;
+constexpr int kTW = kThreadsX * kCX;  // tile width in cells
+constexpr int kTH = kThreadsY * kCY;  // tile height in cells
+
+__device__ __forceinline__ float epilogue(const LaunchParams& P, float v) {
+    for (int i = 0; i < P.nepi; i++) {
+        const EpiStage& e = P.epi[i];
+        v = e.op == STRATA_OP_LOOKUP ? lookup(v, e.a, e.b, e.n) : reclass(v, e.a, e.n, e.b);
+    }
+    return v;
+}
+
+// The 3x3 ops on a window whose centre is c, rows s floats apart.
+template <int OP>
+__device__ __forceinline__ void cell3(const LaunchParams& P, const float* c, int s, float& o0, float& o1) {
+    float z1 = c[-s - 1], z2 = c[-s], z3 = c[-s + 1];
+    float z4 = c[-1], z5 = c[0], z6 = c[1];
+    float z7 = c[s - 1], z8 = c[s], z9 = c[s + 1];
+    if constexpr (OP == STRATA_OP_CURVATURE) {
+        o0 = zt_curvature(z1, z2, z3, z4, z5, z6, z7, z8, z9, P.k, P.kind);
+    } else if constexpr (OP == STRATA_OP_RUGGEDNESS) {
+        o0 = rugged3(z1, z2, z3, z4, z5, z6, z7, z8, z9, P.kind);
+    } else {
+        float gx = mul(horn_dx(z1, z3, z4, z6, z7, z9), P.k[0]);
+        float gy = mul(horn_dy(z1, z2, z3, z7, z8, z9), P.k[1]);
+        if constexpr (OP == STRATA_OP_GRADIENT) {
+            o0 = gx;
+            o1 = gy;
+        } else if constexpr (OP == STRATA_OP_SLOPE) {
+            o0 = slope(gx, gy, P.k[2], P.kind != 0);
+        } else if constexpr (OP == STRATA_OP_ASPECT) {
+            o0 = aspect(gx, gy, P.k[2], P.kind != 0);
+        } else {
+            o0 = shade(gx, gy, P.k[2], P.k[3], P.k[4]);
+        }
+    }
+}
+
+// RuggednessWindowRow for radius R > 1 (internal/stencil/rugged.go:152-210):
+// Riley, Wilson and TPI over the window in row-major order without the
+// centre. c points at the centre cell.
+template <int R>
+__device__ __forceinline__ float rugged_window(const float* c, int s, int kind) {
+    constexpr int D = 2 * R + 1;
+    constexpr float n = (float)(D * D - 1);
+    const float z = c[0];
+    const float* q = c - R * s - R;
+    if (kind == 0) {
+        double a = 0.0;
+#pragma unroll
+        for (int j = 0; j < D; j++)
+#pragma unroll
+            for (int k = 0; k < D; k++)
+                if (!(j == R && k == R)) a = __dadd_rn(a, sq64(sub(q[j * s + k], z)));
+        return __double2float_rn(__dsqrt_rn(a));
+    }
+    if (kind == 1) {
+        float a = 0.0f;
+#pragma unroll
+        for (int j = 0; j < D; j++)
+#pragma unroll
+            for (int k = 0; k < D; k++)
+                if (!(j == R && k == R)) a = add(a, abs32(sub(q[j * s + k], z)));
+        return div(a, n);
+    }
+    float a = q[0];  // TPI folds from the first neighbour's value
+#pragma unroll
+    for (int j = 0; j < D; j++)
+#pragma unroll
+        for (int k = 0; k < D; k++)
+            if (!(j == R && k == R) && !(j == 0 && k == 0)) a = add(a, q[j * s + k]);
+    return sub(z, div(a, n));
+}
+
+// CorrelateRow (internal/focalrow/focalrow.go:217-230): the first product,
+// then every later product added in row-major order of the weights.
+template <int R>
+__device__ __forceinline__ float correlate(const LaunchParams& P, const float* c, int s) {
+    constexpr int D = 2 * R + 1;
+    const float* q = c - R * s - R;
+    float acc = mul(P.w[0], q[0]);
+#pragma unroll
+    for (int j = 0; j < D; j++)
+#pragma unroll
+        for (int k = 0; k < D; k++)
+            if (j | k) acc = add(acc, mul(P.w[j * D + k], q[j * s + k]));
+    return acc;
+}
+
+// Column folds of the separable ops (focalrow.go:232-272): the 2R+1 cells
+// of a column, top to bottom.
+template <int OP, int R>
+__device__ __forceinline__ float column_fold(const LaunchParams& P, const float* top, int s) {
+    constexpr int D = 2 * R + 1;
+    float a;
+    if constexpr (OP == STRATA_OP_SEPARABLE) {
+        a = mul(P.w[17], top[0]);
+#pragma unroll
+        for (int j = 1; j < D; j++) a = add(a, mul(P.w[17 + j], top[j * s]));
+    } else {
+        a = top[0];
+#pragma unroll
+        for (int j = 1; j < D; j++) {
+            float v = top[j * s];
+            if constexpr (OP == STRATA_OP_MEAN) a = add(a, v);
+            else if constexpr (OP == STRATA_OP_MIN) a = go_min(a, v);
+            else a = go_max(a, v);
+        }
+    }
+    return a;
+}
+
+// Row folds (focalrow.go:274-315) of 2R+1 column results, left to right;
+// the mean divides by (2R+1)^2 at the end (divRow, focalrow.go:406-421).
+template <int OP, int R>
+__device__ __forceinline__ float row_fold(const LaunchParams& P, const float* left) {
+    constexpr int D = 2 * R + 1;
+    float a;
+    if constexpr (OP == STRATA_OP_SEPARABLE) {
+        a = mul(P.w[0], left[0]);
+#pragma unroll
+        for (int c = 1; c < D; c++) a = add(a, mul(P.w[c], left[c]));
+    } else {
+        a = left[0];
+#pragma unroll
+        for (int c = 1; c < D; c++) {
+            if constexpr (OP == STRATA_OP_MEAN) a = add(a, left[c]);
+            else if constexpr (OP == STRATA_OP_MIN) a = go_min(a, left[c]);
+            else a = go_max(a, left[c]);
+        }
+        if constexpr (OP == STRATA_OP_MEAN) a = div(a, (float)(D * D));
+    }
+    return a;
+}
+
+template <int OP, int R>
+constexpr bool kTwoPass = OP == STRATA_OP_SEPARABLE || OP == STRATA_OP_MEAN || OP == STRATA_OP_MIN ||
+                          OP == STRATA_OP_MAX;
+
+// The general tile kernel: every op at every radius, any alignment and
+// stride. Tile kTW x kTH output cells; thread (tx, ty) computes cells
+// (tx + 32 i, ty + 8 j).
+template <int OP, int R>
+__global__ void __launch_bounds__(kThreads) tile_kernel(const __grid_constant__ LaunchParams P) {
+    constexpr int SW = kTW + 2 * R;
+    constexpr int SH = kTH + 2 * R;
+    constexpr int SP = SW | 1;  // odd pitch: column walks stay conflict-free
+    constexpr bool two_pass = kTwoPass<OP, R> || (OP == STRATA_OP_RUGGEDNESS && R > 1);
+    __shared__ float tile[SH * SP];
+    __shared__ float colr[two_pass ? kTH * SP : 1];
+    __shared__ float colr2[(OP == STRATA_OP_RUGGEDNESS && R > 1) ? kTH * SP : 1];
+
+    const int tid = threadIdx.y * kThreadsX + threadIdx.x;
+    const int64_t W = P.width, H = P.height;
+    for (int64_t t = blockIdx.x; t < P.tiles; t += gridDim.x) {
+        const int64_t x0 = P.out_x0 + (t % P.tiles_x) * kTW;
+        const int64_t y0 = P.out_y0 + (t / P.tiles_x) * kTH;
+        __syncthreads();
+        for (int i = tid; i < SW * SH; i += kThreads) {
+            const int sy = i / SW, sx = i - sy * SW;
+            const int64_t bx = x0 - R + sx - P.src_x0, by = y0 - R + sy - P.src_y0;
+            float v = 0.0f;
+            if (bx >= 0 && bx < P.src_w && by >= 0 && by < P.src_h) v = P.src[by * P.src_stride + bx];
+            tile[sy * SP + sx] = v;
+        }
+        __syncthreads();
+        if constexpr (two_pass) {
+            // Column pass over the tile's output rows and every column.
+            for (int i = tid; i < kTH * SW; i += kThreads) {
+                const int oy = i / SW, sx = i - oy * SW;
+                const float* top = &tile[oy * SP + sx];
+                if constexpr (OP == STRATA_OP_RUGGEDNESS) {
+                    colr[oy * SP + sx] = column_fold<STRATA_OP_MAX, R>(P, top, SP);
+                    colr2[oy * SP + sx] = column_fold<STRATA_OP_MIN, R>(P, top, SP);
+                } else {
+                    colr[oy * SP + sx] = column_fold<OP, R>(P, top, SP);
+                }
+            }
+            __syncthreads();
+        }
+#pragma unroll
+        for (int j = 0; j < kCY; j++) {
+#pragma unroll
+            for (int i = 0; i < kCX; i++) {
+                const int ox = threadIdx.x + kThreadsX * i;
+                const int oy = threadIdx.y + kThreadsY * j;
+                const int64_t gx = x0 + ox, gy = y0 + oy;
+                if (gx >= P.out_x1 || gy >= P.out_y1) continue;
+                const bool interior = gx >= R && gx < W - R && gy >= R && gy < H - R;
+                float o0 = nanf32(), o1 = nanf32();
+                if (interior) {
+                    const float* c = &tile[(oy + R) * SP + ox + R];
+                    if constexpr (OP == STRATA_OP_RUGGEDNESS && R > 1) {
+                        if (P.kind == STRATA_RUG_ROUGHNESS) {
+                            const float hi = row_fold<STRATA_OP_MAX, R>(P, &colr[oy * SP + ox]);
+                            const float lo = row_fold<STRATA_OP_MIN, R>(P, &colr2[oy * SP + ox]);
+                            o0 = sub(hi, lo);
+                        } else {
+                            o0 = rugged_window<R>(c, SP, P.kind);
+                        }
+                    } else if constexpr (two_pass) {
+                        o0 = row_fold<OP, R>(P, &colr[oy * SP + ox]);
+                    } else if constexpr (OP == STRATA_OP_CORRELATE) {
+                        o0 = correlate<R>(P, c, SP);
+                    } else {
+                        cell3<OP>(P, c, SP, o0, o1);
+                    }
+                    o0 = epilogue(P, o0);
+                }
+                const int64_t dx = gx - P.dst_x0, dy = gy - P.dst_y0;
+                P.dst0[dy * P.dst0_stride + dx] = o0;
+                if constexpr (OP == STRATA_OP_GRADIENT) P.dst1[dy * P.dst1_stride + dx] = o1;
+            }
+        }
+    }
+}
+
+// Pointwise stages alone (radius 0): every cell through the epilogue.
+__global__ void __launch_bounds__(256) pointwise_kernel(const __grid_constant__ LaunchParams P) {
+    const int64_t w = P.out_x1 - P.out_x0;
+    const int64_t n = w * (P.out_y1 - P.out_y0);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t y = i / w, x = i - y * w;
+        const int64_t gx = P.out_x0 + x, gy = P.out_y0 + y;
+        const float v = P.src[(gy - P.src_y0) * P.src_stride + (gx - P.src_x0)];
+        P.dst0[(gy - P.dst_y0) * P.dst0_stride + (gx - P.dst_x0)] = epilogue(P, v);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Validity.
+
+__device__ __forceinline__ int64_t min64(int64_t a, int64_t b) { return a < b ? a : b; }
+
+__device__ __forceinline__ int64_t floor_div32(int64_t b) { return b >= 0 ? b >> 5 : -((-b + 31) >> 5); }
+
+// 64 bits of the source mask from bit b on (b may be negative), with zeros
+// for words outside [lo, hi].
+__device__ __forceinline__ uint64_t bits64(const ValidityParams& v, int64_t b) {
+    const int64_t w = floor_div32(b);
+    const int sh = (int)(b - w * 32);
+    const uint32_t* m = v.src_bits;
+    const uint64_t a0 = (w >= v.src_lo_word && w <= v.src_hi_word) ? m[w] : 0u;
+    const uint64_t a1 = (w + 1 >= v.src_lo_word && w + 1 <= v.src_hi_word) ? m[w + 1] : 0u;
+    const uint64_t a2 = (w + 2 >= v.src_lo_word && w + 2 <= v.src_hi_word) ? m[w + 2] : 0u;
+    uint64_t lo = a0 | (a1 << 32);
+    if (sh == 0) return lo;
+    return (lo >> sh) | (a2 << (64 - sh));
+}
+
+// Output bits of global cells (x .. x+31, y), bit j for cell x + j.
+__device__ __forceinline__ uint32_t segment_bits(const ValidityParams& v, int64_t x, int64_t y) {
+    const int r = v.radius;
+    const int64_t W = v.width, H = v.height;
+    if (r > 0 && (y < r || y >= H - r)) return 0u;
+    uint32_t interior = 0xffffffffu;
+    if (r > 0) {
+        // cells x + j with r <= x + j < W - r
+        const int64_t lo = r - x, hi = W - r - x;  // j in [lo, hi)
+        for (int j = 0; j < 32; j++)
+            if (j < lo || j >= hi) interior &= ~(1u << j);
+    }
+    if (!v.src_bits) return interior;
+    uint64_t acc = ~0ull;
+    const int64_t bx = x - r - v.src_x0;
+    for (int j = -r; j <= r; j++) acc &= bits64(v, v.src_off + (y + j - v.src_y0) * v.src_stride + bx);
+    uint64_t e = acc;
+    for (int d = 1; d <= 2 * r; d++) e &= acc >> d;
+    return (uint32_t)e & interior;
+}
+
+__global__ void __launch_bounds__(256) validity_kernel(const __grid_constant__ ValidityParams v) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= v.dst_words) return;
+    const int64_t wi = v.dst_lo_word + i;
+    const int64_t pos = wi * 32 - v.dst_off;  // destination cell index of the word's bit 0
+    uint32_t bits = 0u, ours = 0u;
+    int k = 0;
+    while (k < 32) {
+        const int64_t c = pos + k;
+        if (c < 0) {
+            k = (int)min64(32, (int64_t)k - c);
+            continue;
+        }
+        const int64_t ly = c / v.dst_stride, lx = c - ly * v.dst_stride;
+        const int64_t y = ly + v.dst_y0, x = lx + v.dst_x0;  // global cell
+        if (y >= v.out_y1) break;
+        if (y < v.out_y0 || x >= v.out_x1) {
+            // Past the region in this row: on to the next row's start.
+            k = (int)min64(32, (int64_t)k + (v.dst_stride - lx));
+            continue;
+        }
+        if (x < v.out_x0) {
+            k = (int)min64(32, (int64_t)k + (v.out_x0 - x));
+            continue;
+        }
+        const int len = (int)min64(32 - k, v.out_x1 - x);
+        const uint32_t m = len == 32 ? 0xffffffffu : ((1u << len) - 1u);
+        const uint32_t seg = segment_bits(v, x, y) & m;
+        bits |= seg << k;
+        ours |= m << k;
+        k += len;
+    }
+    if (ours == 0u) return;
+    const uint32_t old = v.dst_bits[wi];
+    v.dst_bits[wi] = (old & ~ours) | bits;
+}
+
+template <int OP, int R>
+int64_t launch_tiles(const LaunchParams& p0, cudaStream_t s) {
+    LaunchParams p = p0;
+    p.tiles_x = (p.out_x1 - p.out_x0 + kTW - 1) / kTW;
+    p.tiles = p.tiles_x * ((p.out_y1 - p.out_y0 + kTH - 1) / kTH);
+    const int64_t grid = p.tiles < (int64_t)1 << 30 ? p.tiles : (int64_t)1 << 30;
+    tile_kernel<OP, R><<<(unsigned)grid, dim3(kThreadsX, kThreadsY), 0, s>>>(p);
+    return p.tiles;
+}
+
+using Launcher = int64_t (*)(const LaunchParams&, cudaStream_t);
+
+template <int OP>
+Launcher pick_radius(int r) {
+    switch (r) {
+    case 1: return launch_tiles<OP, 1>;
+    case 2: return launch_tiles<OP, 2>;
+    case 3: return launch_tiles<OP, 3>;
+    case 4: return launch_tiles<OP, 4>;
+    case 5: return launch_tiles<OP, 5>;
+    case 6: return launch_tiles<OP, 6>;
+    case 7: return launch_tiles<OP, 7>;
+    case 8: return launch_tiles<OP, 8>;
+    }
+    return nullptr;
+}
+
+}  // namespace
+
+void tile_shape(int op, int radius, int64_t width, int* tw, int* th) {
+    (void)op;
+    (void)radius;
+    (void)width;
+    *tw = kTW;
+    *th = kTH;
+}
+
+int64_t launch_data(const LaunchParams& p, cudaStream_t s, int64_t* window_cells) {
+    Launcher L = nullptr;
+    switch (p.op) {
+    case STRATA_OP_GRADIENT: L = launch_tiles<STRATA_OP_GRADIENT, 1>; break;
+    case STRATA_OP_SLOPE: L = launch_tiles<STRATA_OP_SLOPE, 1>; break;
+    case STRATA_OP_ASPECT: L = launch_tiles<STRATA_OP_ASPECT, 1>; break;
+    case STRATA_OP_HILLSHADE: L = launch_tiles<STRATA_OP_HILLSHADE, 1>; break;
+    case STRATA_OP_CURVATURE: L = launch_tiles<STRATA_OP_CURVATURE, 1>; break;
+    case STRATA_OP_RUGGEDNESS: L = pick_radius<STRATA_OP_RUGGEDNESS>(p.radius); break;
+    case STRATA_OP_CORRELATE: L = pick_radius<STRATA_OP_CORRELATE>(p.radius); break;
+    case STRATA_OP_SEPARABLE: L = pick_radius<STRATA_OP_SEPARABLE>(p.radius); break;
+    case STRATA_OP_MEAN: L = pick_radius<STRATA_OP_MEAN>(p.radius); break;
+    case STRATA_OP_MIN: L = pick_radius<STRATA_OP_MIN>(p.radius); break;
+    case STRATA_OP_MAX: L = pick_radius<STRATA_OP_MAX>(p.radius); break;
+    case STRATA_OP_LOOKUP:
+    case STRATA_OP_RECLASS: {
+        const int64_t n = (p.out_x1 - p.out_x0) * (p.out_y1 - p.out_y0);
+        int64_t blocks = (n + 255) / 256;
+        if (blocks > 148 * 64) blocks = 148 * 64;
+        if (blocks < 1) blocks = 1;
+        pointwise_kernel<<<(unsigned)blocks, 256, 0, s>>>(p);
+        if (window_cells) *window_cells = n;
+        return blocks;
+    }
+    }
+    if (!L) return -1;
+    if (p.out_x1 <= p.out_x0 || p.out_y1 <= p.out_y0) {
+        if (window_cells) *window_cells = 0;
+        return 0;
+    }
+    const int64_t tiles = L(p, s);
+    if (window_cells) {
+        // Each tile reads its cells grown by the radius, clipped to the raster.
+        const int r = p.radius;
+        const int64_t tx = (p.out_x1 - p.out_x0 + kTW - 1) / kTW, ty = (p.out_y1 - p.out_y0 + kTH - 1) / kTH;
+        int64_t wx = 0, wy = 0;
+        for (int64_t i = 0; i < tx; i++) {
+            const int64_t a = p.out_x0 + i * kTW - r, b = p.out_x0 + (i + 1) * kTW + r;
+            wx += (b < p.width ? b : p.width) - (a > 0 ? a : 0);
+        }
+        for (int64_t i = 0; i < ty; i++) {
+            const int64_t a = p.out_y0 + i * kTH - r, b = p.out_y0 + (i + 1) * kTH + r;
+            wy += (b < p.height ? b : p.height) - (a > 0 ? a : 0);
+        }
+        *window_cells = wx * wy;
+    }
+    return tiles;
+}
+
+void launch_validity(const ValidityParams& v, cudaStream_t s) {
+    if (v.dst_words <= 0) return;
+    const int64_t blocks = (v.dst_words + 255) / 256;
+    validity_kernel<<<(unsigned)blocks, 256, 0, s>>>(v);
+}
+
+}  // namespace strata

@@ -1,0 +1,91 @@
+// launch.h - what the host driver (api.cu) hands the kernels (kernels.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "../../include/strata_cuda.h"
+
+namespace strata {
+
+constexpr int kMaxEpilogue = 4;  // pointwise stages fused after a stencil
+constexpr int kMaxWeights = (2 * STRATA_MAX_RADIUS + 1) * (2 * STRATA_MAX_RADIUS + 1);
+
+// One pointwise stage fused as an epilogue: LOOKUP (a = xs, b = ys, n
+// knots) or RECLASS (a = breaks, n breaks, b = values, n + 1 of them).
+struct EpiStage {
+    int op;
+    int n;
+    float a[STRATA_MAX_KNOTS];
+    float b[STRATA_MAX_KNOTS + 1];
+};
+
+// Kernel parameters of one stage launch. Passed by value as a
+// __grid_constant__ parameter, so weights and tables sit in the constant
+// bank and every thread reads them through the broadcast path.
+//
+// Coordinates are the whole raster's: width x height decides the edge
+// ring. src holds the cells [src_x0, src_x0 + src_w) x [src_y0, src_y0 +
+// src_h) and dst0 / dst1 start at cell (dst_x0, dst_y0); the launch writes
+// the output region [out_x0, out_x1) x [out_y0, out_y1). A plain call has
+// every offset 0 and the region the whole raster; a chunked tile or a row
+// strip sets them.
+struct LaunchParams {
+    const float* src;
+    int64_t src_stride;
+    int64_t src_x0, src_y0, src_w, src_h;
+    float* dst0;
+    int64_t dst0_stride;
+    float* dst1;
+    int64_t dst1_stride;
+    int64_t dst_x0, dst_y0;
+    int64_t out_x0, out_y0, out_x1, out_y1;
+    int64_t width, height;
+    int64_t tiles_x;  // thread-block tiles across the region (set by the launcher)
+    int64_t tiles;    // thread-block tiles in the launch (set by the launcher)
+    int op;
+    int radius;
+    int kind;
+    int nepi;
+    float k[16];
+    float w[kMaxWeights];  // CORRELATE weights (rotation applied); SEPARABLE row taps w[0..], column taps w[17..]
+    EpiStage epi[kMaxEpilogue];
+};
+
+// Validity of one output: bits of dst for the width x height raster,
+// derived from src's bits (src_valid may be null: every input cell valid)
+// by erosion over the radius, with the edge ring cleared; radius 0 copies.
+// Coordinates as in LaunchParams: the source mask's cell (0, 0) is global
+// cell (src_x0, src_y0), the destination's is (dst_x0, dst_y0), and only
+// bits of cells in the region [out_x0, out_x1) x [out_y0, out_y1) change.
+struct ValidityParams {
+    const uint32_t* src_bits;  // the source mask as 32-bit words
+    int64_t src_off;           // bit offset of the source's cell (0, 0)
+    int64_t src_stride;
+    int64_t src_x0, src_y0;
+    int64_t src_lo_word, src_hi_word;  // 32-bit words [lo, hi] that hold the source's bits
+    uint32_t* dst_bits;
+    int64_t dst_off;
+    int64_t dst_stride;
+    int64_t dst_x0, dst_y0;
+    int64_t dst_lo_word;  // first 32-bit word holding a destination bit of the region
+    int64_t dst_words;    // 32-bit words from dst_lo_word
+    int64_t out_x0, out_y0, out_x1, out_y1;
+    int64_t width, height;
+    int radius;
+};
+
+// Launches the data kernel of stages (the first any op, the rest pointwise
+// epilogues) over whole rasters. Returns the number of thread-block tiles
+// launched, or -1 if the op / radius has no kernel; *window_cells gets the
+// input cells the tiles read (halo included, clipped to the raster).
+int64_t launch_data(const LaunchParams& p, cudaStream_t stream, int64_t* window_cells);
+
+// Launches the validity kernel for one output.
+void launch_validity(const ValidityParams& v, cudaStream_t stream);
+
+// Tile geometry of the data kernels, for Stats.
+void tile_shape(int op, int radius, int64_t width, int* tw, int* th);
+
+}  // namespace strata

@@ -1,0 +1,194 @@
+"""terrain: Horn gradient, slope, aspect and hillshade, Zevenbergen-Thorne
+curvature and ruggedness on the device backend, with the reference's entry
+points (terrain/gradient.go, slope.go, aspect.go, hillshade.go,
+curvature.go, ruggedness.go): the plain function, its Tiled form (with a
+Context and engine Options) and its Chunked form (sources and sinks).
+
+Option resolution and its checks run in libstrata_cuda's stage builders
+(strata_stage_*), which follow the reference's option code; a programming
+error raises StrataPanic with the reference's message.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+from . import _lib
+from .engine import Background, Context, Options, StageList, process, process_chunked
+from .raster import Float32Raster
+
+SlopeDegrees, SlopePercent, SlopeRadians = 0, 1, 2
+CurvatureProfile, CurvaturePlan, CurvatureMean = 0, 1, 2
+RuggednessTRI, RuggednessTRIWilson, RuggednessTPI, RuggednessRoughness = 0, 1, 2, 3
+AspectFlat = -1
+MaxRadius = 8
+
+
+@dataclass
+class GradientOptions:
+    CellSize: float = 0.0
+    CellSizeY: float = 0.0
+    ZFactor: float = 0.0
+    FitRadius: int = 0
+
+
+@dataclass
+class SlopeOptions:
+    CellSize: float = 0.0
+    CellSizeY: float = 0.0
+    ZFactor: float = 0.0
+    FitRadius: int = 0
+    Units: int = SlopeDegrees
+
+
+@dataclass
+class AspectOptions:
+    CellSize: float = 0.0
+    CellSizeY: float = 0.0
+    ZFactor: float = 0.0
+    FitRadius: int = 0
+    ZeroForFlat: bool = False
+    Trigonometric: bool = False
+
+
+@dataclass
+class HillshadeOptions:
+    CellSize: float = 0.0
+    CellSizeY: float = 0.0
+    ZFactor: float = 0.0
+    FitRadius: int = 0
+    Azimuth: float = 0.0
+    Altitude: float = 0.0
+
+
+@dataclass
+class CurvatureOptions:
+    CellSize: float = 0.0
+    CellSizeY: float = 0.0
+    ZFactor: float = 0.0
+    FitRadius: int = 0
+    Type: int = CurvatureProfile
+
+
+@dataclass
+class RuggednessOptions:
+    Type: int = RuggednessTRI
+    Radius: int = 0
+
+
+def _one(fn, copts) -> StageList:
+    st = _lib.Stage()
+    _lib.check(fn(ctypes.byref(copts), ctypes.byref(st)))
+    return StageList().add(st)
+
+
+def gradient_stage(o: GradientOptions) -> StageList:
+    return _one(_lib.lib().strata_stage_gradient,
+                _lib.GradientOptions(o.CellSize, o.CellSizeY, o.ZFactor, o.FitRadius, 0))
+
+
+def slope_stage(o: SlopeOptions) -> StageList:
+    return _one(_lib.lib().strata_stage_slope,
+                _lib.SlopeOptions(o.CellSize, o.CellSizeY, o.ZFactor, o.FitRadius, o.Units))
+
+
+def aspect_stage(o: AspectOptions) -> StageList:
+    return _one(_lib.lib().strata_stage_aspect,
+                _lib.AspectOptions(o.CellSize, o.CellSizeY, o.ZFactor, o.FitRadius, int(bool(o.ZeroForFlat)),
+                                   int(bool(o.Trigonometric)), 0))
+
+
+def hillshade_stage(o: HillshadeOptions) -> StageList:
+    return _one(_lib.lib().strata_stage_hillshade,
+                _lib.HillshadeOptions(o.CellSize, o.CellSizeY, o.ZFactor, o.FitRadius, 0, o.Azimuth, o.Altitude))
+
+
+def curvature_stage(o: CurvatureOptions) -> StageList:
+    return _one(_lib.lib().strata_stage_curvature,
+                _lib.CurvatureOptions(o.CellSize, o.CellSizeY, o.ZFactor, o.FitRadius, o.Type))
+
+
+def ruggedness_stage(o: RuggednessOptions) -> StageList:
+    return _one(_lib.lib().strata_stage_ruggedness, _lib.RuggednessOptions(o.Type, o.Radius))
+
+
+def _plain(stages, dem, *outs):
+    process(stages, list(outs), [dem], Options(Workers=1), Background())
+
+
+# Gradient (terrain/gradient.go)
+def Gradient(dx: Float32Raster, dy: Float32Raster, dem: Float32Raster, opts: GradientOptions) -> None:
+    _plain(gradient_stage(opts), dem, dx, dy)
+
+
+def GradientTiled(ctx: Context, dx, dy, dem, opts: GradientOptions, eopts: Options):
+    return process(gradient_stage(opts), [dx, dy], [dem], eopts, ctx)
+
+
+def GradientChunked(ctx: Context, dx, dy, dem, opts: GradientOptions, eopts: Options):
+    return process_chunked(gradient_stage(opts), [dx, dy], [dem], eopts, ctx)
+
+
+# Slope (terrain/slope.go)
+def Slope(dst: Float32Raster, dem: Float32Raster, opts: SlopeOptions) -> None:
+    _plain(slope_stage(opts), dem, dst)
+
+
+def SlopeTiled(ctx: Context, dst, dem, opts: SlopeOptions, eopts: Options):
+    return process(slope_stage(opts), [dst], [dem], eopts, ctx)
+
+
+def SlopeChunked(ctx: Context, dst, dem, opts: SlopeOptions, eopts: Options):
+    return process_chunked(slope_stage(opts), [dst], [dem], eopts, ctx)
+
+
+# Aspect (terrain/aspect.go)
+def Aspect(dst: Float32Raster, dem: Float32Raster, opts: AspectOptions) -> None:
+    _plain(aspect_stage(opts), dem, dst)
+
+
+def AspectTiled(ctx: Context, dst, dem, opts: AspectOptions, eopts: Options):
+    return process(aspect_stage(opts), [dst], [dem], eopts, ctx)
+
+
+def AspectChunked(ctx: Context, dst, dem, opts: AspectOptions, eopts: Options):
+    return process_chunked(aspect_stage(opts), [dst], [dem], eopts, ctx)
+
+
+# Hillshade (terrain/hillshade.go)
+def Hillshade(dst: Float32Raster, dem: Float32Raster, opts: HillshadeOptions) -> None:
+    _plain(hillshade_stage(opts), dem, dst)
+
+
+def HillshadeTiled(ctx: Context, dst, dem, opts: HillshadeOptions, eopts: Options):
+    return process(hillshade_stage(opts), [dst], [dem], eopts, ctx)
+
+
+def HillshadeChunked(ctx: Context, dst, dem, opts: HillshadeOptions, eopts: Options):
+    return process_chunked(hillshade_stage(opts), [dst], [dem], eopts, ctx)
+
+
+# Curvature (terrain/curvature.go)
+def Curvature(dst: Float32Raster, dem: Float32Raster, opts: CurvatureOptions) -> None:
+    _plain(curvature_stage(opts), dem, dst)
+
+
+def CurvatureTiled(ctx: Context, dst, dem, opts: CurvatureOptions, eopts: Options):
+    return process(curvature_stage(opts), [dst], [dem], eopts, ctx)
+
+
+def CurvatureChunked(ctx: Context, dst, dem, opts: CurvatureOptions, eopts: Options):
+    return process_chunked(curvature_stage(opts), [dst], [dem], eopts, ctx)
+
+
+# Ruggedness (terrain/ruggedness.go)
+def Ruggedness(dst: Float32Raster, dem: Float32Raster, opts: RuggednessOptions) -> None:
+    _plain(ruggedness_stage(opts), dem, dst)
+
+
+def RuggednessTiled(ctx: Context, dst, dem, opts: RuggednessOptions, eopts: Options):
+    return process(ruggedness_stage(opts), [dst], [dem], eopts, ctx)
+
+
+def RuggednessChunked(ctx: Context, dst, dem, opts: RuggednessOptions, eopts: Options):
+    return process_chunked(ruggedness_stage(opts), [dst], [dem], eopts, ctx)

@@ -1,0 +1,199 @@
+"""The C ABI without a GPU: libstrata_cuda loads and exports every entry
+point include/strata_cuda.h declares, its structs have the header's layout,
+its op codes match the oracle's, and the stage builders resolve options to
+the reference's constants and reject what the reference panics on, with
+its messages."""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+import re
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+from oracle import oracle as orc
+from strata_b200 import _lib, focal, terrain, transfer
+from strata_b200.raster import NotSupported, StrataPanic
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "strata_cuda.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"^[A-Za-z_][\w \*]*?\b(strata_\w+)\s*\(", text, flags=re.M)))
+
+
+def test_library_exports_every_declared_symbol():
+    names = declared_functions()
+    assert len(names) >= 20
+    L = _lib.lib()
+    for n in names:
+        assert hasattr(L, n), f"libstrata_cuda.so does not export {n}"
+    # and the binding covers each one
+    bound = {s[0] for s in _lib.SIGNATURES}
+    assert set(names) <= bound, set(names) - bound
+
+
+def test_abi_version():
+    assert _lib.lib().strata_abi_version() == 1
+
+
+def test_op_codes_match_oracle_and_header():
+    text = open(HEADER).read()
+    for name, val in re.findall(r"STRATA_OP_(\w+) = (\d+)", text):
+        assert getattr(orc, name) == int(val), name
+        assert getattr(_lib, "OP_" + name) == int(val), name
+
+
+def test_struct_layouts_match_header(tmp_path):
+    """Compiles a C program against the header and compares sizeof and
+    offsetof with the ctypes mirrors."""
+    structs = {
+        "strata_raster": _lib.Raster, "strata_stage": _lib.Stage, "strata_exec_opts": _lib.ExecOpts,
+        "strata_stats": _lib.Stats, "strata_source": _lib.Source, "strata_sink": _lib.Sink,
+        "strata_slope_options": _lib.SlopeOptions, "strata_aspect_options": _lib.AspectOptions,
+        "strata_hillshade_options": _lib.HillshadeOptions, "strata_curvature_options": _lib.CurvatureOptions,
+        "strata_gradient_options": _lib.GradientOptions, "strata_ruggedness_options": _lib.RuggednessOptions,
+        "strata_weights_options": _lib.WeightsOptions, "strata_separable_options": _lib.SeparableOptions,
+        "strata_box_options": _lib.BoxOptions,
+    }
+    lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void){"]
+    for cname, ct in structs.items():
+        lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
+        for fname, _ in ct._fields_:
+            lines.append(f'printf("{cname}.{fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines.append("return 0;}")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-o", str(exe), str(src)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = dict(line.split(" ") for line in out if line)
+    for cname, ct in structs.items():
+        assert int(got[cname]) == ctypes.sizeof(ct), cname
+        for fname, _ in ct._fields_:
+            assert int(got[f"{cname}.{fname}"]) == getattr(ct, fname).offset, f"{cname}.{fname}"
+
+
+# ---------------------------------------------------------------------------
+# Stage builders: the reference's option resolution.
+
+def k_of(sl):
+    return [np.float32(v) for v in sl.stages[0].k]
+
+
+@pytest.mark.parametrize("cs,csy,z", [(30, 0, 0), (5, 0, 1), (10, 12.5, -2), (0.25, 0.5, 3.5), (1e-3, 7, 0)])
+def test_horn_scales(cs, csy, z):
+    st = terrain.slope_stage(terrain.SlopeOptions(CellSize=cs, CellSizeY=csy, ZFactor=z))
+    kx, ky = orc.horn_scales(cs, csy or cs, z or 1.0)
+    got = k_of(st)
+    assert got[0] == kx and got[1] == ky
+    assert got[2] == np.float32(180 / math.pi) and st.stages[0].kind == 1
+
+
+def test_slope_units():
+    for units, scale, atan in ((terrain.SlopeDegrees, np.float32(180 / math.pi), 1),
+                               (terrain.SlopePercent, np.float32(100), 0), (terrain.SlopeRadians, np.float32(1), 1)):
+        st = terrain.slope_stage(terrain.SlopeOptions(CellSize=1, Units=units))
+        assert k_of(st)[2] == scale and st.stages[0].kind == atan
+
+
+@pytest.mark.parametrize("az,alt", [(0, 0), (315, 45), (90, 0), (-45, 30), (725, 89.5), (180, 90)])
+def test_hillshade_light(az, alt):
+    st = terrain.hillshade_stage(terrain.HillshadeOptions(CellSize=1, Azimuth=az, Altitude=alt))
+    assert k_of(st)[2:5] == orc.hillshade_light(az, alt)
+
+
+def test_aspect_flat_and_trig():
+    st = terrain.aspect_stage(terrain.AspectOptions(CellSize=1))
+    assert k_of(st)[2] == -1 and st.stages[0].kind == 0
+    st = terrain.aspect_stage(terrain.AspectOptions(CellSize=1, ZeroForFlat=True, Trigonometric=True))
+    assert k_of(st)[2] == 0 and st.stages[0].kind == 1
+
+
+@pytest.mark.parametrize("cs,csy,z", [(1, 0, 0), (3, 0.5, -2), (30, 0, 1), (2, 4, 1)])
+def test_zt_scales(cs, csy, z):
+    st = terrain.curvature_stage(terrain.CurvatureOptions(CellSize=cs, CellSizeY=csy, ZFactor=z, Type=2))
+    assert k_of(st)[:5] == orc.zt_scales(cs, csy or cs, z or 1.0)
+    assert st.stages[0].kind == 2
+
+
+@pytest.mark.parametrize("r,sigma", [(1, 0.5), (3, 1.0), (8, 2.5), (5, 10.0)])
+def test_gaussian_taps(r, sigma):
+    assert (focal.Gaussian(r, sigma).view(np.uint32) == orc.gaussian(r, sigma).view(np.uint32)).all()
+
+
+def test_ruggedness_radius_default():
+    st = terrain.ruggedness_stage(terrain.RuggednessOptions(Type=terrain.RuggednessTPI))
+    assert st.stages[0].radius == 1 and st.stages[0].kind == 2
+
+
+@pytest.mark.parametrize("make,msg", [
+    (lambda: terrain.slope_stage(terrain.SlopeOptions()), "terrain: CellSize must be positive and finite, got 0"),
+    (lambda: terrain.slope_stage(terrain.SlopeOptions(CellSize=float("inf"))),
+     "terrain: CellSize must be positive and finite, got +Inf"),
+    (lambda: terrain.slope_stage(terrain.SlopeOptions(CellSize=1, CellSizeY=-2)),
+     "terrain: CellSizeY must be positive and finite (or 0 for CellSize), got -2"),
+    (lambda: terrain.slope_stage(terrain.SlopeOptions(CellSize=1, ZFactor=float("nan"))),
+     "terrain: ZFactor must be finite, got NaN"),
+    (lambda: terrain.slope_stage(terrain.SlopeOptions(CellSize=1, Units=7)), "terrain: unknown SlopeUnits 7"),
+    (lambda: terrain.slope_stage(terrain.SlopeOptions(CellSize=1e-300)),
+     "terrain: ZFactor/(8·CellSize) and ZFactor/(8·CellSizeY) must be finite and non-zero as float32, got +Inf"),
+    (lambda: terrain.hillshade_stage(terrain.HillshadeOptions(CellSize=1, Altitude=91)),
+     "terrain: Altitude must be in (0, 90] (or 0 for 45), got 91"),
+    (lambda: terrain.hillshade_stage(terrain.HillshadeOptions(CellSize=1, Azimuth=float("inf"))),
+     "terrain: Azimuth must be finite, got +Inf"),
+    (lambda: terrain.curvature_stage(terrain.CurvatureOptions(CellSize=1, Type=3)),
+     "terrain: unknown CurvatureType 3"),
+    (lambda: terrain.ruggedness_stage(terrain.RuggednessOptions(Radius=9)),
+     "terrain: RuggednessOptions.Radius must be 0 to 8, got 9"),
+    (lambda: terrain.ruggedness_stage(terrain.RuggednessOptions(Type=4)), "terrain: unknown RuggednessType 4"),
+    (lambda: terrain.slope_stage(terrain.SlopeOptions(CellSize=1, FitRadius=9)),
+     "terrain: FitRadius must be 0 to 8, got 9"),
+    (lambda: focal.weights_stage(focal.WeightsOptions(Radius=0, Weights=[1]), False),
+     "focal: Radius must be 1 to 8, got 0"),
+    (lambda: focal.weights_stage(focal.WeightsOptions(Radius=1, Weights=[1] * 8), False),
+     "focal: Radius 1 needs 3×3 = 9 Weights, got 8"),
+    (lambda: focal.weights_stage(focal.WeightsOptions(Radius=1, Weights=[1] * 8 + [float("nan")]), False),
+     "focal: Weights must be finite, got NaN at index 8"),
+    (lambda: focal.separable_stage(focal.SeparableOptions(Radius=2, Row=[1] * 5, Col=[1] * 4)),
+     "focal: Radius 2 needs 5 Row and 5 Col taps, got 5 and 4"),
+    (lambda: focal.Gaussian(2, 0), "focal: Gaussian sigma must be positive and finite, got 0"),
+    (lambda: transfer.lookup_stage([], []), "transfer.Lookup: the table needs at least one knot"),
+    (lambda: transfer.lookup_stage([0, 0], [1, 2]),
+     "transfer.Lookup: xs must be strictly increasing, but xs[1] = 0 is not above xs[0] = 0"),
+    (lambda: transfer.lookup_stage([0, float("inf")], [1, 2]), "transfer.Lookup: xs must be finite, but xs[1] = +Inf"),
+    (lambda: transfer.reclass_stage([1, 2], [1, 2]),
+     "transfer.Reclass: values must hold one more element than breaks, got 2 values and 2 breaks"),
+    (lambda: transfer.reclass_stage([1, float("nan")], [1, 2, 3]),
+     "transfer.Reclass: breaks must not hold NaN, but breaks[1] is NaN"),
+])
+def test_builders_panic_like_the_reference(make, msg):
+    with pytest.raises(StrataPanic) as e:
+        make()
+    assert str(e.value).startswith(msg), str(e.value)
+
+
+def test_fit_radius_is_not_on_the_device():
+    with pytest.raises(NotSupported):
+        terrain.slope_stage(terrain.SlopeOptions(CellSize=1, FitRadius=2))
+
+
+def test_context_without_a_device_fails_cleanly():
+    try:
+        import torch
+
+        if torch.cuda.is_available():
+            pytest.skip("a device is present")
+    except ImportError:
+        pass
+    p = ctypes.c_void_p()
+    rc = _lib.lib().strata_ctx_create(0, ctypes.byref(p))
+    assert rc in (_lib.ECUDA, _lib.EINVAL)
+    assert _lib.last_error()

@@ -1,0 +1,271 @@
+"""Device parity: every op of the path through libstrata_cuda against the
+oracle on the same seeded inputs, cell for cell (rastertest.SameFloat:
+same bits, or both NaN) and bit for bit in the validity masks, over the
+shapes, layouts and masks of the reference's engine matrix
+(internal/exec/workers_test.go:29-80): tiny and odd shapes, strided
+windows with bit offsets, unmasked / masked inputs and masked outputs of
+unmasked inputs, host-memory and device-resident operands."""
+from __future__ import annotations
+
+import itertools
+
+import numpy as np
+import pytest
+
+from helpers import (assert_padding_untouched, assert_same_raster, host_raster, like, poison, run_oracle,
+                     to_device, to_host)
+from strata_b200 import engine, focal, synth, terrain, transfer
+from strata_b200.raster import Float32Raster
+
+pytestmark = pytest.mark.gpu
+
+SHAPES = [(1, 1), (2, 5), (3, 3), (17, 5), (61, 37), (300, 9), (129, 67), (257, 131)]
+SMALL_SHAPES = [(3, 3), (19, 23), (61, 37), (129, 40)]
+
+
+def dem_cells(w, h, seed):
+    return poison(synth.fbm_dem(w, h, seed, lo=0, hi=3000), seed, 0.003)
+
+
+def focal_cells(w, h, seed):
+    return poison(synth.normal_trend(w, h, seed), seed, 0.003)
+
+
+def layouts(w, h, seed, masked):
+    """(src, dst) pairs: compact; strided with bit offsets; masked output
+    of an unmasked input."""
+    out = []
+    valid = synth.cell_mask(w, h, seed, 0.03) if masked else None
+    yield dict(src=dict(stride=None, offset=0, valid=valid), dst=dict(stride=None, offset=0, masked=masked))
+    yield dict(src=dict(stride=w + 13, offset=37, valid=valid), dst=dict(stride=w + 5, offset=11, masked=masked))
+    if not masked:
+        yield dict(src=dict(stride=w + 1, offset=0, valid=None), dst=dict(stride=None, offset=63, masked=True))
+
+
+def check_case(stages, cells, nout=1, device=False, lay=None, what=""):
+    h, w = cells.shape
+    src = host_raster(cells, lay["src"]["valid"], lay["src"]["stride"], lay["src"]["offset"])
+    want = [like(src, lay["dst"]["stride"], lay["dst"]["offset"], masked=lay["dst"]["masked"]) for _ in range(nout)]
+    got = [like(src, lay["dst"]["stride"], lay["dst"]["offset"], masked=lay["dst"]["masked"]) for _ in range(nout)]
+    before = [Float32Raster(np.array(g.data), g.width, g.height, g.stride,
+                            None if g.valid is None else np.array(g.valid), g.valid_offset) for g in got]
+    run_oracle(stages, src, want)
+    if device:
+        dsrc = to_device(src)
+        dgot = [to_device(g) for g in got]
+        assert engine.process(stages, dgot, [dsrc]) is None
+        got = [to_host(g) for g in dgot]
+    else:
+        assert engine.process(stages, got, [src]) is None
+    for i in range(nout):
+        assert_same_raster(got[i], want[i], f"{what} out{i}")
+        assert_padding_untouched(before[i], got[i], f"{what} out{i}")
+
+
+def run_matrix(make_stages, cells_fn, nout=1, shapes=SHAPES, seed=1):
+    for (w, h), masked, device in itertools.product(shapes, (False, True), (False, True)):
+        cells = cells_fn(w, h, seed + w * 7 + h)
+        for li, lay in enumerate(layouts(w, h, seed + w + h, masked)):
+            check_case(make_stages(), cells, nout, device, lay,
+                       f"{w}x{h} masked={masked} device={device} layout={li}")
+
+
+TERRAIN = {
+    "slope_deg": lambda: terrain.slope_stage(terrain.SlopeOptions(CellSize=30)),
+    "slope_pct": lambda: terrain.slope_stage(terrain.SlopeOptions(CellSize=10, Units=terrain.SlopePercent)),
+    "slope_rad_aniso": lambda: terrain.slope_stage(terrain.SlopeOptions(CellSize=3, CellSizeY=7, ZFactor=2,
+                                                                        Units=terrain.SlopeRadians)),
+    "aspect": lambda: terrain.aspect_stage(terrain.AspectOptions(CellSize=30)),
+    "aspect_trig_zero": lambda: terrain.aspect_stage(terrain.AspectOptions(CellSize=5, ZeroForFlat=True,
+                                                                           Trigonometric=True)),
+    "hillshade": lambda: terrain.hillshade_stage(terrain.HillshadeOptions(CellSize=10)),
+    "hillshade_light": lambda: terrain.hillshade_stage(terrain.HillshadeOptions(CellSize=2, CellSizeY=3,
+                                                                                Azimuth=97.5, Altitude=30)),
+    "curv_profile": lambda: terrain.curvature_stage(terrain.CurvatureOptions(CellSize=10, Type=0)),
+    "curv_plan": lambda: terrain.curvature_stage(terrain.CurvatureOptions(CellSize=10, Type=1)),
+    "curv_mean": lambda: terrain.curvature_stage(terrain.CurvatureOptions(CellSize=3, CellSizeY=4, Type=2)),
+}
+
+
+@pytest.mark.parametrize("name", sorted(TERRAIN))
+def test_terrain_ops(name):
+    run_matrix(TERRAIN[name], dem_cells)
+
+
+def test_gradient_two_outputs():
+    run_matrix(lambda: terrain.gradient_stage(terrain.GradientOptions(CellSize=30, CellSizeY=25)), dem_cells, nout=2)
+
+
+@pytest.mark.parametrize("kind", range(4))
+@pytest.mark.parametrize("r", [1, 2, 3, 5, 8])
+def test_ruggedness(kind, r):
+    run_matrix(lambda: terrain.ruggedness_stage(terrain.RuggednessOptions(Type=kind, Radius=r)), dem_cells,
+               shapes=SMALL_SHAPES, seed=kind * 10 + r)
+
+
+@pytest.mark.parametrize("r", range(1, 9))
+def test_correlate(r):
+    w = synth.uniform_weights((2 * r + 1) ** 2, r)
+    run_matrix(lambda: focal.weights_stage(focal.WeightsOptions(Radius=r, Weights=w), False), focal_cells,
+               shapes=SMALL_SHAPES, seed=r)
+
+
+@pytest.mark.parametrize("r", [1, 3, 8])
+def test_convolve(r):
+    w = synth.uniform_weights((2 * r + 1) ** 2, 100 + r)
+    run_matrix(lambda: focal.weights_stage(focal.WeightsOptions(Radius=r, Weights=w), True), focal_cells,
+               shapes=SMALL_SHAPES, seed=r)
+
+
+@pytest.mark.parametrize("r", range(1, 9))
+def test_separable(r):
+    row = synth.uniform_weights(2 * r + 1, 200 + r)
+    col = focal.Gaussian(r, 2.5)
+    run_matrix(lambda: focal.separable_stage(focal.SeparableOptions(Radius=r, Row=row, Col=col)), focal_cells,
+               shapes=SMALL_SHAPES, seed=r)
+
+
+@pytest.mark.parametrize("op", ["mean", "min", "max"])
+@pytest.mark.parametrize("r", range(1, 9))
+def test_box(op, r):
+    opc = {"mean": engine._lib.OP_MEAN, "min": engine._lib.OP_MIN, "max": engine._lib.OP_MAX}[op]
+    run_matrix(lambda: focal.box_stage(focal.BoxOptions(Radius=r), opc), focal_cells, shapes=SMALL_SHAPES, seed=r)
+
+
+SLOPE_XS, SLOPE_YS = [0, 5, 10, 20, 30, 40], [1, 1.1, 1.3, 1.9, 3, 4.5]
+BREAKS, VALUES = [1.2, 1.6, 2.2, 3], [1, 2, 3, 4, 5]
+
+
+def test_lookup_and_reclass():
+    def cells(w, h, seed):
+        return poison((synth.normal_trend(w, h, seed) * 15 + 20).astype(np.float32), seed, 0.01)
+
+    run_matrix(lambda: transfer.lookup_stage(SLOPE_XS, SLOPE_YS), cells)
+    run_matrix(lambda: transfer.reclass_stage(BREAKS, VALUES), cells)
+
+
+def test_pipeline_slope_lookup_reclass():
+    """The fused Slope -> Lookup -> Reclass pass equals the oracle's three
+    stages, which equal three separate calls (internal/exec/pipeline.go)."""
+    def stages():
+        return (terrain.slope_stage(terrain.SlopeOptions(CellSize=10))
+                .extend(transfer.lookup_stage(SLOPE_XS, SLOPE_YS))
+                .extend(transfer.reclass_stage(BREAKS, VALUES)))
+
+    run_matrix(stages, dem_cells)
+
+
+def test_pipeline_equals_separate_calls():
+    w, h = 200, 77
+    cells = dem_cells(w, h, 9)
+    valid = synth.block_mask(w, h, 9, 0.05)
+    src = host_raster(cells, valid)
+    fused = like(src)
+    engine.process(terrain.slope_stage(terrain.SlopeOptions(CellSize=10))
+                   .extend(transfer.lookup_stage(SLOPE_XS, SLOPE_YS))
+                   .extend(transfer.reclass_stage(BREAKS, VALUES)), [fused], [src])
+    a, b, c = like(src), like(src), like(src)
+    terrain.Slope(a, src, terrain.SlopeOptions(CellSize=10))
+    transfer.Lookup(b, a, SLOPE_XS, SLOPE_YS)
+    transfer.Reclass(c, b, BREAKS, VALUES)
+    assert_same_raster(fused, c, "pipeline vs separate")
+
+
+def test_in_place_pointwise():
+    """A pointwise op may run in place (dst is src), as transfer allows."""
+    w, h = 100, 30
+    cells = poison(synth.normal_trend(w, h, 3) * 10, 3)
+    src = host_raster(cells, synth.cell_mask(w, h, 3))
+    want = like(src)
+    run_oracle(transfer.reclass_stage(BREAKS, VALUES), src, [want])
+    engine.process(transfer.reclass_stage(BREAKS, VALUES), [src], [src])
+    assert_same_raster(src, want, "in place")
+
+
+def test_edges_are_nan_and_invalid():
+    w, h = 40, 30
+    src = host_raster(dem_cells(w, h, 4), np.ones((h, w), bool))
+    for r in (1, 4, 8):
+        dst = like(src)
+        focal.Mean(dst, src, focal.BoxOptions(Radius=r))
+        a = dst.numpy()
+        v = dst.valid_numpy()
+        ring = np.ones((h, w), bool)
+        ring[r:h - r, r:w - r] = False
+        assert np.isnan(a[ring]).all() and not v[ring].any()
+        assert v[~ring].all()
+
+
+def test_window_smaller_than_radius_is_all_edge():
+    for w, h, r in ((5, 40, 3), (40, 2, 1), (16, 16, 8)):
+        src = host_raster(focal_cells(w, h, 1), np.ones((h, w), bool))
+        dst = like(src)
+        focal.Max(dst, src, focal.BoxOptions(Radius=r))
+        assert np.isnan(dst.numpy()).all() and not dst.valid_numpy().any()
+
+
+def test_tiled_options_give_the_same_bits():
+    """Tiled entry points write the same bits for every engine.Options
+    (the reference's TestTilesAndWorkers rule)."""
+    w, h = 300, 200
+    src = host_raster(dem_cells(w, h, 5), synth.cell_mask(w, h, 5))
+    want = like(src)
+    terrain.Slope(want, src, terrain.SlopeOptions(CellSize=30))
+    for tw, th, workers in ((1, 1, 1), (7, 64, 2), (256, 3, 3), (0, 0, 0), (1 << 20, 1 << 20, 8)):
+        got = like(src)
+        st = engine.Stats()
+        err = terrain.SlopeTiled(engine.Background(), got, src, terrain.SlopeOptions(CellSize=30),
+                                 engine.Options(TileWidth=tw, TileHeight=th, Workers=workers, Stats=st))
+        assert err is None
+        assert_same_raster(got, want, f"tiled {tw}x{th}")
+        assert st.Cells == w * h and st.Ideal == w * h * 8 and st.KernelWritten == w * h * 4
+        assert st.KernelRead >= w * h * 4
+
+
+@pytest.mark.parametrize("tile", [(1, 1), (7, 5), (64, 64), (300, 13), (0, 0), (1000, 1000)])
+def test_chunked_equals_plain(tile):
+    """Chunked through memory sources and sinks writes the plain call's bits
+    (internal/exec/chunked_test.go:162-200), for several tile shapes."""
+    w, h = 150, 90
+    src = host_raster(dem_cells(w, h, 6), synth.block_mask(w, h, 6, 0.05))
+    for name, mk in (("slope", lambda: terrain.slope_stage(terrain.SlopeOptions(CellSize=30))),
+                     ("tpi r3", lambda: terrain.ruggedness_stage(terrain.RuggednessOptions(Type=2, Radius=3))),
+                     ("max r4", lambda: focal.box_stage(focal.BoxOptions(Radius=4), engine._lib.OP_MAX))):
+        want = like(src)
+        engine.process(mk(), [want], [src])
+        got = like(src)
+        st = engine.Stats()
+        err = engine.process_chunked(mk(), [engine.MemorySink(got)], [engine.MemorySource(src)],
+                                     engine.Options(TileWidth=tile[0], TileHeight=tile[1], Stats=st))
+        assert err is None
+        assert_same_raster(got, want, f"chunked {name} {tile}")
+        assert st.Cells == w * h and st.SinkWritten == w * h * 4
+        tw = tile[0] if tile[0] else w
+        th = tile[1] if tile[1] else h
+        assert st.Tiles == -(-w // min(tw, w)) * -(-h // min(th, h))
+
+
+def test_chunked_gradient_two_sinks():
+    w, h = 77, 51
+    src = host_raster(dem_cells(w, h, 8), synth.cell_mask(w, h, 8))
+    want = [like(src), like(src)]
+    terrain.Gradient(want[0], want[1], src, terrain.GradientOptions(CellSize=30))
+    got = [like(src), like(src)]
+    err = terrain.GradientChunked(engine.Background(), engine.MemorySink(got[0]), engine.MemorySink(got[1]),
+                                  engine.MemorySource(src), terrain.GradientOptions(CellSize=30),
+                                  engine.Options(TileWidth=20, TileHeight=16))
+    assert err is None
+    assert_same_raster(got[0], want[0], "dx")
+    assert_same_raster(got[1], want[1], "dy")
+
+
+def test_slope_c1_size_against_oracle():
+    """Slope on the 2048 x 2048 workload (CellSize 30, 2% NoData in 8x8
+    blocks) equals the oracle on every cell."""
+    w = h = 2048
+    seed = 0x5EED0001
+    src = host_raster(synth.fbm_dem(w, h, seed), synth.block_mask(w, h, seed))
+    want, got = like(src), like(src)
+    run_oracle(terrain.slope_stage(terrain.SlopeOptions(CellSize=30)), src, [want], nthreads=8)
+    terrain.Slope(got, src, terrain.SlopeOptions(CellSize=30))
+    assert_same_raster(got, want, "slope 2048")
