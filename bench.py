@@ -119,6 +119,13 @@ def workload(name):
         return dict(name="Slope on 2048x2048 f32 DEM", width=n, height=n, cells=synth.fbm_dem(n, n, seed),
                     valid=synth.block_mask(n, n, seed, 0.02), cell_size=cs, mask="2% NoData in 8x8 blocks",
                     ops=[("slope", lambda: terrain.slope_stage(terrain.SlopeOptions(CellSize=cs)), 1)])
+    if name == "slope8k":
+        n, seed, cs = 8192, 0x5EED0001, 30
+        from strata_b200 import terrain
+
+        return dict(name="Slope on 8192x8192 f32 DEM", width=n, height=n, cells=synth.fbm_dem(n, n, seed),
+                    valid=synth.block_mask(n, n, seed, 0.02), cell_size=cs, mask="2% NoData in 8x8 blocks",
+                    ops=[("slope", lambda: terrain.slope_stage(terrain.SlopeOptions(CellSize=cs)), 1)])
     if name == "focal8k":
         n, seed = 8192, 0x5EED0003
         return dict(name="focal ops on 8192x8192 f32 raster", width=n, height=n, cells=synth.normal_trend(n, n, seed),
@@ -388,7 +395,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="terrain16k", choices=["terrain16k", "slope2k", "focal8k"])
+    ap.add_argument("--workload", default="terrain16k", choices=["terrain16k", "slope2k", "slope8k", "focal8k"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -13,6 +13,7 @@
 // every other bit of the word preserved.
 #include "cellops.cuh"
 #include "launch.h"
+#include "ops3.cuh"
 
 namespace strata {
 namespace {
@@ -26,40 +27,6 @@ constexpr int kCX = 2;
 constexpr int kCY = 4;
 constexpr int kTW = kThreadsX * kCX;  // tile width in cells
 constexpr int kTH = kThreadsY * kCY;  // tile height in cells
-
-__device__ __forceinline__ float epilogue(const LaunchParams& P, float v) {
-    for (int i = 0; i < P.nepi; i++) {
-        const EpiStage& e = P.epi[i];
-        v = e.op == STRATA_OP_LOOKUP ? lookup(v, e.a, e.b, e.n) : reclass(v, e.a, e.n, e.b);
-    }
-    return v;
-}
-
-// The 3x3 ops on a window whose centre is c, rows s floats apart.
-template <int OP>
-__device__ __forceinline__ void cell3(const LaunchParams& P, const float* c, int s, float& o0, float& o1) {
-    float z1 = c[-s - 1], z2 = c[-s], z3 = c[-s + 1];
-    float z4 = c[-1], z5 = c[0], z6 = c[1];
-    float z7 = c[s - 1], z8 = c[s], z9 = c[s + 1];
-    if constexpr (OP == STRATA_OP_CURVATURE) {
-        o0 = zt_curvature(z1, z2, z3, z4, z5, z6, z7, z8, z9, P.k, P.kind);
-    } else if constexpr (OP == STRATA_OP_RUGGEDNESS) {
-        o0 = rugged3(z1, z2, z3, z4, z5, z6, z7, z8, z9, P.kind);
-    } else {
-        float gx = mul(horn_dx(z1, z3, z4, z6, z7, z9), P.k[0]);
-        float gy = mul(horn_dy(z1, z2, z3, z7, z8, z9), P.k[1]);
-        if constexpr (OP == STRATA_OP_GRADIENT) {
-            o0 = gx;
-            o1 = gy;
-        } else if constexpr (OP == STRATA_OP_SLOPE) {
-            o0 = slope(gx, gy, P.k[2], P.kind != 0);
-        } else if constexpr (OP == STRATA_OP_ASPECT) {
-            o0 = aspect(gx, gy, P.k[2], P.kind != 0);
-        } else {
-            o0 = shade(gx, gy, P.k[2], P.k[3], P.k[4]);
-        }
-    }
-}
 
 // RuggednessWindowRow for radius R > 1 (internal/stencil/rugged.go:152-210):
 // Riley, Wilson and TPI over the window in row-major order without the
@@ -228,7 +195,9 @@ __global__ void __launch_bounds__(kThreads) tile_kernel(const __grid_constant__ 
                     } else if constexpr (OP == STRATA_OP_CORRELATE) {
                         o0 = correlate<R>(P, c, SP);
                     } else {
-                        cell3<OP>(P, c, SP, o0, o1);
+                        const float z[9] = {c[-SP - 1], c[-SP], c[-SP + 1], c[-1], c[0], c[1],
+                                            c[SP - 1], c[SP], c[SP + 1]};
+                        apply3<OP>(P, z, o0, o1);
                     }
                     o0 = epilogue(P, o0);
                 }
@@ -280,10 +249,11 @@ __device__ __forceinline__ uint32_t segment_bits(const ValidityParams& v, int64_
     if (r > 0 && (y < r || y >= H - r)) return 0u;
     uint32_t interior = 0xffffffffu;
     if (r > 0) {
-        // cells x + j with r <= x + j < W - r
-        const int64_t lo = r - x, hi = W - r - x;  // j in [lo, hi)
-        for (int j = 0; j < 32; j++)
-            if (j < lo || j >= hi) interior &= ~(1u << j);
+        // bits j of cells x + j with r <= x + j < W - r: j in [lo, hi)
+        const int64_t lo = r - x, hi = W - r - x;
+        const uint32_t mlo = lo <= 0 ? 0xffffffffu : (lo >= 32 ? 0u : ~((1u << lo) - 1u));
+        const uint32_t mhi = hi >= 32 ? 0xffffffffu : (hi <= 0 ? 0u : ((1u << hi) - 1u));
+        interior = mlo & mhi;
     }
     if (!v.src_bits) return interior;
     uint64_t acc = ~0ull;
@@ -397,6 +367,17 @@ int64_t launch_data(const LaunchParams& p, cudaStream_t s, int64_t* window_cells
     if (p.out_x1 <= p.out_x0 || p.out_y1 <= p.out_y0) {
         if (window_cells) *window_cells = 0;
         return 0;
+    }
+    if (march3_eligible(p)) {
+        const int64_t blocks = launch_march3(p, s);
+        if (window_cells) {
+            // Each warp reads its 128 columns and two halo columns, over its
+            // strip and one halo row above and below, clipped to the raster.
+            const int64_t w = p.out_x1 - p.out_x0, segs = (w + 127) / 128;
+            const int64_t rows = (p.out_y1 - p.out_y0) + 2 * (blocks / ((segs + 3) / 4));
+            *window_cells = (w + 2 * segs) * (rows < p.height ? rows : p.height);
+        }
+        return blocks;
     }
     const int64_t tiles = L(p, s);
     if (window_cells) {

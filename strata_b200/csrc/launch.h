@@ -5,7 +5,7 @@
 
 #include <cstdint>
 
-#include "../../include/strata_cuda.h"
+#include "strata_cuda.h"
 
 namespace strata {
 
@@ -84,6 +84,12 @@ int64_t launch_data(const LaunchParams& p, cudaStream_t stream, int64_t* window_
 
 // Launches the validity kernel for one output.
 void launch_validity(const ValidityParams& v, cudaStream_t stream);
+
+// The radius-1 marching kernel (march3.cu): whether it can run these
+// parameters (16-byte aligned rows at the region's first column, width a
+// multiple of 4), and its launcher.
+bool march3_eligible(const LaunchParams& p);
+int64_t launch_march3(const LaunchParams& p, cudaStream_t stream);
 
 // Tile geometry of the data kernels, for Stats.
 void tile_shape(int op, int radius, int64_t width, int* tw, int* th);

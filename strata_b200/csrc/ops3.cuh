@@ -1,0 +1,76 @@
+// ops3.cuh - every radius-1 op on a 3x3 window held in registers.
+//
+// z[0..8] is the window in row-major order (strata's z1..z9, z[4] the
+// centre). The Horn, Zevenbergen-Thorne and ruggedness ops call the cell
+// functions of cellops.cuh; the focal ops at radius 1 fold their terms in
+// the reference's order (internal/focalrow/focalrow.go:217-315): the 2-D
+// correlation from the first product in row-major order, the separable
+// ops column by column (top to bottom) and then across the three column
+// results (left to right).
+#pragma once
+
+#include "cellops.cuh"
+#include "launch.h"
+
+namespace strata {
+
+template <int OP>
+__device__ __forceinline__ void apply3(const LaunchParams& P, const float (&z)[9], float& o0, float& o1) {
+    using namespace cell;
+    if constexpr (OP == STRATA_OP_CURVATURE) {
+        o0 = zt_curvature(z[0], z[1], z[2], z[3], z[4], z[5], z[6], z[7], z[8], P.k, P.kind);
+    } else if constexpr (OP == STRATA_OP_RUGGEDNESS) {
+        o0 = rugged3(z[0], z[1], z[2], z[3], z[4], z[5], z[6], z[7], z[8], P.kind);
+    } else if constexpr (OP == STRATA_OP_CORRELATE) {
+        float acc = mul(P.w[0], z[0]);
+#pragma unroll
+        for (int i = 1; i < 9; i++) acc = add(acc, mul(P.w[i], z[i]));
+        o0 = acc;
+    } else if constexpr (OP == STRATA_OP_SEPARABLE) {
+        float t[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+            t[c] = add(add(mul(P.w[17], z[c]), mul(P.w[18], z[3 + c])), mul(P.w[19], z[6 + c]));
+        o0 = add(add(mul(P.w[0], t[0]), mul(P.w[1], t[1])), mul(P.w[2], t[2]));
+    } else if constexpr (OP == STRATA_OP_MEAN) {
+        float t[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) t[c] = add(add(z[c], z[3 + c]), z[6 + c]);
+        o0 = div(add(add(t[0], t[1]), t[2]), 9.0f);
+    } else if constexpr (OP == STRATA_OP_MIN) {
+        float t[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) t[c] = go_min(go_min(z[c], z[3 + c]), z[6 + c]);
+        o0 = go_min(go_min(t[0], t[1]), t[2]);
+    } else if constexpr (OP == STRATA_OP_MAX) {
+        float t[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) t[c] = go_max(go_max(z[c], z[3 + c]), z[6 + c]);
+        o0 = go_max(go_max(t[0], t[1]), t[2]);
+    } else {
+        float gx = mul(horn_dx(z[0], z[2], z[3], z[5], z[6], z[8]), P.k[0]);
+        float gy = mul(horn_dy(z[0], z[1], z[2], z[6], z[7], z[8]), P.k[1]);
+        if constexpr (OP == STRATA_OP_GRADIENT) {
+            o0 = gx;
+            o1 = gy;
+        } else if constexpr (OP == STRATA_OP_SLOPE) {
+            o0 = slope(gx, gy, P.k[2], P.kind != 0);
+        } else if constexpr (OP == STRATA_OP_ASPECT) {
+            o0 = aspect(gx, gy, P.k[2], P.kind != 0);
+        } else {
+            o0 = shade(gx, gy, P.k[2], P.k[3], P.k[4]);
+        }
+    }
+}
+
+// The pointwise stages fused after a stencil (exec.Pipeline's staged
+// Lookup / Reclass tail, internal/exec/pipeline.go:539-574).
+__device__ __forceinline__ float epilogue(const LaunchParams& P, float v) {
+    for (int i = 0; i < P.nepi; i++) {
+        const EpiStage& e = P.epi[i];
+        v = e.op == STRATA_OP_LOOKUP ? cell::lookup(v, e.a, e.b, e.n) : cell::reclass(v, e.a, e.n, e.b);
+    }
+    return v;
+}
+
+}  // namespace strata

@@ -19,8 +19,8 @@ from strata_b200.raster import Float32Raster
 
 pytestmark = pytest.mark.gpu
 
-SHAPES = [(1, 1), (2, 5), (3, 3), (17, 5), (61, 37), (300, 9), (129, 67), (257, 131)]
-SMALL_SHAPES = [(3, 3), (19, 23), (61, 37), (129, 40)]
+SHAPES = [(1, 1), (2, 5), (3, 3), (4, 4), (17, 5), (61, 37), (300, 9), (129, 67), (257, 131), (516, 70), (1028, 33)]
+SMALL_SHAPES = [(3, 3), (4, 9), (19, 23), (61, 37), (128, 40), (132, 21)]
 
 
 def dem_cells(w, h, seed):
@@ -38,6 +38,7 @@ def layouts(w, h, seed, masked):
     valid = synth.cell_mask(w, h, seed, 0.03) if masked else None
     yield dict(src=dict(stride=None, offset=0, valid=valid), dst=dict(stride=None, offset=0, masked=masked))
     yield dict(src=dict(stride=w + 13, offset=37, valid=valid), dst=dict(stride=w + 5, offset=11, masked=masked))
+    yield dict(src=dict(stride=w + 8, offset=5, valid=valid), dst=dict(stride=w + 4, offset=70, masked=masked))
     if not masked:
         yield dict(src=dict(stride=w + 1, offset=0, valid=None), dst=dict(stride=None, offset=63, masked=True))
 
