@@ -182,6 +182,20 @@ int strata_process(strata_ctx *ctx, const strata_stage *stages, int nstages,
                    const strata_exec_opts *opts, strata_stats *stats);
 
 /*
+ * terrain.Features / terrain.Surface (terrain/features.go:60-92,
+ * terrain/surface.go:57-98): several pipelines over one input in one call.
+ * Feature f is stages[s_f .. s_f + counts[f]) (s_f the sum of the earlier
+ * counts), a stencil stage with optional pointwise stages as in
+ * strata_process, writing the next 1 outputs of dst (2 for GRADIENT).
+ * Each output gets its own op's edge ring and validity. A host input
+ * crosses to the device once, and each output's copy back overlaps the
+ * next feature's kernels.
+ */
+int strata_process_features(strata_ctx *ctx, const strata_stage *stages, const int32_t *counts, int nfeatures,
+                            const strata_raster *src, const strata_raster *dst, int ndst,
+                            const strata_exec_opts *opts, strata_stats *stats);
+
+/*
  * engine.RasterSource / RasterSink (engine/source.go:19-70) as callbacks.
  * read fills buf (a host raster of buf->width x buf->height cells, with a
  * validity mask iff masked) from the window at (x, y); write takes buf

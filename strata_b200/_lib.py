@@ -117,6 +117,9 @@ SIGNATURES = [
     ("strata_process", ctypes.c_int, [c_p, ctypes.POINTER(Stage), ctypes.c_int, ctypes.POINTER(Raster),
                                       ctypes.c_int, ctypes.POINTER(Raster), ctypes.c_int,
                                       ctypes.POINTER(ExecOpts), ctypes.POINTER(Stats)]),
+    ("strata_process_features", ctypes.c_int, [c_p, ctypes.POINTER(Stage), ctypes.POINTER(c_i32), ctypes.c_int,
+                                               ctypes.POINTER(Raster), ctypes.POINTER(Raster), ctypes.c_int,
+                                               ctypes.POINTER(ExecOpts), ctypes.POINTER(Stats)]),
     ("strata_process_chunked", ctypes.c_int, [c_p, ctypes.POINTER(Stage), ctypes.c_int, ctypes.POINTER(Source),
                                               ctypes.c_int, ctypes.POINTER(Sink), ctypes.c_int,
                                               ctypes.POINTER(ExecOpts), ctypes.POINTER(Stats)]),

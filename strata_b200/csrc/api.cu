@@ -94,20 +94,26 @@ std::string fmt_v(double x, bool f32 = false) {
 struct strata_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t copy_stream = nullptr;  // device-to-host copies that overlap the next kernel
     std::mutex mu;
     // Device buffers for host operands, grown on demand and reused.
     struct Buf {
         void* p = nullptr;
         size_t n = 0;
     };
-    Buf bufs[8];
+    std::vector<Buf> bufs;
     // Page-locked staging for mask merges.
     std::vector<uint64_t> host_words;
+    // A device word kernels set when a bounded wait runs out, and its
+    // page-locked host copy.
+    int* d_status = nullptr;
+    int* h_status = nullptr;
 };
 
 namespace {
 
 int ensure(strata_ctx* c, int slot, size_t bytes, void** out) {
+    if ((int)c->bufs.size() <= slot) c->bufs.resize(slot + 1);
     auto& b = c->bufs[slot];
     if (b.n < bytes) {
         if (b.p) cudaFree(b.p);
@@ -143,10 +149,15 @@ extern "C" int strata_ctx_create(int device, strata_ctx** out) {
     auto* c = new strata_ctx;
     c->device = device;
     e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&c->d_status, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(c->d_status, 0, sizeof(int));
+    if (e == cudaSuccess) e = cudaHostAlloc(&c->h_status, sizeof(int), cudaHostAllocDefault);
     if (e != cudaSuccess) {
-        delete c;
-        return cuda_fail(e, "cudaStreamCreate");
+        strata_ctx_destroy(c);
+        return cuda_fail(e, "context set-up");
     }
+    *c->h_status = 0;
     *out = c;
     return STRATA_OK;
 }
@@ -157,18 +168,40 @@ extern "C" void strata_ctx_destroy(strata_ctx* c) {
     cudaStreamSynchronize(c->stream);
     for (auto& b : c->bufs)
         if (b.p) cudaFree(b.p);
-    cudaStreamDestroy(c->stream);
+    if (c->d_status) cudaFree(c->d_status);
+    if (c->h_status) cudaFreeHost(c->h_status);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     delete c;
 }
 
 extern "C" int strata_ctx_device(const strata_ctx* c) { return c ? c->device : -1; }
 
+namespace {
+
+// Reads and clears the status word after the work on st: STRATA_OK, or
+// the code a kernel recorded (STRATA_ETIMEDOUT).
+int take_status(strata_ctx* c, cudaStream_t st) {
+    cudaError_t e = cudaMemcpyAsync(c->h_status, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(e, "kernel");
+    int code = *c->h_status;
+    if (code != 0) {
+        cudaMemsetAsync(c->d_status, 0, sizeof(int), st);
+        cudaStreamSynchronize(st);
+        return fail(code, "strata_cuda: a device-side wait ran out (status %d)", code);
+    }
+    return STRATA_OK;
+}
+
+}  // namespace
+
 extern "C" int strata_ctx_synchronize(strata_ctx* c) {
     if (!c) return fail(STRATA_EINVAL, "strata_cuda: nil context");
     cudaSetDevice(c->device);
-    cudaError_t e = cudaStreamSynchronize(c->stream);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamSynchronize");
-    return STRATA_OK;
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceSynchronize");
+    return take_status(c, c->stream);
 }
 
 extern "C" int strata_alloc(strata_ctx* c, size_t bytes, void** dev) {
@@ -314,6 +347,12 @@ int fill_stage(const strata_stage& s, LaunchParams& p, int epi_index) {
         if (n < (s.op == STRATA_OP_LOOKUP ? 1 : 0) || n > STRATA_MAX_KNOTS || !s.table[0] || !s.table[1])
             return fail(STRATA_EINVAL, "engine: stage table of %d entries (1 to %d)", n, STRATA_MAX_KNOTS);
         e.n = n;
+        // transfer.checkIncreasing (transfer/transfer.go:225-239): the
+        // device's table index relies on strictly increasing knots.
+        for (int i = 0; i < n; i++)
+            if (s.table[0][i] != s.table[0][i] || (i > 0 && !(s.table[0][i - 1] < s.table[0][i])))
+                return fail(STRATA_EINVAL, "engine: %s table must be strictly increasing and free of NaN",
+                            s.op == STRATA_OP_LOOKUP ? "Lookup" : "Reclass");
         memcpy(e.a, s.table[0], sizeof(float) * n);
         memcpy(e.b, s.table[1], sizeof(float) * (s.op == STRATA_OP_LOOKUP ? n : n + 1));
         return STRATA_OK;
@@ -587,6 +626,7 @@ extern "C" int strata_process(strata_ctx* c, const strata_stage* stages, int nst
     p.height = H;
     p.out_x0 = 0;
     p.out_x1 = W;
+    p.status = c->d_status;
 
     // Row strips: the whole raster at once, or strips of about 2^22 cells
     // with the cancel flag polled between them.
@@ -630,8 +670,7 @@ extern "C" int strata_process(strata_ctx* c, const strata_stage* stages, int nst
     for (int i = 0; i < ndst; i++)
         if ((rc = stage_out(c, st, dst[i], dd[i]))) return rc;
     if (!(all_device && opts && (opts->flags & STRATA_EXEC_ASYNC))) {
-        cudaError_t e = cudaStreamSynchronize(st);
-        if (e != cudaSuccess) return cuda_fail(e, "kernel");
+        if ((rc = take_status(c, st))) return rc;
     }
     if (stats) {
         int64_t cells = done_rows * W;
@@ -1171,6 +1210,7 @@ extern "C" int strata_process_chunked(strata_ctx* c, const strata_stage* stages,
         q.out_y1 = y1;
         q.width = W;
         q.height = H;
+        q.status = c->d_status;
         int64_t wc = 0;
         int64_t nt = strata::launch_data(q, st, &wc);
         if (nt < 0) {
@@ -1258,6 +1298,161 @@ extern "C" int strata_process_chunked(strata_ctx* c, const strata_stage* stages,
         stats->kernel_read += local.kernel_read;
         stats->kernel_written += local.kernel_written;
     }
+    if (status == STRATA_OK) status = take_status(c, st);
     if (status == STRATA_ECANCELED) return fail(STRATA_ECANCELED, "context canceled");
     return status;
+}
+
+// ---------------------------------------------------------------------------
+// terrain.Features / terrain.Surface (terrain/features.go:60-92,
+// terrain/surface.go:57-98): several pipelines over one input in one
+// call. A host input crosses to the device once; each output's copy back
+// runs on a second stream while the next pipeline computes.
+
+namespace {
+
+// Mask bits of a host destination merged into the caller's words: the
+// words the raster's span shares with other rasters keep their other bits.
+void merge_mask(const strata_raster& r, const DevOperand& d, const std::vector<uint64_t>& words) {
+    int64_t lo = r.valid_offset, hi = r.valid_offset + span_cells(r);
+    for (int64_t k = 0; k < d.nwords64; k++) {
+        int64_t w = d.host_w0 + k;
+        uint64_t own = ~0ull;
+        if (w * 64 < lo) own &= ~0ull << (lo - w * 64);
+        if ((w + 1) * 64 > hi) own &= (hi - w * 64) >= 64 ? ~0ull : ((1ull << (hi - w * 64)) - 1);
+        r.valid[w] = (r.valid[w] & ~own) | (words[(size_t)k] & own);
+    }
+}
+
+}  // namespace
+
+extern "C" int strata_process_features(strata_ctx* c, const strata_stage* stages, const int32_t* counts,
+                                       int nfeatures, const strata_raster* src, const strata_raster* dst,
+                                       int ndst, const strata_exec_opts* opts, strata_stats* stats) {
+    if (!c) return fail(STRATA_EINVAL, "engine: nil context");
+    if (nfeatures < 1 || !stages || !counts || !src || !dst)
+        return fail(STRATA_EINVAL, "terrain: Features has no outputs");
+    int rc;
+    if ((rc = check_opts(opts))) return rc;
+    // Resolve every feature's pipeline and its outputs.
+    std::vector<LaunchParams> plans((size_t)nfeatures);
+    std::vector<int> nouts((size_t)nfeatures), first((size_t)nfeatures);
+    int off = 0, outs = 0, rmax = 0;
+    for (int f = 0; f < nfeatures; f++) {
+        if (counts[f] < 1) return fail(STRATA_EINVAL, "terrain: Features output %d has no Op", f);
+        if ((rc = plan_stages(stages + off, counts[f], plans[(size_t)f], &nouts[(size_t)f]))) return rc;
+        first[(size_t)f] = outs;
+        outs += nouts[(size_t)f];
+        off += counts[f];
+        rmax = std::max(rmax, plans[(size_t)f].radius);
+    }
+    if (ndst != outs)
+        return fail(STRATA_EINVAL, "engine: the features write %d outputs, got %d rasters", outs, ndst);
+    // The checks of one ProcessN call with every output (the pipeline's
+    // radius is the largest of its stages').
+    if ((rc = check_operands(src, 1, dst, ndst, ndst, rmax))) return rc;
+
+    std::lock_guard<std::mutex> lock(c->mu);
+    cudaSetDevice(c->device);
+    cudaStream_t st = (opts && opts->stream) ? (cudaStream_t)opts->stream : c->stream;
+    cudaStream_t cs = c->copy_stream;
+    const int64_t W = src[0].width, H = src[0].height;
+    DevOperand ds;
+    if ((rc = stage_in(c, st, src[0], 0, true, &ds))) return rc;
+    std::vector<DevOperand> dd((size_t)ndst);
+    for (int i = 0; i < ndst; i++)
+        if ((rc = stage_in(c, st, dst[i], 2 + 2 * i, false, &dd[(size_t)i]))) return rc;
+    std::vector<std::vector<uint64_t>> words((size_t)ndst);
+    std::vector<cudaEvent_t> events;
+    auto cleanup = [&] {
+        for (auto e : events) cudaEventDestroy(e);
+    };
+    int64_t bands = 0, window = 0;
+    for (int f = 0; f < nfeatures; f++) {
+        LaunchParams& p = plans[(size_t)f];
+        const int o = first[(size_t)f];
+        p.src = ds.data;
+        p.src_stride = ds.stride;
+        p.src_x0 = p.src_y0 = 0;
+        p.src_w = W;
+        p.src_h = H;
+        p.dst0 = dd[(size_t)o].data;
+        p.dst0_stride = dd[(size_t)o].stride;
+        if (nouts[(size_t)f] > 1) {
+            p.dst1 = dd[(size_t)o + 1].data;
+            p.dst1_stride = dd[(size_t)o + 1].stride;
+        }
+        p.dst_x0 = p.dst_y0 = 0;
+        p.width = W;
+        p.height = H;
+        p.out_x0 = 0;
+        p.out_x1 = W;
+        p.out_y0 = 0;
+        p.out_y1 = H;
+        p.status = c->d_status;
+        int64_t wc = 0;
+        int64_t t = strata::launch_data(p, st, &wc);
+        if (t < 0) {
+            cleanup();
+            return fail(STRATA_ENOTSUP, "engine: op %d at radius %d has no device kernel", p.op, p.radius);
+        }
+        bands += t;
+        window += wc;
+        for (int i = o; i < o + nouts[(size_t)f]; i++) {
+            if (!dst[i].valid) continue;
+            ValidityParams v;
+            fill_validity(v, ds, src[0].valid != nullptr, dd[(size_t)i], span_cells(dst[i]), W, H, p.radius, 0, H);
+            strata::launch_validity(v, st);
+        }
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) {
+            cleanup();
+            return cuda_fail(e, "kernel launch");
+        }
+        // The outputs' copies back overlap the next feature's kernels.
+        bool any_host = false;
+        for (int i = o; i < o + nouts[(size_t)f]; i++) any_host = any_host || !dst[i].on_device;
+        if (!any_host) continue;
+        cudaEvent_t ev;
+        if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) {
+            cleanup();
+            return cuda_fail(e, "event");
+        }
+        events.push_back(ev);
+        cudaEventRecord(ev, st);
+        cudaStreamWaitEvent(cs, ev, 0);
+        for (int i = o; i < o + nouts[(size_t)f]; i++) {
+            if (dst[i].on_device) continue;
+            const DevOperand& d = dd[(size_t)i];
+            e = cudaMemcpy2DAsync(dst[i].data, (size_t)dst[i].stride * 4, d.data, (size_t)dst[i].stride * 4,
+                                  (size_t)W * 4, (size_t)H, cudaMemcpyDeviceToHost, cs);
+            if (e == cudaSuccess && dst[i].valid) {
+                words[(size_t)i].resize((size_t)d.nwords64);
+                e = cudaMemcpyAsync(words[(size_t)i].data(), d.bits, (size_t)d.nwords64 * 8,
+                                    cudaMemcpyDeviceToHost, cs);
+            }
+            if (e != cudaSuccess) {
+                cleanup();
+                return cuda_fail(e, "copy to host");
+            }
+        }
+    }
+    cudaError_t e = cudaStreamSynchronize(cs);
+    cleanup();
+    if (e != cudaSuccess) return cuda_fail(e, "copy to host");
+    bool all_device = src[0].on_device != 0;
+    for (int i = 0; i < ndst; i++) all_device = all_device && dst[i].on_device;
+    if (!(all_device && opts && (opts->flags & STRATA_EXEC_ASYNC)))
+        if ((rc = take_status(c, st))) return rc;
+    for (int i = 0; i < ndst; i++)
+        if (!dst[i].on_device && dst[i].valid) merge_mask(dst[i], dd[(size_t)i], words[(size_t)i]);
+    if (stats) {
+        const int64_t cells = W * H;
+        stats->cells += cells;
+        stats->ideal += cells * 4 * (1 + ndst);
+        stats->bands += bands;
+        stats->kernel_read += window * 4;
+        stats->kernel_written += cells * 4 * ndst;
+    }
+    return STRATA_OK;
 }

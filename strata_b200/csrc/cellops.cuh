@@ -28,18 +28,21 @@ __device__ __forceinline__ float sqrt64of32(float x) { return __fsqrt_rn(x); }
 __device__ __forceinline__ float nanf32() { return __int_as_float(0x7fc00000); }
 __device__ __forceinline__ float abs32(float x) { return __int_as_float(__float_as_int(x) & 0x7fffffff); }
 
-// Go's builtin min and max for float32: NaN wins, -0 orders below +0.
+// Go's builtin min and max for float32: NaN wins, -0 orders below +0. The
+// PTX min.NaN / max.NaN instructions have exactly these rules (a NaN
+// operand gives NaN, and -0 is below +0); tests/test_gpu_minmax.py pins
+// them against the oracle's restatement over every ordered pair of
+// special values. Any NaN matches any NaN under the reference's
+// comparison rule, so the canonical NaN they return is the same result.
 __device__ __forceinline__ float go_min(float a, float b) {
-    if (a != a) return a;
-    if (b != b) return b;
-    if (a == b) return __int_as_float(__float_as_int(a) | __float_as_int(b));
-    return a < b ? a : b;
+    float r;
+    asm("min.NaN.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
+    return r;
 }
 __device__ __forceinline__ float go_max(float a, float b) {
-    if (a != a) return a;
-    if (b != b) return b;
-    if (a == b) return __int_as_float(__float_as_int(a) & __float_as_int(b));
-    return a > b ? a : b;
+    float r;
+    asm("max.NaN.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
+    return r;
 }
 
 // Atan32 constants (internal/stencil/horn.go:226-235, aspect.go:10-14),
@@ -214,35 +217,37 @@ __device__ __forceinline__ float rugged3(float v1, float v2, float v3, float v4,
     return sub(hi, lo);
 }
 
-// scalarLookupFloat32 (internal/curve/scalar.go:84-114).
-__device__ __forceinline__ float lookup(float v, const float* xs, const float* ys, int n) {
-    if (v != v) return v;
-    int k = n;
-    for (int j = 0; j < n; j++) {
-        if (v < xs[j]) {
-            k = j;
-            break;
-        }
-    }
-    if (k == 0) return ys[0];
-    if (k == n) return ys[n - 1];
-    float x0 = xs[k - 1], y0 = ys[k - 1];
-    if (v == x0) return y0;
-    float t = div(sub(v, x0), sub(xs[k], x0));
-    return add(y0, mul(t, sub(ys[k], y0)));
+// The reference's table index, k = the first j with v < xs[j] (or n):
+// for strictly increasing, NaN-free knots and a non-NaN v that is the
+// number of knots at or below v, which this counts without branches. The
+// engine rejects tables that are not strictly increasing.
+__device__ __forceinline__ int knots_at_or_below(float v, const float* xs, int n) {
+    int k = 0;
+    for (int j = 0; j < n; j++) k += xs[j] <= v ? 1 : 0;
+    return k;
 }
 
-// scalarReclassFloat32 (internal/curve/scalar.go:39-60).
+// scalarLookupFloat32 (internal/curve/scalar.go:84-114): NaN passes
+// through, the ends clamp, a cell on a knot takes the knot's y, and
+// elsewhere y0 + float32(t * (y1 - y0)) with t = (v - x0) / (x1 - x0).
+__device__ __forceinline__ float lookup(float v, const float* xs, const float* ys, int n) {
+    const int k = knots_at_or_below(v, xs, n);
+    const int lo = k == 0 ? 0 : k - 1;
+    const int hi = k == n ? n - 1 : k;
+    const float x0 = xs[lo], y0 = ys[lo];
+    const float t = div(sub(v, x0), sub(xs[hi], x0));
+    float r = add(y0, mul(t, sub(ys[hi], y0)));
+    r = v == x0 ? y0 : r;
+    r = k == n ? ys[n - 1] : r;
+    r = k == 0 ? ys[0] : r;
+    return v != v ? v : r;
+}
+
+// scalarReclassFloat32 (internal/curve/scalar.go:39-60): values[k] for k
+// the number of breaks at or below v; NaN passes through.
 __device__ __forceinline__ float reclass(float v, const float* breaks, int nb, const float* values) {
-    if (v != v) return v;
-    int k = nb;
-    for (int j = 0; j < nb; j++) {
-        if (v < breaks[j]) {
-            k = j;
-            break;
-        }
-    }
-    return values[k];
+    const float r = values[knots_at_or_below(v, breaks, nb)];
+    return v != v ? v : r;
 }
 
 }  // namespace cell

@@ -44,6 +44,7 @@ struct LaunchParams {
     int64_t width, height;
     int64_t tiles_x;  // thread-block tiles across the region (set by the launcher)
     int64_t tiles;    // thread-block tiles in the launch (set by the launcher)
+    int* status;  // device word a kernel sets to a STRATA_E* code (a bounded wait that ran out)
     int op;
     int radius;
     int kind;

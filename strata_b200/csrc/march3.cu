@@ -1,27 +1,38 @@
-// march3.cu - the radius-1 data kernel: register marching down row strips.
+// march3.cu - the radius-1 data kernels: register marching down row strips.
 //
 // Each warp owns 128 consecutive columns of a strip of rows, four per
-// lane. A lane reads each input row once as one aligned float4 (a warp
-// reads 512 contiguous bytes), takes the column to its left and right
-// from its neighbours with warp shuffles (the warp's two outer columns
-// with one extra load each), and keeps the rows it still needs in
-// registers while it walks down the strip, so every input cell is read
-// from memory once per strip plus two halo rows. Loads run kAhead rows
-// ahead of the arithmetic. Each lane writes its four results with one
-// float4 store.
+// lane, and walks down the strip keeping the window's three rows in
+// registers, so every input cell is read from memory once per strip plus
+// two halo rows. Each lane writes its four results with one float4 store.
+//
+// Rows reach the registers one of two ways:
+//   * march3_tma_kernel (the default): each warp has a private ring of
+//     boxes in shared memory, each box four rows of its 128 columns plus
+//     halo, filled by tensor copies (cp.async.bulk.tensor.2d, the TMA
+//     engine, completion counted on an mbarrier; cells outside the source
+//     read as zero, so no copy needs clipping). Lane 0 keeps kBoxes boxes
+//     (up to 12 rows) in flight per warp, so the memory system sees many
+//     rows of loads per warp without registers holding them; a lane reads
+//     its four cells with one LDS.128 and takes its neighbours by warp
+//     shuffle. Every wait is bounded: on a timeout the kernel records
+//     STRATA_ETIMEDOUT in the status word, waits (bounded) for its own
+//     copies in flight and returns.
+//   * march3_kernel: aligned float4 loads straight into registers, one row
+//     ahead, when the tensor map cannot be encoded.
 //
 // Horn ops (gradient, slope, aspect, hillshade) reuse each row's
 // horizontal differences: hornDX's z3 - z1, z6 - z4 and z9 - z7
 // (internal/stencil/horn.go:152-155) are one row's x+1 minus x-1 seen as
 // the window's top, middle and bottom row, so each row's difference is
 // computed once and used by three output rows. The operations and their
-// order per cell are the reference's, so the bits are too.
+// order per cell are the reference's, so the bits are too. The other ops
+// evaluate apply3 (ops3.cuh), shared with the general tile kernel.
 //
-// The per-cell arithmetic of the other ops is apply3 (ops3.cuh), shared
-// with the general tile kernel. The launcher takes this path only when
-// every row of the source and destination starts on a 16-byte boundary at
-// the region's first column and the region is a multiple of 4 wide;
-// otherwise the tile kernel runs.
+// The launcher takes these paths only when every row of the source and
+// destination starts on a 16-byte boundary at the region's first column
+// and the region is a multiple of 4 wide; otherwise the tile kernel runs.
+#include <cuda.h>
+
 #include "launch.h"
 #include "ops3.cuh"
 
@@ -31,22 +42,136 @@ namespace {
 using namespace cell;
 
 constexpr int kWarps = 4;  // warps per block, side by side: 512 columns
-constexpr int kAhead = 1;  // rows loaded ahead of the arithmetic
-constexpr int kRing = kAhead + 3;
 constexpr unsigned kFull = 0xffffffffu;
 
 struct Row6 {
     float v[6];  // columns x-1 .. x+4 around the lane's four
 };
 
-// Marching state for one lane: where its rows live and which are inside
-// the source.
+// hornDX's horizontal difference of one row for the four cells.
+__device__ __forceinline__ void hdiff(const Row6& r, float (&h)[4]) {
+#pragma unroll
+    for (int i = 0; i < 4; i++) h[i] = sub(r.v[i + 2], r.v[i]);
+}
+
+// The shared-memory copy of the epilogue's tables, for kernels with one.
+template <bool EPI>
+struct EpiSmem {
+    __device__ static EpiTables* get() {
+        __shared__ EpiTables t;
+        return &t;
+    }
+};
+template <>
+struct EpiSmem<false> {
+    __device__ static EpiTables* get() { return nullptr; }
+};
+
+template <int OP>
+constexpr bool kIsHorn = OP == STRATA_OP_GRADIENT || OP == STRATA_OP_SLOPE || OP == STRATA_OP_ASPECT ||
+                         OP == STRATA_OP_HILLSHADE;
+
+// One output row of four cells from the window rows a (top), b, c
+// (bottom) and, for Horn ops, their horizontal differences.
+template <int OP, int KIND, bool EPI>
+__device__ __forceinline__ void row_compute(const LaunchParams& P, const EpiTables* T, const Row6& a, const Row6& b,
+                                            const Row6& c,
+                                            const float (&ha)[4], const float (&hb)[4], const float (&hc)[4],
+                                            bool rowin, const bool (&colin)[4], float (&o0)[4], float (&o1)[4]) {
+    const float nan = nanf32();
+    if constexpr (kIsHorn<OP>) {
+        // hornDY's vertical differences: bottom row minus top row.
+        float v[6];
+#pragma unroll
+        for (int j = 0; j < 6; j++) v[j] = sub(c.v[j], a.v[j]);
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const float dx = add(add(ha[i], hc[i]), add(hb[i], hb[i]));
+            const float dy = add(add(v[i], v[i + 2]), add(v[i + 1], v[i + 1]));
+            const float gx = mul(dx, P.k[0]);
+            const float gy = mul(dy, P.k[1]);
+            const bool in = rowin && colin[i];
+            if constexpr (OP == STRATA_OP_GRADIENT) {
+                o0[i] = in ? gx : nan;
+                o1[i] = in ? gy : nan;
+            } else {
+                float r;
+                if constexpr (OP == STRATA_OP_SLOPE) r = slope(gx, gy, P.k[2], KIND != 0);
+                else if constexpr (OP == STRATA_OP_ASPECT) r = aspect(gx, gy, P.k[2], KIND != 0);
+                else r = shade(gx, gy, P.k[2], P.k[3], P.k[4]);
+                if constexpr (EPI) r = epilogue(P, *T, r);
+                o0[i] = in ? r : nan;
+            }
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const float z[9] = {a.v[i], a.v[i + 1], a.v[i + 2], b.v[i], b.v[i + 1],
+                                b.v[i + 2], c.v[i], c.v[i + 1], c.v[i + 2]};
+            float r0 = nan, r1 = nan;
+            apply3<OP>(P, z, r0, r1);
+            if constexpr (EPI) r0 = epilogue(P, *T, r0);
+            o0[i] = (rowin && colin[i]) ? r0 : nan;
+        }
+    }
+}
+
+// What every marching kernel works out first: the warp's columns, rows and
+// interior tests, and where its outputs go.
+struct Strip {
+    int64_t xs, x, y0;
+    int rows, lane;
+    bool active, last;
+    bool colin[4];
+    int yrel, ylast;
+    float* d0;
+    float* d1;
+};
+
+template <int OP>
+__device__ __forceinline__ bool strip_setup(const LaunchParams& P, int strip, int col_blocks, Strip& S) {
+    S.lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int cb = blockIdx.x % col_blocks;
+    const int sb = blockIdx.x / col_blocks;
+    S.xs = P.out_x0 + (int64_t)(cb * kWarps + warp) * 128;
+    if (S.xs >= P.out_x1) return false;  // warp-uniform
+    S.x = S.xs + 4 * S.lane;
+    S.y0 = P.out_y0 + (int64_t)sb * strip;
+    S.rows = (int)min((int64_t)strip, P.out_y1 - S.y0);
+    // The region's width is a multiple of 4, so a lane is wholly in or out.
+    S.active = S.x < P.out_x1;
+    S.last = S.active && (S.lane == 31 || S.x + 4 >= P.out_x1);
+    const int64_t W = P.width;
+#pragma unroll
+    for (int i = 0; i < 4; i++) S.colin[i] = S.x + i >= 1 && S.x + i < W - 1;
+    S.yrel = (int)(S.y0 - 1);
+    S.ylast = (int)(P.height - 2);
+    S.d0 = P.dst0 + (S.y0 - P.dst_y0) * P.dst0_stride + (S.x - P.dst_x0);
+    S.d1 = OP == STRATA_OP_GRADIENT ? P.dst1 + (S.y0 - P.dst_y0) * P.dst1_stride + (S.x - P.dst_x0) : nullptr;
+    return true;
+}
+
+template <int OP>
+__device__ __forceinline__ void store_row(const LaunchParams& P, Strip& S, const float (&o0)[4],
+                                          const float (&o1)[4]) {
+    if (S.active) {
+        *reinterpret_cast<float4*>(S.d0) = make_float4(o0[0], o0[1], o0[2], o0[3]);
+        if constexpr (OP == STRATA_OP_GRADIENT)
+            *reinterpret_cast<float4*>(S.d1) = make_float4(o1[0], o1[1], o1[2], o1[3]);
+    }
+    S.d0 += P.dst0_stride;
+    if constexpr (OP == STRATA_OP_GRADIENT) S.d1 += P.dst1_stride;
+}
+
+// ---------------------------------------------------------------------------
+// Loads straight into registers.
+
 struct Lane {
-    const float* p;    // &src[row][x] of the next row to load
-    int64_t stride;    // source row stride
-    int by, src_h;     // next row, relative to the source's first row
-    bool active, first, last;
-    bool left_in, right_in;  // x-1 / x+4 inside the source columns
+    const float* p;  // &src[row][x] of the next row to load
+    int64_t stride;
+    int by, src_h;  // next row, relative to the source's first row
+    bool active, first, last, left_in, right_in;
 };
 
 __device__ __forceinline__ Row6 load_row(Lane& L) {
@@ -69,139 +194,257 @@ __device__ __forceinline__ Row6 load_row(Lane& L) {
     return r;
 }
 
-// hornDX's horizontal difference of one row for the four cells.
-__device__ __forceinline__ void hdiff(const Row6& r, float (&h)[4]) {
-#pragma unroll
-    for (int i = 0; i < 4; i++) h[i] = sub(r.v[i + 2], r.v[i]);
-}
-
-// The Horn finishers (slope, aspect, hillshade) of ops3 on gx, gy, with the
-// op's kind fixed at compile time.
-template <int OP, int KIND>
-__device__ __forceinline__ float horn_finish(const LaunchParams& P, float gx, float gy) {
-    if constexpr (OP == STRATA_OP_SLOPE) {
-        return slope(gx, gy, P.k[2], KIND != 0);
-    } else if constexpr (OP == STRATA_OP_ASPECT) {
-        return aspect(gx, gy, P.k[2], KIND != 0);
-    } else {
-        return shade(gx, gy, P.k[2], P.k[3], P.k[4]);
-    }
-}
+constexpr int kRing = 4;  // three window rows and one in flight
 
 template <int OP, int KIND, bool EPI>
 __global__ void __launch_bounds__(kWarps * 32, 8) march3_kernel(const __grid_constant__ LaunchParams P, int strip,
                                                                  int col_blocks) {
-    constexpr bool kHorn = OP == STRATA_OP_GRADIENT || OP == STRATA_OP_SLOPE || OP == STRATA_OP_ASPECT ||
-                           OP == STRATA_OP_HILLSHADE;
-    const int lane = threadIdx.x & 31;
-    const int warp = threadIdx.x >> 5;
-    const int cb = blockIdx.x % col_blocks;
-    const int sb = blockIdx.x / col_blocks;
-    const int64_t xs = P.out_x0 + (int64_t)(cb * kWarps + warp) * 128;
-    if (xs >= P.out_x1) return;  // warp-uniform
-    const int64_t x = xs + 4 * lane;
-    const int64_t y0 = P.out_y0 + (int64_t)sb * strip;
-    const int rows = (int)min((int64_t)strip, P.out_y1 - y0);
-
+    constexpr bool kHorn = kIsHorn<OP>;
+    EpiTables* T = EpiSmem<EPI>::get();
+    if constexpr (EPI) {
+        stage_epilogue(P, *T);
+        __syncthreads();
+    }
+    Strip S;
+    if (!strip_setup<OP>(P, strip, col_blocks, S)) return;
     Lane L;
-    L.active = x < P.out_x1;
-    // The region's width is a multiple of 4, so a lane is wholly in or out;
-    // the last active lane fetches its right neighbour itself.
-    L.first = lane == 0;
-    L.last = L.active && (lane == 31 || x + 4 >= P.out_x1);
-    L.left_in = x - 1 >= P.src_x0;
-    L.right_in = x + 4 < P.src_x0 + P.src_w;
+    L.active = S.active;
+    L.first = S.lane == 0;
+    L.last = S.last;
+    L.left_in = S.x - 1 >= P.src_x0;
+    L.right_in = S.x + 4 < P.src_x0 + P.src_w;
     L.stride = P.src_stride;
-    L.by = (int)(y0 - 1 - P.src_y0);
+    L.by = (int)(S.y0 - 1 - P.src_y0);
     L.src_h = (int)P.src_h;
-    L.p = P.src + (int64_t)L.by * P.src_stride + (x - P.src_x0);
+    L.p = P.src + (int64_t)L.by * P.src_stride + (S.x - P.src_x0);
+    const int rows = S.rows;
 
-    float* d0 = P.dst0 + (y0 - P.dst_y0) * P.dst0_stride + (x - P.dst_x0);
-    float* d1 = OP == STRATA_OP_GRADIENT ? P.dst1 + (y0 - P.dst_y0) * P.dst1_stride + (x - P.dst_x0) : nullptr;
-
-    // Interior: x + i in [1, W - 1) and y in [1, H - 1).
-    const int64_t W = P.width;
-    bool colin[4];
-#pragma unroll
-    for (int i = 0; i < 4; i++) colin[i] = x + i >= 1 && x + i < W - 1;
-    int yrel = (int)(y0 - 1);          // y - 1 of the current output row, for the row test
-    const int ylast = (int)(P.height - 2);  // last interior row
-    const float nan = nanf32();
-
-    // kRing rows live at once (three for the window, kAhead in flight),
-    // kept in a ring that the unrolled loop renames instead of copying.
+    // Ring slot m % kRing holds row y0 - 1 + m; output row y0 + k reads
+    // m = k .. k + 2, and row k + 3 loads while row k computes.
     Row6 ring[kRing];
-    float hr[kRing][4];  // each ring row's horizontal differences (Horn ops)
-    // Ring slot m % kRing holds row y0 - 1 + m: the window of output row
-    // y0 + k is m = k .. k + 2, and rows m <= 1 + kAhead load up front.
+    float hr[kRing][4];
 #pragma unroll
-    for (int j = 0; j < 2 + kAhead; j++) {
-        if (j < 3 || j - 2 < rows) {
-            ring[j] = load_row(L);
-            if constexpr (kHorn) hdiff(ring[j], hr[j]);
-        }
+    for (int j = 0; j < 3; j++) {
+        ring[j] = load_row(L);
+        if constexpr (kHorn) hdiff(ring[j], hr[j]);
     }
     for (int k0 = 0; k0 < rows; k0 += kRing) {
 #pragma unroll
         for (int u = 0; u < kRing; u++) {
             const int k = k0 + u;
             if (k >= rows) break;
-            const Row6& a = ring[u % kRing];
-            const Row6& b = ring[(u + 1) % kRing];
-            const Row6& c = ring[(u + 2) % kRing];
-            // Row m = k + 2 + kAhead, the bottom of output row k + kAhead's
-            // window, into the slot row m = k - 1 no longer needs.
-            if (k + kAhead < rows) {
-                ring[(u + 3 + kAhead - 1) % kRing] = load_row(L);
-                if constexpr (kHorn) hdiff(ring[(u + 3 + kAhead - 1) % kRing], hr[(u + 3 + kAhead - 1) % kRing]);
+            if (k + 1 < rows) {
+                ring[(u + 3) % kRing] = load_row(L);
+                if constexpr (kHorn) hdiff(ring[(u + 3) % kRing], hr[(u + 3) % kRing]);
             }
-            yrel++;
-            const bool rowin = yrel >= 1 && yrel <= ylast;
+            S.yrel++;
+            const bool rowin = S.yrel >= 1 && S.yrel <= S.ylast;
             float o0[4], o1[4];
-            if constexpr (kHorn) {
-                const float(&ha)[4] = hr[u % kRing];
-                const float(&hb)[4] = hr[(u + 1) % kRing];
-                const float(&hc)[4] = hr[(u + 2) % kRing];
-                // hornDY's vertical differences: bottom row minus top row.
-                float v[6];
-#pragma unroll
-                for (int j = 0; j < 6; j++) v[j] = sub(c.v[j], a.v[j]);
-#pragma unroll
-                for (int i = 0; i < 4; i++) {
-                    const float dx = add(add(ha[i], hc[i]), add(hb[i], hb[i]));
-                    const float dy = add(add(v[i], v[i + 2]), add(v[i + 1], v[i + 1]));
-                    const float gx = mul(dx, P.k[0]);
-                    const float gy = mul(dy, P.k[1]);
-                    const bool in = rowin && colin[i];
-                    if constexpr (OP == STRATA_OP_GRADIENT) {
-                        o0[i] = in ? gx : nan;
-                        o1[i] = in ? gy : nan;
-                    } else {
-                        float r = horn_finish<OP, KIND>(P, gx, gy);
-                        if constexpr (EPI) r = epilogue(P, r);
-                        o0[i] = in ? r : nan;
-                    }
-                }
-            } else {
-#pragma unroll
-                for (int i = 0; i < 4; i++) {
-                    const float z[9] = {a.v[i], a.v[i + 1], a.v[i + 2], b.v[i], b.v[i + 1],
-                                        b.v[i + 2], c.v[i], c.v[i + 1], c.v[i + 2]};
-                    float r0 = nan, r1 = nan;
-                    apply3<OP>(P, z, r0, r1);
-                    if constexpr (EPI) r0 = epilogue(P, r0);
-                    o0[i] = (rowin && colin[i]) ? r0 : nan;
-                }
-            }
-            if (L.active) {
-                *reinterpret_cast<float4*>(d0) = make_float4(o0[0], o0[1], o0[2], o0[3]);
-                if constexpr (OP == STRATA_OP_GRADIENT)
-                    *reinterpret_cast<float4*>(d1) = make_float4(o1[0], o1[1], o1[2], o1[3]);
-            }
-            d0 += P.dst0_stride;
-            if constexpr (OP == STRATA_OP_GRADIENT) d1 += P.dst1_stride;
+            row_compute<OP, KIND, EPI>(P, T, ring[u % kRing], ring[(u + 1) % kRing], ring[(u + 2) % kRing],
+                                       hr[u % kRing], hr[(u + 1) % kRing], hr[(u + 2) % kRing], rowin, S.colin,
+                                       o0, o1);
+            store_row<OP>(P, S, o0, o1);
         }
     }
+}
+
+// ---------------------------------------------------------------------------
+// Tensor copies (TMA) into a per-warp shared-memory ring.
+
+constexpr int kBoxRows = 4;            // rows per tensor copy
+constexpr int kBoxCols = 136;          // columns xs-4 .. xs+131
+constexpr int kBoxes = 3;              // ring slots (boxes in flight) per warp
+constexpr uint32_t kBoxBytes = kBoxRows * kBoxCols * 4;
+constexpr uint32_t kSpinLimit = 1u << 20;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_fence_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// The bounded wait for the phase of `parity` on bar; false on timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    for (uint32_t i = 0; !mbar_try_wait(bar, parity); i++)
+        if (i >= kSpinLimit) return false;
+    return true;
+}
+
+// One box of the source tensor (kBoxCols x kBoxRows cells whose first cell
+// is column x, row y of the source) into 128-byte aligned shared memory,
+// completing on bar. Cells outside the source read as zero. No multicast:
+// the destination is this CTA's own shared memory.
+__device__ __forceinline__ void tma_box(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+template <int OP, int KIND, bool EPI>
+__global__ void __launch_bounds__(kWarps * 32, 6)
+    march3_tma_kernel(const __grid_constant__ LaunchParams P, const __grid_constant__ CUtensorMap map, int strip,
+                      int col_blocks) {
+    constexpr bool kHorn = kIsHorn<OP>;
+    __shared__ __align__(128) float sbuf[kWarps][kBoxes][kBoxRows * kBoxCols];
+    __shared__ __align__(8) uint64_t sbar[kWarps][kBoxes];
+    EpiTables* T = EpiSmem<EPI>::get();
+    if constexpr (EPI) {
+        stage_epilogue(P, *T);
+        __syncthreads();
+    }
+    Strip S;
+    if (!strip_setup<OP>(P, strip, col_blocks, S)) return;
+    const int warp = threadIdx.x >> 5;
+    float* boxes = &sbuf[warp][0][0];
+    uint64_t* bars = sbar[warp];
+    const int lane = S.lane;
+    const int rows = S.rows;
+    const int need = rows + 2;  // rows m = 0 .. rows + 1 (y0 - 1 .. y0 + rows)
+    const int nbox = (need + kBoxRows - 1) / kBoxRows;
+    // Box b holds rows m = 4b .. 4b + 3; its first cell is source column
+    // xs - 4 (a multiple of 4: the copy's 16-byte rule) and source row
+    // y0 - 1 + 4b.
+    const int bx = (int)(S.xs - 4 - P.src_x0);
+    const int by = (int)(S.y0 - 1 - P.src_y0);
+
+    if (lane == 0) {
+#pragma unroll
+        for (int s = 0; s < kBoxes; s++) mbar_init(&bars[s], 1);
+        mbar_fence_init();
+    }
+    __syncwarp();
+    // Box b into slot b % kBoxes, phase b / kBoxes of that slot's barrier.
+    auto issue = [&](int b) {
+        uint64_t* bar = &bars[b % kBoxes];
+        mbar_arrive_expect_tx(bar, kBoxBytes);
+        tma_box(boxes + (b % kBoxes) * (kBoxRows * kBoxCols), &map, bx, by + b * kBoxRows, bar);
+    };
+    int issued = min(nbox, kBoxes);  // boxes 0 .. issued - 1 have been issued
+    int waited = 0;                  // boxes 0 .. waited - 1 have landed and been waited for
+    if (lane == 0)
+        for (int b = 0; b < issued; b++) issue(b);
+
+    bool ok = true;
+    // Reads row m (waiting for its box first when it is the box's first
+    // row), and when m is its box's last row, gives the slot to the box
+    // kBoxes later.
+    auto take = [&](int m, Row6& r) {
+        const int b = m / kBoxRows;
+        if ((m % kBoxRows) == 0) {
+            if (ok) ok = __all_sync(kFull, mbar_wait(&bars[b % kBoxes], (uint32_t)(b / kBoxes) & 1u));
+            waited = b + 1;
+        }
+        const float* row = boxes + (b % kBoxes) * (kBoxRows * kBoxCols) + (m % kBoxRows) * kBoxCols;
+        const float4 q = *reinterpret_cast<const float4*>(row + 4 + 4 * lane);
+        float l = __shfl_up_sync(kFull, q.w, 1);
+        float rr = __shfl_down_sync(kFull, q.x, 1);
+        if (lane == 0) l = row[3];
+        if (S.last) rr = row[8 + 4 * lane];
+        r.v[0] = l;
+        r.v[1] = q.x;
+        r.v[2] = q.y;
+        r.v[3] = q.z;
+        r.v[4] = q.w;
+        r.v[5] = rr;
+        if ((m % kBoxRows) == kBoxRows - 1 && ok && b + kBoxes < nbox) {
+            __syncwarp();
+            if (lane == 0) {
+                fence_proxy_async();  // this warp's reads of the slot before the copy overwrites it
+                issue(b + kBoxes);
+            }
+            issued = b + kBoxes + 1;
+        }
+    };
+
+    // Register slot m % 4 holds row m: output row k reads m = k .. k + 2
+    // and takes row k + 2; unrolled by 4, every index is a constant.
+    Row6 ring[4];
+    float hr[4][4];
+    take(0, ring[0]);
+    take(1, ring[1]);
+    if constexpr (kHorn) {
+        hdiff(ring[0], hr[0]);
+        hdiff(ring[1], hr[1]);
+    }
+    for (int k0 = 0; k0 < rows && ok; k0 += 4) {
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int k = k0 + u;
+            if (k >= rows) break;
+            take(k + 2, ring[(u + 2) % 4]);
+            if constexpr (kHorn) hdiff(ring[(u + 2) % 4], hr[(u + 2) % 4]);
+            S.yrel++;
+            const bool rowin = S.yrel >= 1 && S.yrel <= S.ylast;
+            float o0[4], o1[4];
+            row_compute<OP, KIND, EPI>(P, T, ring[u % 4], ring[(u + 1) % 4], ring[(u + 2) % 4], hr[u % 4],
+                                       hr[(u + 1) % 4], hr[(u + 2) % 4], rowin, S.colin, o0, o1);
+            if (ok) store_row<OP>(P, S, o0, o1);
+        }
+    }
+    if (!ok) {
+        // A copy did not land in time: report it, then wait (bounded) for
+        // the boxes this warp still has in flight before its shared memory
+        // goes away.
+        if (lane == 0 && P.status) atomicExch(P.status, STRATA_ETIMEDOUT);
+        for (int b = waited; b < issued; b++) mbar_wait(&bars[b % kBoxes], (uint32_t)(b / kBoxes) & 1u);
+    }
+}
+
+// The source as a 2-D tensor for the box copies: cuTensorMapEncodeTiled,
+// reached through the runtime's driver entry point (no libcuda link).
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return reinterpret_cast<EncodeTiledFn>(p);
+    }();
+    return fn;
+}
+
+bool source_map(const LaunchParams& p, CUtensorMap* map) {
+    EncodeTiledFn fn = encode_tiled();
+    if (!fn) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)p.src_w, (cuuint64_t)p.src_h};
+    const cuuint64_t strides[1] = {(cuuint64_t)p.src_stride * 4};
+    const cuuint32_t box[2] = {kBoxCols, kBoxRows};
+    const cuuint32_t elem[2] = {1, 1};
+    return fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(p.src), dims, strides, box, elem,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
@@ -217,7 +460,12 @@ int64_t launch_march(const LaunchParams& p, cudaStream_t s) {
     strip = strip < 8 ? 8 : (strip > 64 ? 64 : strip);
     const int64_t strips = (h + strip - 1) / strip;
     const int64_t blocks = col_blocks * strips;
-    march3_kernel<OP, KIND, EPI><<<(unsigned)blocks, kWarps * 32, 0, s>>>(p, (int)strip, (int)col_blocks);
+    CUtensorMap map;
+    if (source_map(p, &map))
+        march3_tma_kernel<OP, KIND, EPI><<<(unsigned)blocks, kWarps * 32, 0, s>>>(p, map, (int)strip,
+                                                                                 (int)col_blocks);
+    else
+        march3_kernel<OP, KIND, EPI><<<(unsigned)blocks, kWarps * 32, 0, s>>>(p, (int)strip, (int)col_blocks);
     return blocks;
 }
 

@@ -64,12 +64,73 @@ __device__ __forceinline__ void apply3(const LaunchParams& P, const float (&z)[9
 }
 
 // The pointwise stages fused after a stencil (exec.Pipeline's staged
-// Lookup / Reclass tail, internal/exec/pipeline.go:539-574).
+// Lookup / Reclass tail, internal/exec/pipeline.go:539-574), reading their
+// tables from the launch parameters.
 __device__ __forceinline__ float epilogue(const LaunchParams& P, float v) {
     for (int i = 0; i < P.nepi; i++) {
         const EpiStage& e = P.epi[i];
         v = e.op == STRATA_OP_LOOKUP ? cell::lookup(v, e.a, e.b, e.n) : cell::reclass(v, e.a, e.n, e.b);
     }
+    return v;
+}
+
+// The epilogue's tables staged in shared memory: each cell reads the
+// knots of its own segment, and lanes reading different addresses of the
+// constant bank are served one address at a time, where shared memory
+// serves them together.
+struct EpiTables {
+    float a[kMaxEpilogue][STRATA_MAX_KNOTS];
+    float b[kMaxEpilogue][STRATA_MAX_KNOTS + 1];
+};
+
+// Copies the tables in with every thread of the block; the caller
+// synchronises the block before reading them.
+__device__ __forceinline__ void stage_epilogue(const LaunchParams& P, EpiTables& T) {
+    constexpr int per = 2 * STRATA_MAX_KNOTS + 1;
+    for (int i = threadIdx.x + threadIdx.y * blockDim.x; i < P.nepi * per; i += blockDim.x * blockDim.y) {
+        const int s = i / per, j = i - s * per;
+        if (j < STRATA_MAX_KNOTS) T.a[s][j] = P.epi[s].a[j];
+        else T.b[s][j - STRATA_MAX_KNOTS] = P.epi[s].b[j - STRATA_MAX_KNOTS];
+    }
+}
+
+// Knots of a short table (n <= kShortTable) at or below v, counted against
+// the launch parameters: the loop unrolls, so each knot is a constant-bank
+// operand of one compare.
+constexpr int kShortTable = 8;
+
+__device__ __forceinline__ int short_count(float v, const float* xs, int n) {
+    int k = 0;
+#pragma unroll
+    for (int j = 0; j < kShortTable; j++) k += (j < n && xs[j] <= v) ? 1 : 0;
+    return k;
+}
+
+// One pointwise stage on v: the count against the parameters when the
+// table is short, the gather from the shared-memory copy.
+__device__ __forceinline__ float epi_stage(const EpiStage& e, const float* ta, const float* tb, float v) {
+    const int n = e.n;
+    const int k = n <= kShortTable ? short_count(v, e.a, n) : cell::knots_at_or_below(v, ta, n);
+    if (e.op == STRATA_OP_RECLASS) {
+        const float r = tb[k];
+        return v != v ? v : r;
+    }
+    // Lookup, as cell::lookup from its table index on.
+    const int lo = k == 0 ? 0 : k - 1;
+    const int hi = k == n ? n - 1 : k;
+    const float x0 = ta[lo], y0 = tb[lo];
+    const float t = cell::div(cell::sub(v, x0), cell::sub(ta[hi], x0));
+    float r = cell::add(y0, cell::mul(t, cell::sub(tb[hi], y0)));
+    r = v == x0 ? y0 : r;
+    r = k == n ? tb[n - 1] : r;
+    r = k == 0 ? tb[0] : r;
+    return v != v ? v : r;
+}
+
+__device__ __forceinline__ float epilogue(const LaunchParams& P, const EpiTables& T, float v) {
+#pragma unroll
+    for (int i = 0; i < kMaxEpilogue; i++)
+        if (i < P.nepi) v = epi_stage(P.epi[i], T.a[i], T.b[i], v);
     return v;
 }
 

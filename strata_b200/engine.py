@@ -192,6 +192,33 @@ def process(stages: StageList, dst: Sequence[Float32Raster], src: Sequence[Float
     return None
 
 
+def process_features(features: Sequence[StageList], dst: Sequence[Float32Raster], src: Float32Raster,
+                     opts: Optional[Options] = None, ctx: Optional[Context] = None):
+    """Several pipelines over one input in one call (terrain.Features,
+    terrain.Surface): features[i] writes the next outputs of dst (two for a
+    gradient). A host input crosses to the device once. Returns None;
+    raises StrataPanic on programming errors."""
+    dev = opts.Device if opts is not None else 0
+    c = device_context(dev)
+    all_stages = StageList()
+    counts = []
+    for f in features:
+        all_stages.extend(f)
+        counts.append(len(f.stages))
+    cnt = (ctypes.c_int32 * len(counts))(*counts)
+    srcs = (_lib.Raster * 1)(c_raster(src))
+    dsts = (_lib.Raster * len(dst))(*[c_raster(d) for d in dst])
+    o = c_opts(opts, ctx)
+    cst = _lib.Stats()
+    rc = _lib.lib().strata_process_features(c, all_stages.c_array(), cnt, len(counts), srcs, dsts, len(dst),
+                                            ctypes.byref(o), ctypes.byref(cst))
+    _stats_out(opts, cst)
+    if rc == _lib.ECANCELED:
+        return Canceled("context canceled")
+    _lib.check(rc)
+    return None
+
+
 # ---------------------------------------------------------------------------
 # Sources and sinks (engine/source.go).
 

@@ -116,6 +116,101 @@ def _plain(stages, dem, *outs):
     process(stages, list(outs), [dem], Options(Workers=1), Background())
 
 
+# Features (terrain/features.go): several ops over one DEM in one call.
+@dataclass
+class Feature:
+    Op: object  # SlopeOptions, AspectOptions, HillshadeOptions, CurvatureOptions or RuggednessOptions
+    Dst: Float32Raster
+
+
+_FEATURE_STAGES = {
+    SlopeOptions: slope_stage,
+    AspectOptions: aspect_stage,
+    HillshadeOptions: hillshade_stage,
+    CurvatureOptions: curvature_stage,
+    RuggednessOptions: ruggedness_stage,
+}
+
+
+def _feature_stage(i: int, op) -> StageList:
+    from .raster import StrataPanic
+
+    if op is None:
+        raise StrataPanic(f"terrain: Features output {i} has no Op")
+    fn = _FEATURE_STAGES.get(type(op))
+    if fn is None:
+        raise StrataPanic(f"terrain: Features output {i}: {type(op).__name__} is not a feature op")
+    return fn(op)
+
+
+def Features(out, dem: Float32Raster) -> None:
+    FeaturesTiled(Background(), out, dem, Options(Workers=1))
+
+
+def FeaturesTiled(ctx: Context, out, dem: Float32Raster, eopts: Options):
+    from .engine import process_features
+    from .raster import StrataPanic
+
+    if not out:
+        raise StrataPanic("terrain: Features has no outputs")
+    return process_features([_feature_stage(i, f.Op) for i, f in enumerate(out)], [f.Dst for f in out], dem,
+                            eopts, ctx)
+
+
+# Surface (terrain/surface.go): the Horn gradient and the products that
+# finish it, from one DEM pass.
+@dataclass
+class SurfaceOptions:
+    CellSize: float = 0.0
+    CellSizeY: float = 0.0
+    ZFactor: float = 0.0
+    FitRadius: int = 0
+    Units: int = SlopeDegrees
+    ZeroForFlat: bool = False
+    Trigonometric: bool = False
+    Azimuth: float = 0.0
+    Altitude: float = 0.0
+
+
+@dataclass
+class SurfaceOutputs:
+    Dx: Float32Raster = None
+    Dy: Float32Raster = None
+    Slope: Float32Raster = None
+    Aspect: Float32Raster = None
+    Hillshade: Float32Raster = None
+
+
+def Surface(out: SurfaceOutputs, dem: Float32Raster, opts: SurfaceOptions) -> None:
+    SurfaceTiled(Background(), out, dem, opts, Options(Workers=1))
+
+
+def SurfaceTiled(ctx: Context, out: SurfaceOutputs, dem: Float32Raster, opts: SurfaceOptions, eopts: Options):
+    from .engine import process_features
+    from .raster import NewFloat32Like, StrataPanic
+
+    c = dict(CellSize=opts.CellSize, CellSizeY=opts.CellSizeY, ZFactor=opts.ZFactor, FitRadius=opts.FitRadius)
+    features, dsts = [], []
+    if out.Dx is not None or out.Dy is not None:
+        features.append(gradient_stage(GradientOptions(**c)))
+        like = out.Dx if out.Dx is not None else out.Dy
+        dsts += [out.Dx if out.Dx is not None else NewFloat32Like(like),
+                 out.Dy if out.Dy is not None else NewFloat32Like(like)]
+    if out.Slope is not None:
+        features.append(slope_stage(SlopeOptions(Units=opts.Units, **c)))
+        dsts.append(out.Slope)
+    if out.Aspect is not None:
+        features.append(aspect_stage(AspectOptions(ZeroForFlat=opts.ZeroForFlat, Trigonometric=opts.Trigonometric,
+                                                   **c)))
+        dsts.append(out.Aspect)
+    if out.Hillshade is not None:
+        features.append(hillshade_stage(HillshadeOptions(Azimuth=opts.Azimuth, Altitude=opts.Altitude, **c)))
+        dsts.append(out.Hillshade)
+    if not features:
+        raise StrataPanic("terrain: Surface has no outputs; set at least one of Dx, Dy, Slope, Aspect and Hillshade")
+    return process_features(features, dsts, dem, eopts, ctx)
+
+
 # Gradient (terrain/gradient.go)
 def Gradient(dx: Float32Raster, dy: Float32Raster, dem: Float32Raster, opts: GradientOptions) -> None:
     _plain(gradient_stage(opts), dem, dx, dy)

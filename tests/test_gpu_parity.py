@@ -270,3 +270,97 @@ def test_slope_c1_size_against_oracle():
     run_oracle(terrain.slope_stage(terrain.SlopeOptions(CellSize=30)), src, [want], nthreads=8)
     terrain.Slope(got, src, terrain.SlopeOptions(CellSize=30))
     assert_same_raster(got, want, "slope 2048")
+
+
+def test_features_equal_separate_calls():
+    """terrain.Features (terrain/features.go): every output equals its op run
+    alone, with mixed radii (each output its own edge ring), host and device."""
+    w, h = 203, 71
+    cells = dem_cells(w, h, 12)
+    src = host_raster(cells, synth.block_mask(w, h, 12, 0.05))
+    ops = [terrain.SlopeOptions(CellSize=10), terrain.AspectOptions(CellSize=10),
+           terrain.HillshadeOptions(CellSize=10), terrain.CurvatureOptions(CellSize=10, Type=1),
+           terrain.RuggednessOptions(Type=terrain.RuggednessTPI, Radius=3),
+           terrain.RuggednessOptions(Type=terrain.RuggednessRoughness)]
+    singles = {terrain.SlopeOptions: terrain.Slope, terrain.AspectOptions: terrain.Aspect,
+               terrain.HillshadeOptions: terrain.Hillshade, terrain.CurvatureOptions: terrain.Curvature,
+               terrain.RuggednessOptions: terrain.Ruggedness}
+    for device in (False, True):
+        s = to_device(src) if device else src
+        outs = [to_device(like(src)) if device else like(src) for _ in ops]
+        terrain.Features([terrain.Feature(op, d) for op, d in zip(ops, outs)], s)
+        for op, got in zip(ops, outs):
+            want = like(src)
+            singles[type(op)](want, src, op)
+            assert_same_raster(to_host(got), want, f"features {type(op).__name__} device={device}")
+
+
+def test_surface_equals_separate_calls():
+    w, h = 128, 40
+    src = host_raster(dem_cells(w, h, 13), synth.cell_mask(w, h, 13))
+    o = terrain.SurfaceOptions(CellSize=5, Units=terrain.SlopePercent, Azimuth=200, Altitude=30)
+    out = terrain.SurfaceOutputs(Dx=like(src), Dy=like(src), Slope=like(src), Aspect=like(src),
+                                 Hillshade=like(src))
+    terrain.Surface(out, src, o)
+    dx, dy, sl, asp, hs = like(src), like(src), like(src), like(src), like(src)
+    terrain.Gradient(dx, dy, src, terrain.GradientOptions(CellSize=5))
+    terrain.Slope(sl, src, terrain.SlopeOptions(CellSize=5, Units=terrain.SlopePercent))
+    terrain.Aspect(asp, src, terrain.AspectOptions(CellSize=5))
+    terrain.Hillshade(hs, src, terrain.HillshadeOptions(CellSize=5, Azimuth=200, Altitude=30))
+    for got, want, n in ((out.Dx, dx, "dx"), (out.Dy, dy, "dy"), (out.Slope, sl, "slope"),
+                         (out.Aspect, asp, "aspect"), (out.Hillshade, hs, "hillshade")):
+        assert_same_raster(got, want, f"surface {n}")
+    only = terrain.SurfaceOutputs(Dy=like(src))
+    terrain.Surface(only, src, o)
+    assert_same_raster(only.Dy, dy, "surface dy alone")
+
+
+def test_graph_run_equals_engine():
+    from strata_b200 import graph
+
+    w, h = 96, 50
+    src = host_raster(dem_cells(w, h, 14), synth.block_mask(w, h, 14, 0.05))
+    g = graph.New()
+    dem = g.Input("dem")
+    g.Output("class", graph.Reclass(graph.Lookup(graph.Slope(dem, terrain.SlopeOptions(CellSize=10)),
+                                                 SLOPE_XS, SLOPE_YS), BREAKS, VALUES))
+    out = like(src)
+    assert g.Plan().Run(engine.Background(), {"dem": src}, {"class": out}) is None
+    want = like(src)
+    run_oracle(terrain.slope_stage(terrain.SlopeOptions(CellSize=10)).extend(transfer.lookup_stage(SLOPE_XS, SLOPE_YS))
+               .extend(transfer.reclass_stage(BREAKS, VALUES)), src, [want])
+    assert_same_raster(out, want, "graph")
+
+
+def test_cancel_before_start_returns_canceled():
+    w, h = 64, 64
+    src = host_raster(dem_cells(w, h, 15))
+    dst = like(src)
+    ctx = engine.Context()
+    ctx.cancel()
+    err = terrain.SlopeTiled(ctx, dst, src, terrain.SlopeOptions(CellSize=1), engine.Options())
+    assert isinstance(err, engine.Canceled)
+
+
+def test_chunked_source_error_is_returned():
+    """A failing source ends the call with its error, wrapped with the
+    operand and position (internal/exec/chunked.go:379-393), and the sink
+    holds only whole tiles in plan order before it."""
+    w, h = 64, 48
+    src = host_raster(dem_cells(w, h, 16))
+
+    class Failing(engine.MemorySource):
+        def ReadWindow(self, dst, x, y):
+            if y > 20:
+                return IOError("disk on fire")
+            return super().ReadWindow(dst, x, y)
+
+    got = like(src)
+    err = terrain.SlopeChunked(engine.Background(), engine.MemorySink(got), Failing(src),
+                               terrain.SlopeOptions(CellSize=1), engine.Options(TileWidth=64, TileHeight=16))
+    assert isinstance(err, engine.SourceSinkError) and "disk on fire" in str(err) and "src[0]" in str(err)
+    want = like(src)
+    terrain.Slope(want, src, terrain.SlopeOptions(CellSize=1))
+    from helpers import same_bits
+
+    assert same_bits(got.numpy()[:16], want.numpy()[:16]).all()
