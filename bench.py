@@ -126,6 +126,16 @@ def workload(name):
         return dict(name="Slope on 8192x8192 f32 DEM", width=n, height=n, cells=synth.fbm_dem(n, n, seed),
                     valid=synth.block_mask(n, n, seed, 0.02), cell_size=cs, mask="2% NoData in 8x8 blocks",
                     ops=[("slope", lambda: terrain.slope_stage(terrain.SlopeOptions(CellSize=cs)), 1)])
+    if name == "pipeline8k":
+        n, seed, cs = 8192, 0x5EED0002, 10
+        from strata_b200 import terrain, transfer
+
+        return dict(name="Slope->Lookup->Reclass on 8192x8192 f32 DEM", width=n, height=n,
+                    cells=synth.fbm_dem(n, n, seed), valid=synth.block_mask(n, n, seed, 0.02), cell_size=cs,
+                    mask="2% NoData in 8x8 blocks",
+                    ops=[("slope_lookup_reclass", lambda: terrain.slope_stage(terrain.SlopeOptions(CellSize=cs))
+                          .extend(transfer.lookup_stage(SLOPE_XS, SLOPE_YS))
+                          .extend(transfer.reclass_stage(BREAKS, VALUES)), 1)])
     if name == "focal8k":
         n, seed = 8192, 0x5EED0003
         return dict(name="focal ops on 8192x8192 f32 raster", width=n, height=n, cells=synth.normal_trend(n, n, seed),
@@ -376,6 +386,112 @@ def run_ours(args, rank, world, local_rank):
         print(json.dumps(line), flush=True)
 
 
+def batch_rasters(seed=0x5EED0004, count=512):
+    """The batched workload: `count` rasters with width and height each
+    log-uniform in 64..4096 (windows of one seeded fBm mosaic, so each is
+    fBm terrain), 2% NoData in 8x8 blocks, each with one op from {Slope,
+    Hillshade, Curvature (kind uniform), Correlate r in 1..8 (uniform
+    [-1, 1] weights)} and CellSize uniform in 1..90."""
+    from strata_b200 import focal, synth, terrain
+
+    rng = np.random.default_rng(seed)
+    mosaic = synth.fbm_dem(8192, 8192, seed)
+    out = []
+    for i in range(count):
+        w = int(np.exp(rng.uniform(np.log(64), np.log(4096))))
+        h = int(np.exp(rng.uniform(np.log(64), np.log(4096))))
+        x = int(rng.integers(0, 8192 - w + 1))
+        y = int(rng.integers(0, 8192 - h + 1))
+        cells = np.ascontiguousarray(mosaic[y:y + h, x:x + w])
+        valid = synth.block_mask(w, h, seed + i, 0.02)
+        cs = float(rng.uniform(1, 90))
+        kind = int(rng.integers(4))
+        if kind == 0:
+            name, st = "slope", terrain.slope_stage(terrain.SlopeOptions(CellSize=cs))
+        elif kind == 1:
+            name, st = "hillshade", terrain.hillshade_stage(terrain.HillshadeOptions(CellSize=cs))
+        elif kind == 2:
+            t = int(rng.integers(3))
+            name, st = f"curvature{t}", terrain.curvature_stage(terrain.CurvatureOptions(CellSize=cs, Type=t))
+        else:
+            r = int(rng.integers(1, 9))
+            wts = synth.uniform_weights((2 * r + 1) ** 2, seed + 7 * i)
+            name, st = f"correlate_r{r}", focal.weights_stage(focal.WeightsOptions(r, wts), False)
+        out.append((name, st, cells, valid))
+    return out
+
+
+def run_batch(args, rank, world, local_rank):
+    """The batched form against per-raster plain launches, same rasters."""
+    import torch
+
+    from strata_b200 import batch, engine
+    from strata_b200.raster import Float32Raster, mask_from_bool
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    rasters = batch_rasters()
+    items, cells = [], 0
+    for name, st, c, v in rasters:
+        h, w = c.shape
+        n = w * h
+        words = (n + 63) // 64
+        src = Float32Raster(torch.from_numpy(c.reshape(-1)).to(dev), w, h, w,
+                            torch.from_numpy(mask_from_bool(v).view(np.int64)).to(dev), 0)
+        dst = Float32Raster(torch.empty(n, dtype=torch.float32, device=dev), w, h, w,
+                            torch.empty(words, dtype=torch.int64, device=dev), 0)
+        items.append(batch.Item(st, src, [dst]))
+        cells += n
+    tuner = batch.Autotuner(path=os.path.join(ROOT, "strata_b200", "tuning.json") if args.tune_cache else None)
+    b = batch.Batch(items, local_rank, tuner)
+    opts = engine.Options(Device=local_rank)
+
+    def plain_step():
+        for it in items:
+            assert engine.process(it.stages, it.dst, [it.src], opts) is None
+
+    for _ in range(args.warmup):
+        b.run()
+        plain_step()
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stream = torch.cuda.current_stream(dev)
+    with Clocks(local_rank) as clk:
+        start.record(stream)
+        for _ in range(args.steps):
+            b.run(stream=stream, synchronize=False)
+        end.record(stream)
+        torch.cuda.synchronize()
+    ms = start.elapsed_time(end) / args.steps
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        plain_step()
+    torch.cuda.synchronize()
+    plain_ms = (time.perf_counter() - t0) / args.steps * 1e3
+    st, classes = b.stats()
+    value = world * cells / (ms / 1e3) / 1e6
+    plain = world * cells / (plain_ms / 1e3) / 1e6
+    peak, peak_kind = hbm_peak()
+    alg = sum(alg_bytes(it.src.width * it.src.height, 1, True) for it in items)
+    line = {
+        "metric": "Mcells/s (batched rasters, one graph launch)", "value": round(value, 1), "unit": "Mcells/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "batch of 512 rasters, sides log-uniform 64..4096, mixed ops", "rasters": len(items),
+                   "cells": cells, "classes": classes, "l2": "inputs larger than L2 (no flush)"},
+        "plain_launches": {"value": round(plain, 1), "unit": "Mcells/s", "ms_per_step": round(plain_ms, 3),
+                           "api": "engine.process per raster, synchronous"},
+        "batched_over_plain": round(plain_ms / ms, 2),
+        "roofline": {"bound": "hbm", "kernel": "batch_kernel (all classes)", "achieved": round(alg / (ms / 1e3) / 1e9, 1),
+                     "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": round(alg / (ms / 1e3) / 1e9 / peak, 4), "traffic": None},
+        "gpu_launches": classes * args.steps, "clocks": clk.summary(),
+    }
+    b.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def run_reference(args):
     wl = workload(args.workload)
     threads = os.cpu_count() or 1
@@ -408,7 +524,9 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="terrain16k", choices=["terrain16k", "slope2k", "slope8k", "focal8k"])
+    ap.add_argument("--workload", default="terrain16k",
+                    choices=["terrain16k", "slope2k", "slope8k", "pipeline8k", "focal8k", "batch512"])
+    ap.add_argument("--tune-cache", action="store_true", help="keep the batch autotuner's choices in a file")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -427,7 +545,10 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     try:
-        run_ours(args, rank, world, local_rank)
+        if args.workload == "batch512":
+            run_batch(args, rank, world, local_rank)
+        else:
+            run_ours(args, rank, world, local_rank)
     finally:
         if world > 1:
             import torch.distributed as dist

@@ -228,6 +228,37 @@ int strata_process_chunked(strata_ctx *ctx, const strata_stage *stages, int nsta
                            const strata_source *src, int nsrc, const strata_sink *dst, int ndst,
                            const strata_exec_opts *opts, strata_stats *stats);
 
+/*
+ * Batches (the batched form of the path; no counterpart call in strata,
+ * whose plain functions take one raster each): many device-resident
+ * rasters of mixed sizes and ops, each item one pipeline (stages as in
+ * strata_process) over src into dst[0] (and dst[1] for GRADIENT), with the
+ * edge and validity rules of strata_process per raster. strata_batch_create
+ * checks every item as strata_process would, groups the rasters by op
+ * class, uploads their descriptors and captures one persistent kernel per
+ * class into a CUDA graph; strata_batch_run replays it with one launch
+ * (synchronize != 0 waits for it). tile_width / tile_height pick an item's
+ * output tile (0 = 64 x 32); the Python autotuner chooses them per class.
+ * The rasters must stay allocated, and the batch be run on one stream at a
+ * time, until strata_batch_destroy.
+ */
+typedef struct {
+    const strata_stage *stages;
+    int32_t nstages;
+    int32_t tile_width, tile_height;
+    int32_t reserved;
+    strata_raster src;
+    strata_raster dst[2];
+} strata_batch_item;
+
+typedef struct strata_batch strata_batch;
+
+int strata_batch_create(strata_ctx *ctx, const strata_batch_item *items, int nitems, strata_batch **out);
+int strata_batch_run(strata_batch *batch, void *stream, int synchronize);
+/* Adds the batch's Stats (as one call would count them) and reports its op classes. */
+int strata_batch_info(const strata_batch *batch, strata_stats *stats, int *classes);
+void strata_batch_destroy(strata_batch *batch);
+
 /* ---------------------------------------------------------------------- */
 /* Stage builders: option resolution and checks of the typed entry points. */
 

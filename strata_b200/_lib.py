@@ -60,6 +60,11 @@ class Sink(ctypes.Structure):
                 ("user", c_p), ("write", WRITE_FN)]
 
 
+class BatchItem(ctypes.Structure):
+    _fields_ = [("stages", ctypes.POINTER(Stage)), ("nstages", c_i32), ("tile_width", c_i32),
+                ("tile_height", c_i32), ("reserved", c_i32), ("src", Raster), ("dst", Raster * 2)]
+
+
 class GradientOptions(ctypes.Structure):
     _fields_ = [("cell_size", c_f64), ("cell_size_y", c_f64), ("z_factor", c_f64),
                 ("fit_radius", c_i32), ("reserved", c_i32)]
@@ -123,6 +128,10 @@ SIGNATURES = [
     ("strata_process_chunked", ctypes.c_int, [c_p, ctypes.POINTER(Stage), ctypes.c_int, ctypes.POINTER(Source),
                                               ctypes.c_int, ctypes.POINTER(Sink), ctypes.c_int,
                                               ctypes.POINTER(ExecOpts), ctypes.POINTER(Stats)]),
+    ("strata_batch_create", ctypes.c_int, [c_p, ctypes.POINTER(BatchItem), ctypes.c_int, ctypes.POINTER(c_p)]),
+    ("strata_batch_run", ctypes.c_int, [c_p, c_p, ctypes.c_int]),
+    ("strata_batch_info", ctypes.c_int, [c_p, ctypes.POINTER(Stats), ctypes.POINTER(ctypes.c_int)]),
+    ("strata_batch_destroy", None, [c_p]),
     ("strata_stage_gradient", ctypes.c_int, [ctypes.POINTER(GradientOptions), ctypes.POINTER(Stage)]),
     ("strata_stage_slope", ctypes.c_int, [ctypes.POINTER(SlopeOptions), ctypes.POINTER(Stage)]),
     ("strata_stage_aspect", ctypes.c_int, [ctypes.POINTER(AspectOptions), ctypes.POINTER(Stage)]),

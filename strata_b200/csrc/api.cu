@@ -1456,3 +1456,186 @@ extern "C" int strata_process_features(strata_ctx* c, const strata_stage* stages
     }
     return STRATA_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Batches: many device-resident rasters of mixed sizes and ops, planned
+// once (descriptors uploaded, one persistent kernel per op class captured
+// in a CUDA graph) and run with one graph launch.
+
+struct strata_batch {
+    strata_ctx* ctx = nullptr;
+    strata::BatchItem* d_items = nullptr;  // the descriptors, on the device
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int classes = 0;
+    int64_t tiles = 0, cells = 0, window = 0;
+    int64_t out_cells = 0, in_bytes = 0, out_bytes = 0;
+};
+
+extern "C" int strata_batch_create(strata_ctx* c, const strata_batch_item* items, int nitems, strata_batch** out) {
+    if (!c || !out) return fail(STRATA_EINVAL, "engine: nil context");
+    *out = nullptr;
+    if (nitems < 1 || !items) return fail(STRATA_EINVAL, "engine: a batch needs at least one raster");
+    std::lock_guard<std::mutex> lock(c->mu);
+    cudaSetDevice(c->device);
+    std::vector<strata::BatchItem> host((size_t)nitems);
+    std::vector<std::pair<std::pair<int, int>, int>> keyed;  // ((op, radius), item)
+    int64_t cells = 0, in_bytes = 0, out_bytes = 0;
+    for (int i = 0; i < nitems; i++) {
+        const strata_batch_item& it = items[i];
+        LaunchParams p;
+        int nout = 0, rc;
+        if ((rc = plan_stages(it.stages, it.nstages, p, &nout))) return rc;
+        if ((rc = check_operands(&it.src, 1, it.dst, nout, nout, p.radius))) return rc;
+        if (!it.src.on_device || !it.dst[0].on_device || (nout > 1 && !it.dst[1].on_device))
+            return fail(STRATA_EINVAL, "engine: batch raster %d: the rasters of a batch must be on the device", i);
+        if (p.op == STRATA_OP_LOOKUP || p.op == STRATA_OP_RECLASS)
+            return fail(STRATA_ENOTSUP, "engine: batch raster %d: a pointwise op alone has no batch kernel", i);
+        DevOperand ds, dd[2];
+        if ((rc = stage_in(c, nullptr, it.src, 0, false, &ds))) return rc;
+        for (int k = 0; k < nout; k++)
+            if ((rc = stage_in(c, nullptr, it.dst[k], 0, false, &dd[k]))) return rc;
+        const int64_t W = it.src.width, H = it.src.height;
+        p.src = ds.data;
+        p.src_stride = ds.stride;
+        p.src_x0 = p.src_y0 = 0;
+        p.src_w = W;
+        p.src_h = H;
+        p.dst0 = dd[0].data;
+        p.dst0_stride = dd[0].stride;
+        if (nout > 1) {
+            p.dst1 = dd[1].data;
+            p.dst1_stride = dd[1].stride;
+        }
+        p.dst_x0 = p.dst_y0 = 0;
+        p.width = W;
+        p.height = H;
+        p.out_x0 = p.out_y0 = 0;
+        p.out_x1 = W;
+        p.out_y1 = H;
+        p.status = c->d_status;
+        strata::BatchItem& b = host[(size_t)i];
+        memset(&b, 0, sizeof b);
+        b.p = p;
+        for (int k = 0; k < nout; k++) {
+            if (!it.dst[k].valid) continue;
+            fill_validity(b.v[b.nvalid], ds, it.src.valid != nullptr, dd[k], span_cells(it.dst[k]), W, H, p.radius, 0,
+                          H);
+            b.nvalid++;
+        }
+        b.tw = it.tile_width > 0 ? it.tile_width : 64;
+        b.th = it.tile_height > 0 ? it.tile_height : 32;
+        if (b.tw > 1024 || b.th > 1024 || strata::batch_smem_bytes(p.op, p.radius, b.tw, b.th) > 200 * 1024)
+            return fail(STRATA_EINVAL, "engine: batch raster %d: tile %d x %d is too large", i, b.tw, b.th);
+        b.tiles_x = (W + b.tw - 1) / b.tw;
+        keyed.push_back({{p.op, p.radius}, i});
+        cells += W * H;
+        in_bytes += W * H * 4;
+        out_bytes += W * H * 4 * nout;
+    }
+    // Group by class; each class's rasters get consecutive work units.
+    std::stable_sort(keyed.begin(), keyed.end(),
+                     [](const auto& a, const auto& b) { return a.first < b.first; });
+    std::vector<strata::BatchItem> ordered;
+    ordered.reserve((size_t)nitems);
+    struct Class {
+        int op, radius;
+        int first, count;
+        int64_t total;
+        size_t smem;
+    };
+    std::vector<Class> classes;
+    int64_t window = 0;
+    for (size_t i = 0; i < keyed.size();) {
+        Class cl{keyed[i].first.first, keyed[i].first.second, (int)ordered.size(), 0, 0, 0};
+        for (; i < keyed.size() && keyed[i].first == std::make_pair(cl.op, cl.radius); i++) {
+            strata::BatchItem b = host[(size_t)keyed[i].second];
+            const int64_t ty = (b.p.height + b.th - 1) / b.th;
+            b.tile0 = cl.total;
+            cl.total += b.tiles_x * ty;
+            cl.smem = std::max(cl.smem, strata::batch_smem_bytes(cl.op, cl.radius, b.tw, b.th));
+            window += (int64_t)(b.tw + 2 * cl.radius) * (b.th + 2 * cl.radius) * b.tiles_x * ty;
+            ordered.push_back(b);
+            cl.count++;
+        }
+        classes.push_back(cl);
+    }
+    auto* B = new strata_batch;
+    B->ctx = c;
+    B->classes = (int)classes.size();
+    B->cells = cells;
+    B->in_bytes = in_bytes;
+    B->out_bytes = out_bytes;
+    B->window = window;
+    cudaError_t e = cudaMalloc(&B->d_items, sizeof(strata::BatchItem) * ordered.size());
+    if (e == cudaSuccess)
+        e = cudaMemcpy(B->d_items, ordered.data(), sizeof(strata::BatchItem) * ordered.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        strata_batch_destroy(B);
+        return cuda_fail(e, "batch descriptors");
+    }
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+    // Capture every class's persistent kernel into one graph.
+    cudaStream_t cap;
+    if ((e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking)) != cudaSuccess) {
+        strata_batch_destroy(B);
+        return cuda_fail(e, "capture stream");
+    }
+    e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+    bool ok = e == cudaSuccess;
+    for (const Class& cl : classes) {
+        if (!ok) break;
+        // Enough blocks to fill the GPU at the class's occupancy, never
+        // more than its work units.
+        const int per_sm = cl.smem > 100 * 1024 ? 1 : (cl.smem > 48 * 1024 ? 2 : 4);
+        const int64_t grid = std::min<int64_t>(cl.total, (int64_t)sms * per_sm);
+        B->tiles += cl.total;
+        ok = strata::launch_batch_class(cl.op, cl.radius, B->d_items + cl.first, cl.count, cl.total, (int)grid,
+                                        cl.smem, cap);
+    }
+    cudaError_t e2 = cudaStreamEndCapture(cap, &B->graph);
+    if (ok && e2 == cudaSuccess) e2 = cudaGraphInstantiate(&B->exec, B->graph, 0);
+    cudaStreamDestroy(cap);
+    if (!ok || e2 != cudaSuccess) {
+        cudaGetLastError();
+        strata_batch_destroy(B);
+        return ok ? cuda_fail(e2, "batch graph") : fail(STRATA_ENOTSUP, "engine: an op of the batch has no batch kernel");
+    }
+    B->tiles = 0;
+    for (const Class& cl : classes) B->tiles += cl.total;
+    *out = B;
+    return STRATA_OK;
+}
+
+extern "C" int strata_batch_run(strata_batch* B, void* stream, int synchronize) {
+    if (!B) return fail(STRATA_EINVAL, "engine: nil batch");
+    cudaSetDevice(B->ctx->device);
+    cudaStream_t st = stream ? (cudaStream_t)stream : B->ctx->stream;
+    cudaError_t e = cudaGraphLaunch(B->exec, st);
+    if (e != cudaSuccess) return cuda_fail(e, "batch launch");
+    if (synchronize) return take_status(B->ctx, st);
+    return STRATA_OK;
+}
+
+extern "C" int strata_batch_info(const strata_batch* B, strata_stats* stats, int* classes) {
+    if (!B) return fail(STRATA_EINVAL, "engine: nil batch");
+    if (classes) *classes = B->classes;
+    if (stats) {
+        stats->cells += B->cells;
+        stats->ideal += B->in_bytes + B->out_bytes;
+        stats->bands += B->tiles;
+        stats->kernel_read += B->window * 4;
+        stats->kernel_written += B->out_bytes;
+    }
+    return STRATA_OK;
+}
+
+extern "C" void strata_batch_destroy(strata_batch* B) {
+    if (!B) return;
+    cudaSetDevice(B->ctx->device);
+    if (B->exec) cudaGraphExecDestroy(B->exec);
+    if (B->graph) cudaGraphDestroy(B->graph);
+    if (B->d_items) cudaFree(B->d_items);
+    delete B;
+}

@@ -12,8 +12,10 @@
 // bits over each cell's window (internal/stencil/mask.go:43-161), with
 // every other bit of the word preserved.
 #include "cellops.cuh"
+#include "focalops.cuh"
 #include "launch.h"
 #include "ops3.cuh"
+#include "validity.cuh"
 
 namespace strata {
 namespace {
@@ -27,107 +29,6 @@ constexpr int kCX = 2;
 constexpr int kCY = 4;
 constexpr int kTW = kThreadsX * kCX;  // tile width in cells
 constexpr int kTH = kThreadsY * kCY;  // tile height in cells
-
-// RuggednessWindowRow for radius R > 1 (internal/stencil/rugged.go:152-210):
-// Riley, Wilson and TPI over the window in row-major order without the
-// centre. c points at the centre cell.
-template <int R>
-__device__ __forceinline__ float rugged_window(const float* c, int s, int kind) {
-    constexpr int D = 2 * R + 1;
-    constexpr float n = (float)(D * D - 1);
-    const float z = c[0];
-    const float* q = c - R * s - R;
-    if (kind == 0) {
-        double a = 0.0;
-#pragma unroll
-        for (int j = 0; j < D; j++)
-#pragma unroll
-            for (int k = 0; k < D; k++)
-                if (!(j == R && k == R)) a = __dadd_rn(a, sq64(sub(q[j * s + k], z)));
-        return __double2float_rn(__dsqrt_rn(a));
-    }
-    if (kind == 1) {
-        float a = 0.0f;
-#pragma unroll
-        for (int j = 0; j < D; j++)
-#pragma unroll
-            for (int k = 0; k < D; k++)
-                if (!(j == R && k == R)) a = add(a, abs32(sub(q[j * s + k], z)));
-        return div(a, n);
-    }
-    float a = q[0];  // TPI folds from the first neighbour's value
-#pragma unroll
-    for (int j = 0; j < D; j++)
-#pragma unroll
-        for (int k = 0; k < D; k++)
-            if (!(j == R && k == R) && !(j == 0 && k == 0)) a = add(a, q[j * s + k]);
-    return sub(z, div(a, n));
-}
-
-// CorrelateRow (internal/focalrow/focalrow.go:217-230): the first product,
-// then every later product added in row-major order of the weights.
-template <int R>
-__device__ __forceinline__ float correlate(const LaunchParams& P, const float* c, int s) {
-    constexpr int D = 2 * R + 1;
-    const float* q = c - R * s - R;
-    float acc = mul(P.w[0], q[0]);
-#pragma unroll
-    for (int j = 0; j < D; j++)
-#pragma unroll
-        for (int k = 0; k < D; k++)
-            if (j | k) acc = add(acc, mul(P.w[j * D + k], q[j * s + k]));
-    return acc;
-}
-
-// Column folds of the separable ops (focalrow.go:232-272): the 2R+1 cells
-// of a column, top to bottom.
-template <int OP, int R>
-__device__ __forceinline__ float column_fold(const LaunchParams& P, const float* top, int s) {
-    constexpr int D = 2 * R + 1;
-    float a;
-    if constexpr (OP == STRATA_OP_SEPARABLE) {
-        a = mul(P.w[17], top[0]);
-#pragma unroll
-        for (int j = 1; j < D; j++) a = add(a, mul(P.w[17 + j], top[j * s]));
-    } else {
-        a = top[0];
-#pragma unroll
-        for (int j = 1; j < D; j++) {
-            float v = top[j * s];
-            if constexpr (OP == STRATA_OP_MEAN) a = add(a, v);
-            else if constexpr (OP == STRATA_OP_MIN) a = go_min(a, v);
-            else a = go_max(a, v);
-        }
-    }
-    return a;
-}
-
-// Row folds (focalrow.go:274-315) of 2R+1 column results, left to right;
-// the mean divides by (2R+1)^2 at the end (divRow, focalrow.go:406-421).
-template <int OP, int R>
-__device__ __forceinline__ float row_fold(const LaunchParams& P, const float* left) {
-    constexpr int D = 2 * R + 1;
-    float a;
-    if constexpr (OP == STRATA_OP_SEPARABLE) {
-        a = mul(P.w[0], left[0]);
-#pragma unroll
-        for (int c = 1; c < D; c++) a = add(a, mul(P.w[c], left[c]));
-    } else {
-        a = left[0];
-#pragma unroll
-        for (int c = 1; c < D; c++) {
-            if constexpr (OP == STRATA_OP_MEAN) a = add(a, left[c]);
-            else if constexpr (OP == STRATA_OP_MIN) a = go_min(a, left[c]);
-            else a = go_max(a, left[c]);
-        }
-        if constexpr (OP == STRATA_OP_MEAN) a = div(a, (float)(D * D));
-    }
-    return a;
-}
-
-template <int OP, int R>
-constexpr bool kTwoPass = OP == STRATA_OP_SEPARABLE || OP == STRATA_OP_MEAN || OP == STRATA_OP_MIN ||
-                          OP == STRATA_OP_MAX;
 
 // The general tile kernel: every op at every radius, any alignment and
 // stride. Tile kTW x kTH output cells; thread (tx, ty) computes cells
@@ -224,45 +125,6 @@ __global__ void __launch_bounds__(256) pointwise_kernel(const __grid_constant__ 
 // ---------------------------------------------------------------------------
 // Validity.
 
-__device__ __forceinline__ int64_t min64(int64_t a, int64_t b) { return a < b ? a : b; }
-
-__device__ __forceinline__ int64_t floor_div32(int64_t b) { return b >= 0 ? b >> 5 : -((-b + 31) >> 5); }
-
-// 64 bits of the source mask from bit b on (b may be negative), with zeros
-// for words outside [lo, hi].
-__device__ __forceinline__ uint64_t bits64(const ValidityParams& v, int64_t b) {
-    const int64_t w = floor_div32(b);
-    const int sh = (int)(b - w * 32);
-    const uint32_t* m = v.src_bits;
-    const uint64_t a0 = (w >= v.src_lo_word && w <= v.src_hi_word) ? m[w] : 0u;
-    const uint64_t a1 = (w + 1 >= v.src_lo_word && w + 1 <= v.src_hi_word) ? m[w + 1] : 0u;
-    const uint64_t a2 = (w + 2 >= v.src_lo_word && w + 2 <= v.src_hi_word) ? m[w + 2] : 0u;
-    uint64_t lo = a0 | (a1 << 32);
-    if (sh == 0) return lo;
-    return (lo >> sh) | (a2 << (64 - sh));
-}
-
-// Output bits of global cells (x .. x+31, y), bit j for cell x + j.
-__device__ __forceinline__ uint32_t segment_bits(const ValidityParams& v, int64_t x, int64_t y) {
-    const int r = v.radius;
-    const int64_t W = v.width, H = v.height;
-    if (r > 0 && (y < r || y >= H - r)) return 0u;
-    uint32_t interior = 0xffffffffu;
-    if (r > 0) {
-        // bits j of cells x + j with r <= x + j < W - r: j in [lo, hi)
-        const int64_t lo = r - x, hi = W - r - x;
-        const uint32_t mlo = lo <= 0 ? 0xffffffffu : (lo >= 32 ? 0u : ~((1u << lo) - 1u));
-        const uint32_t mhi = hi >= 32 ? 0xffffffffu : (hi <= 0 ? 0u : ((1u << hi) - 1u));
-        interior = mlo & mhi;
-    }
-    if (!v.src_bits) return interior;
-    uint64_t acc = ~0ull;
-    const int64_t bx = x - r - v.src_x0;
-    for (int j = -r; j <= r; j++) acc &= bits64(v, v.src_off + (y + j - v.src_y0) * v.src_stride + bx);
-    uint64_t e = acc;
-    for (int d = 1; d <= 2 * r; d++) e &= acc >> d;
-    return (uint32_t)e & interior;
-}
 
 __global__ void __launch_bounds__(256) validity_kernel(const __grid_constant__ ValidityParams v) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;

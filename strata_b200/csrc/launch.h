@@ -31,7 +31,7 @@ struct EpiStage {
 // the output region [out_x0, out_x1) x [out_y0, out_y1). A plain call has
 // every offset 0 and the region the whole raster; a chunked tile or a row
 // strip sets them.
-struct LaunchParams {
+struct alignas(16) LaunchParams {
     const float* src;
     int64_t src_stride;
     int64_t src_x0, src_y0, src_w, src_h;
@@ -60,7 +60,7 @@ struct LaunchParams {
 // Coordinates as in LaunchParams: the source mask's cell (0, 0) is global
 // cell (src_x0, src_y0), the destination's is (dst_x0, dst_y0), and only
 // bits of cells in the region [out_x0, out_x1) x [out_y0, out_y1) change.
-struct ValidityParams {
+struct alignas(16) ValidityParams {
     const uint32_t* src_bits;  // the source mask as 32-bit words
     int64_t src_off;           // bit offset of the source's cell (0, 0)
     int64_t src_stride;
@@ -76,6 +76,27 @@ struct ValidityParams {
     int64_t width, height;
     int radius;
 };
+
+// One raster of a batch (batch.cu): its launch parameters, the validity
+// of its masked outputs, and where its work units (tiles of tw x th
+// output cells, tiles_x across) start among its class's.
+struct alignas(16) BatchItem {
+    LaunchParams p;
+    ValidityParams v[2];
+    int64_t tile0;
+    int64_t tiles_x;
+    int tw, th;
+    int nvalid;  // masked outputs: v[0 .. nvalid)
+    int pad;
+};
+
+// Shared memory a batch kernel block needs for a tw x th tile of this op.
+size_t batch_smem_bytes(int op, int radius, int tw, int th);
+// Launches the persistent kernel of one op class over items[0 .. nitems)
+// (device memory), total work units, on grid blocks. False if the op has
+// no batch kernel.
+bool launch_batch_class(int op, int radius, const BatchItem* items, int nitems, int64_t total, int grid, size_t smem,
+                        cudaStream_t stream);
 
 // Launches the data kernel of stages (the first any op, the rest pointwise
 // epilogues) over whole rasters. Returns the number of thread-block tiles
