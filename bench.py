@@ -455,7 +455,7 @@ def run_batch(args, rank, world, local_rank):
         plain_step()
     torch.cuda.synchronize()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    stream = torch.cuda.current_stream(dev)
+    stream = torch.cuda.Stream(dev)  # the graph runs on this stream, which the events time
     with Clocks(local_rank) as clk:
         start.record(stream)
         for _ in range(args.steps):

@@ -259,6 +259,46 @@ int strata_batch_run(strata_batch *batch, void *stream, int synchronize);
 int strata_batch_info(const strata_batch *batch, strata_stats *stats, int *classes);
 void strata_batch_destroy(strata_batch *batch);
 
+/*
+ * Serving (no counterpart call in strata, which serves no requests): window
+ * requests over a device-resident mosaic, run with continuous batching. A
+ * scheduler thread takes queued requests whenever one of `streams` streams
+ * is free, admits them in arrival order while their outputs fit in
+ * budget_bytes, and launches them as one batch (up to max_batch requests);
+ * batches on different streams overlap, and requests that arrive while
+ * others run join the next batch. A request is one pipeline (as in
+ * strata_process) over the w x h window of the mosaic at (x, y), which is
+ * a raster of its own (its border is its edge ring), with the window's
+ * validity bits when the mosaic has a mask. Its outputs live in device
+ * memory the server allocates; strata_server_wait returns them and the
+ * request's submit / start / done times (steady clock, ns), and
+ * strata_server_release frees them and their budget.
+ */
+typedef struct {
+    int64_t budget_bytes; /* 0 = 120 GiB */
+    int32_t streams;      /* 0 = 4 */
+    int32_t max_batch;    /* 0 = 64 */
+} strata_server_opts;
+
+typedef struct {
+    int32_t status; /* 0 done, < 0 a STRATA_E* code */
+    int32_t nout;
+    strata_raster out[2];
+    int64_t t_submit_ns, t_start_ns, t_done_ns;
+} strata_server_result;
+
+typedef struct strata_server strata_server;
+
+int strata_server_create(strata_ctx *ctx, const strata_raster *mosaic, const strata_server_opts *opts,
+                         strata_server **out);
+int strata_server_submit(strata_server *srv, const strata_stage *stages, int nstages, int64_t x, int64_t y,
+                         int64_t w, int64_t h, uint64_t *ticket);
+/* Waits up to timeout_ms (< 0: without limit) for a request; STRATA_ETIMEDOUT if it is not done by then. */
+int strata_server_wait(strata_server *srv, uint64_t ticket, int64_t timeout_ms, strata_server_result *result);
+int strata_server_release(strata_server *srv, uint64_t ticket);
+int strata_server_stats(strata_server *srv, int64_t *batches, int64_t *served, int64_t *used_bytes);
+void strata_server_destroy(strata_server *srv);
+
 /* ---------------------------------------------------------------------- */
 /* Stage builders: option resolution and checks of the typed entry points. */
 

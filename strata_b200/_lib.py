@@ -65,6 +65,15 @@ class BatchItem(ctypes.Structure):
                 ("tile_height", c_i32), ("reserved", c_i32), ("src", Raster), ("dst", Raster * 2)]
 
 
+class ServerOpts(ctypes.Structure):
+    _fields_ = [("budget_bytes", c_i64), ("streams", c_i32), ("max_batch", c_i32)]
+
+
+class ServerResult(ctypes.Structure):
+    _fields_ = [("status", c_i32), ("nout", c_i32), ("out", Raster * 2), ("t_submit_ns", c_i64),
+                ("t_start_ns", c_i64), ("t_done_ns", c_i64)]
+
+
 class GradientOptions(ctypes.Structure):
     _fields_ = [("cell_size", c_f64), ("cell_size_y", c_f64), ("z_factor", c_f64),
                 ("fit_radius", c_i32), ("reserved", c_i32)]
@@ -132,6 +141,15 @@ SIGNATURES = [
     ("strata_batch_run", ctypes.c_int, [c_p, c_p, ctypes.c_int]),
     ("strata_batch_info", ctypes.c_int, [c_p, ctypes.POINTER(Stats), ctypes.POINTER(ctypes.c_int)]),
     ("strata_batch_destroy", None, [c_p]),
+    ("strata_server_create", ctypes.c_int, [c_p, ctypes.POINTER(Raster), ctypes.POINTER(ServerOpts),
+                                            ctypes.POINTER(c_p)]),
+    ("strata_server_submit", ctypes.c_int, [c_p, ctypes.POINTER(Stage), ctypes.c_int, c_i64, c_i64, c_i64, c_i64,
+                                            ctypes.POINTER(ctypes.c_uint64)]),
+    ("strata_server_wait", ctypes.c_int, [c_p, ctypes.c_uint64, c_i64, ctypes.POINTER(ServerResult)]),
+    ("strata_server_release", ctypes.c_int, [c_p, ctypes.c_uint64]),
+    ("strata_server_stats", ctypes.c_int, [c_p, ctypes.POINTER(c_i64), ctypes.POINTER(c_i64),
+                                           ctypes.POINTER(c_i64)]),
+    ("strata_server_destroy", None, [c_p]),
     ("strata_stage_gradient", ctypes.c_int, [ctypes.POINTER(GradientOptions), ctypes.POINTER(Stage)]),
     ("strata_stage_slope", ctypes.c_int, [ctypes.POINTER(SlopeOptions), ctypes.POINTER(Stage)]),
     ("strata_stage_aspect", ctypes.c_int, [ctypes.POINTER(AspectOptions), ctypes.POINTER(Stage)]),

@@ -1639,3 +1639,391 @@ extern "C" void strata_batch_destroy(strata_batch* B) {
     if (B->d_items) cudaFree(B->d_items);
     delete B;
 }
+
+// ---------------------------------------------------------------------------
+// Serving: window requests over a resident mosaic, admitted under a memory
+// budget and batched as they arrive (continuous batching). A scheduler
+// thread takes the queued requests whenever one of its streams is free,
+// admits them in arrival order while their outputs fit the budget, and
+// launches them as one batch (one persistent kernel per op class) on that
+// stream; batches on different streams overlap on the device, and a
+// request that arrives while others run joins the next batch. Outputs are
+// allocated from a stream-ordered pool and count against the budget until
+// released.
+
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <thread>
+#include <unordered_map>
+
+namespace {
+
+int64_t now_ns() {
+    return std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now().time_since_epoch())
+        .count();
+}
+
+struct Request {
+    uint64_t ticket = 0;
+    int64_t x = 0, y = 0, w = 0, h = 0;
+    std::vector<strata_stage> stages;
+    std::vector<std::vector<float>> tables;  // copies of the stages' tables
+    LaunchParams p;
+    int nout = 0;
+    int status = 1;  // 1 queued, 2 running, 0 done, < 0 failed
+    float* out[2] = {nullptr, nullptr};
+    uint32_t* out_bits[2] = {nullptr, nullptr};
+    size_t bytes = 0;  // budget charge
+    int64_t t_submit = 0, t_start = 0, t_done = 0;
+};
+
+struct Slot {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    strata::BatchItem* d_items = nullptr;
+    strata::BatchItem* h_items = nullptr;  // page-locked staging
+    std::vector<Request*> reqs;
+    bool busy = false;
+};
+
+}  // namespace
+
+struct strata_server {
+    strata_ctx* ctx = nullptr;
+    strata_raster mosaic{};
+    DevOperand dm;
+    size_t budget = 0, used = 0;
+    int max_batch = 64;
+    std::vector<Slot> slots;
+    std::mutex mu;
+    std::condition_variable cv;       // the scheduler waits here
+    std::condition_variable done_cv;  // callers waiting for results
+    std::deque<Request*> queue;
+    std::unordered_map<uint64_t, Request*> all;
+    uint64_t next_ticket = 1;
+    bool stop = false;
+    std::thread thread;
+    cudaMemPool_t pool = nullptr;
+    int sms = 148;
+    int64_t batches = 0, served = 0;
+};
+
+namespace {
+
+// Launches one batch of admitted requests on slot s (scheduler thread,
+// with the server lock held).
+int launch_batch(strata_server* S, Slot& s) {
+    cudaStream_t st = s.stream;
+    std::vector<std::pair<std::pair<int, int>, int>> keyed;
+    for (int i = 0; i < (int)s.reqs.size(); i++) keyed.push_back({{s.reqs[i]->p.op, s.reqs[i]->p.radius}, i});
+    std::stable_sort(keyed.begin(), keyed.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+    struct Class {
+        int op, radius, first, count;
+        int64_t total;
+        size_t smem;
+    };
+    std::vector<Class> classes;
+    int n = 0;
+    for (size_t i = 0; i < keyed.size();) {
+        Class cl{keyed[i].first.first, keyed[i].first.second, n, 0, 0, 0};
+        for (; i < keyed.size() && keyed[i].first == std::make_pair(cl.op, cl.radius); i++) {
+            Request* r = s.reqs[(size_t)keyed[i].second];
+            strata::BatchItem& b = s.h_items[n++];
+            memset(&b, 0, sizeof b);
+            b.p = r->p;
+            b.tw = 64;
+            b.th = 32;
+            b.tiles_x = (r->w + b.tw - 1) / b.tw;
+            b.tile0 = cl.total;
+            cl.total += b.tiles_x * ((r->h + b.th - 1) / b.th);
+            for (int k = 0; k < r->nout; k++) {
+                if (!r->out_bits[k]) continue;
+                ValidityParams& v = b.v[b.nvalid++];
+                memset(&v, 0, sizeof v);
+                if (S->mosaic.valid) {
+                    v.src_bits = S->dm.bits;
+                    v.src_off = S->dm.bit_off + r->y * S->dm.stride + r->x;
+                    v.src_stride = S->dm.stride;
+                    v.src_lo_word = S->dm.lo_word;
+                    v.src_hi_word = S->dm.hi_word;
+                }
+                v.dst_bits = r->out_bits[k];
+                v.dst_off = 0;
+                v.dst_stride = r->w;
+                v.out_x1 = r->w;
+                v.out_y1 = r->h;
+                v.width = r->w;
+                v.height = r->h;
+                v.radius = r->p.radius;
+                v.dst_words = (r->w * r->h + 31) / 32;
+            }
+            cl.smem = std::max(cl.smem, strata::batch_smem_bytes(cl.op, cl.radius, b.tw, b.th));
+            cl.count++;
+        }
+        classes.push_back(cl);
+    }
+    cudaError_t e = cudaMemcpyAsync(s.d_items, s.h_items, sizeof(strata::BatchItem) * (size_t)n,
+                                    cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return cuda_fail(e, "serve descriptors");
+    for (const Class& cl : classes) {
+        const int per_sm = cl.smem > 48 * 1024 ? 2 : 4;
+        const int64_t grid = std::min<int64_t>(cl.total, (int64_t)S->sms * per_sm);
+        if (!strata::launch_batch_class(cl.op, cl.radius, s.d_items + cl.first, cl.count, cl.total, (int)grid, cl.smem,
+                                        st))
+            return fail(STRATA_ENOTSUP, "engine: an op of the request has no batch kernel");
+    }
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaEventRecord(s.done, st);
+    if (e != cudaSuccess) return cuda_fail(e, "serve launch");
+    return STRATA_OK;
+}
+
+void scheduler(strata_server* S) {
+    cudaSetDevice(S->ctx->device);
+    std::unique_lock<std::mutex> lk(S->mu);
+    while (!S->stop) {
+        bool progressed = false;
+        // Retire finished batches.
+        for (Slot& s : S->slots) {
+            if (!s.busy) continue;
+            cudaError_t q = cudaEventQuery(s.done);
+            if (q == cudaErrorNotReady) continue;
+            const int64_t t = now_ns();
+            for (Request* r : s.reqs) {
+                r->status = q == cudaSuccess ? 0 : STRATA_ECUDA;
+                r->t_done = t;
+            }
+            S->served += (int64_t)s.reqs.size();
+            s.reqs.clear();
+            s.busy = false;
+            progressed = true;
+            S->done_cv.notify_all();
+        }
+        // Admit queued requests onto a free stream, in arrival order, while
+        // their outputs fit the budget.
+        for (Slot& s : S->slots) {
+            if (s.busy || S->queue.empty()) continue;
+            while (!S->queue.empty() && (int)s.reqs.size() < S->max_batch) {
+                Request* r = S->queue.front();
+                if (S->used + r->bytes > S->budget && !(S->used == 0 && s.reqs.empty())) break;
+                // Outputs from the stream-ordered pool.
+                bool ok = true;
+                for (int k = 0; k < r->nout && ok; k++) {
+                    ok = cudaMallocFromPoolAsync((void**)&r->out[k], (size_t)(r->w * r->h) * 4, S->pool, s.stream) ==
+                         cudaSuccess;
+                    if (ok && S->mosaic.valid)
+                        ok = cudaMallocFromPoolAsync((void**)&r->out_bits[k], (size_t)((r->w * r->h + 63) / 64) * 8,
+                                                     S->pool, s.stream) == cudaSuccess;
+                }
+                if (!ok) {
+                    cudaGetLastError();
+                    break;
+                }
+                S->queue.pop_front();
+                S->used += r->bytes;
+                r->p.dst0 = r->out[0];
+                r->p.dst0_stride = r->w;
+                r->p.dst1 = r->out[1];
+                r->p.dst1_stride = r->w;
+                r->status = 2;
+                r->t_start = now_ns();
+                s.reqs.push_back(r);
+            }
+            if (s.reqs.empty()) break;  // the budget holds even one request back
+            int rc = launch_batch(S, s);
+            if (rc != STRATA_OK) {
+                for (Request* r : s.reqs) {
+                    r->status = rc;
+                    r->t_done = now_ns();
+                }
+                s.reqs.clear();
+                S->done_cv.notify_all();
+                continue;
+            }
+            s.busy = true;
+            S->batches++;
+            progressed = true;
+        }
+        if (!progressed) {
+            bool any_busy = false;
+            for (Slot& s : S->slots) any_busy = any_busy || s.busy;
+            // Poll running batches often; sleep until work arrives otherwise.
+            if (any_busy) S->cv.wait_for(lk, std::chrono::microseconds(20));
+            else S->cv.wait_for(lk, std::chrono::milliseconds(5));
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" int strata_server_create(strata_ctx* c, const strata_raster* mosaic, const strata_server_opts* o,
+                                    strata_server** out) {
+    if (!c || !mosaic || !out) return fail(STRATA_EINVAL, "engine: nil argument");
+    *out = nullptr;
+    int rc = validate("src", 0, *mosaic);
+    if (rc) return rc;
+    if (!mosaic->on_device) return fail(STRATA_EINVAL, "engine: the served mosaic must be on the device");
+    auto* S = new strata_server;
+    S->ctx = c;
+    S->mosaic = *mosaic;
+    S->budget = o && o->budget_bytes ? (size_t)o->budget_bytes : (size_t)120 << 30;
+    S->max_batch = o && o->max_batch > 0 ? o->max_batch : 64;
+    const int nstreams = o && o->streams > 0 ? o->streams : 4;
+    cudaSetDevice(c->device);
+    cudaDeviceGetAttribute(&S->sms, cudaDevAttrMultiProcessorCount, c->device);
+    if ((rc = stage_in(c, nullptr, *mosaic, 0, false, &S->dm))) {
+        delete S;
+        return rc;
+    }
+    cudaError_t e = cudaDeviceGetDefaultMemPool(&S->pool, c->device);
+    S->slots.resize((size_t)nstreams);
+    for (Slot& s : S->slots) {
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaMalloc(&s.d_items, sizeof(strata::BatchItem) * (size_t)S->max_batch);
+        if (e == cudaSuccess)
+            e = cudaHostAlloc(&s.h_items, sizeof(strata::BatchItem) * (size_t)S->max_batch, cudaHostAllocDefault);
+    }
+    if (e != cudaSuccess) {
+        strata_server_destroy(S);
+        return cuda_fail(e, "server set-up");
+    }
+    S->thread = std::thread(scheduler, S);
+    *out = S;
+    return STRATA_OK;
+}
+
+extern "C" int strata_server_submit(strata_server* S, const strata_stage* stages, int nstages, int64_t x, int64_t y,
+                                    int64_t w, int64_t h, uint64_t* ticket) {
+    if (!S || !ticket) return fail(STRATA_EINVAL, "engine: nil server");
+    const strata_raster& M = S->mosaic;
+    if (w <= 0 || h <= 0 || x < 0 || y < 0 || x + w > M.width || y + h > M.height)
+        return fail(STRATA_EINVAL, "raster: window %lld×%lld at (%lld, %lld) outside %lld×%lld raster", (long long)w,
+                    (long long)h, (long long)x, (long long)y, (long long)M.width, (long long)M.height);
+    auto* r = new Request;
+    r->x = x;
+    r->y = y;
+    r->w = w;
+    r->h = h;
+    // Keep the stages and their tables: the caller's may go away.
+    r->stages.assign(stages, stages + (nstages > 0 ? nstages : 0));
+    for (auto& st : r->stages)
+        for (int k = 0; k < 4; k++)
+            if (st.table[k] && st.table_len[k] > 0) {
+                int n = st.table_len[k] + (st.op == STRATA_OP_RECLASS && k == 1 ? 0 : 0);
+                r->tables.emplace_back(st.table[k], st.table[k] + n);
+                st.table[k] = r->tables.back().data();
+            }
+    int rc = plan_stages(r->stages.data(), (int)r->stages.size(), r->p, &r->nout);
+    if (rc == STRATA_OK && (r->p.op == STRATA_OP_LOOKUP || r->p.op == STRATA_OP_RECLASS))
+        rc = fail(STRATA_ENOTSUP, "engine: a pointwise op alone has no batch kernel");
+    if (rc) {
+        delete r;
+        return rc;
+    }
+    LaunchParams& p = r->p;
+    p.src = S->dm.data + y * S->dm.stride + x;
+    p.src_stride = S->dm.stride;
+    p.src_w = w;
+    p.src_h = h;
+    p.width = w;
+    p.height = h;
+    p.out_x1 = w;
+    p.out_y1 = h;
+    p.status = S->ctx->d_status;
+    r->bytes = (size_t)(w * h) * 4 * (size_t)r->nout + (M.valid ? (size_t)((w * h + 63) / 64) * 8 * r->nout : 0);
+    std::lock_guard<std::mutex> lk(S->mu);
+    r->ticket = S->next_ticket++;
+    r->t_submit = now_ns();
+    S->all[r->ticket] = r;
+    S->queue.push_back(r);
+    *ticket = r->ticket;
+    S->cv.notify_one();
+    return STRATA_OK;
+}
+
+extern "C" int strata_server_wait(strata_server* S, uint64_t ticket, int64_t timeout_ms, strata_server_result* res) {
+    if (!S) return fail(STRATA_EINVAL, "engine: nil server");
+    std::unique_lock<std::mutex> lk(S->mu);
+    auto it = S->all.find(ticket);
+    if (it == S->all.end()) return fail(STRATA_EINVAL, "engine: unknown ticket %llu", (unsigned long long)ticket);
+    Request* r = it->second;
+    auto done = [&] { return r->status <= 0; };
+    if (timeout_ms < 0) S->done_cv.wait(lk, done);
+    else if (!S->done_cv.wait_for(lk, std::chrono::milliseconds(timeout_ms), done))
+        return fail(STRATA_ETIMEDOUT, "engine: request %llu is not done", (unsigned long long)ticket);
+    if (res) {
+        memset(res, 0, sizeof *res);
+        res->status = r->status;
+        for (int k = 0; k < r->nout; k++) {
+            res->out[k].data = r->out[k];
+            res->out[k].width = r->w;
+            res->out[k].height = r->h;
+            res->out[k].stride = r->w;
+            res->out[k].valid = reinterpret_cast<uint64_t*>(r->out_bits[k]);
+            res->out[k].on_device = 1;
+        }
+        res->nout = r->nout;
+        res->t_submit_ns = r->t_submit;
+        res->t_start_ns = r->t_start;
+        res->t_done_ns = r->t_done;
+    }
+    return r->status < 0 ? fail(r->status, "engine: request %llu failed", (unsigned long long)ticket) : STRATA_OK;
+}
+
+extern "C" int strata_server_release(strata_server* S, uint64_t ticket) {
+    if (!S) return fail(STRATA_EINVAL, "engine: nil server");
+    std::lock_guard<std::mutex> lk(S->mu);
+    auto it = S->all.find(ticket);
+    if (it == S->all.end()) return fail(STRATA_EINVAL, "engine: unknown ticket %llu", (unsigned long long)ticket);
+    Request* r = it->second;
+    if (r->status > 0) return fail(STRATA_EINVAL, "engine: request %llu is still running", (unsigned long long)ticket);
+    cudaSetDevice(S->ctx->device);
+    for (int k = 0; k < 2; k++) {
+        if (r->out[k]) cudaFreeAsync(r->out[k], S->ctx->stream);
+        if (r->out_bits[k]) cudaFreeAsync(r->out_bits[k], S->ctx->stream);
+    }
+    if (r->t_start) S->used -= r->bytes;
+    S->all.erase(it);
+    delete r;
+    S->cv.notify_one();
+    return STRATA_OK;
+}
+
+extern "C" int strata_server_stats(strata_server* S, int64_t* batches, int64_t* served, int64_t* used_bytes) {
+    if (!S) return fail(STRATA_EINVAL, "engine: nil server");
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (batches) *batches = S->batches;
+    if (served) *served = S->served;
+    if (used_bytes) *used_bytes = (int64_t)S->used;
+    return STRATA_OK;
+}
+
+extern "C" void strata_server_destroy(strata_server* S) {
+    if (!S) return;
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->stop = true;
+        S->cv.notify_all();
+    }
+    if (S->thread.joinable()) S->thread.join();
+    cudaSetDevice(S->ctx->device);
+    for (Slot& s : S->slots) {
+        if (s.stream) cudaStreamSynchronize(s.stream);
+        if (s.done) cudaEventDestroy(s.done);
+        if (s.d_items) cudaFree(s.d_items);
+        if (s.h_items) cudaFreeHost(s.h_items);
+        if (s.stream) cudaStreamDestroy(s.stream);
+    }
+    cudaStreamSynchronize(S->ctx->stream);
+    for (auto& kv : S->all) {
+        Request* r = kv.second;
+        for (int k = 0; k < 2; k++) {
+            if (r->out[k]) cudaFree(r->out[k]);
+            if (r->out_bits[k]) cudaFree(r->out_bits[k]);
+        }
+        delete r;
+    }
+    delete S;
+}

@@ -99,10 +99,11 @@ __device__ __forceinline__ void row_compute(const LaunchParams& P, const EpiTabl
                 if constexpr (OP == STRATA_OP_SLOPE) r = slope(gx, gy, P.k[2], KIND != 0);
                 else if constexpr (OP == STRATA_OP_ASPECT) r = aspect(gx, gy, P.k[2], KIND != 0);
                 else r = shade(gx, gy, P.k[2], P.k[3], P.k[4]);
-                if constexpr (EPI) r = epilogue(P, *T, r);
                 o0[i] = in ? r : nan;
             }
         }
+        // The epilogue maps NaN to itself, so the edge ring stays NaN.
+        if constexpr (EPI && OP != STRATA_OP_GRADIENT) epilogue4(P, *T, o0);
     } else {
 #pragma unroll
         for (int i = 0; i < 4; i++) {
@@ -110,9 +111,9 @@ __device__ __forceinline__ void row_compute(const LaunchParams& P, const EpiTabl
                                 b.v[i + 2], c.v[i], c.v[i + 1], c.v[i + 2]};
             float r0 = nan, r1 = nan;
             apply3<OP>(P, z, r0, r1);
-            if constexpr (EPI) r0 = epilogue(P, *T, r0);
             o0[i] = (rowin && colin[i]) ? r0 : nan;
         }
+        if constexpr (EPI) epilogue4(P, *T, o0);
     }
 }
 

@@ -79,59 +79,76 @@ __device__ __forceinline__ float epilogue(const LaunchParams& P, float v) {
 // constant bank are served one address at a time, where shared memory
 // serves them together.
 struct EpiTables {
-    float a[kMaxEpilogue][STRATA_MAX_KNOTS];
+    // a: the knots (breaks), padded with NaN to a power of two; b: the
+    // values; p2: the padded length, the binary search's span.
+    float a[kMaxEpilogue][2 * STRATA_MAX_KNOTS];
     float b[kMaxEpilogue][STRATA_MAX_KNOTS + 1];
+    int p2[kMaxEpilogue];
 };
 
 // Copies the tables in with every thread of the block; the caller
 // synchronises the block before reading them.
 __device__ __forceinline__ void stage_epilogue(const LaunchParams& P, EpiTables& T) {
-    constexpr int per = 2 * STRATA_MAX_KNOTS + 1;
-    for (int i = threadIdx.x + threadIdx.y * blockDim.x; i < P.nepi * per; i += blockDim.x * blockDim.y) {
+    constexpr int per = 2 * STRATA_MAX_KNOTS + STRATA_MAX_KNOTS + 1;
+    const int nt = blockDim.x * blockDim.y;
+    for (int i = threadIdx.x + threadIdx.y * blockDim.x; i < P.nepi * per; i += nt) {
         const int s = i / per, j = i - s * per;
-        if (j < STRATA_MAX_KNOTS) T.a[s][j] = P.epi[s].a[j];
-        else T.b[s][j - STRATA_MAX_KNOTS] = P.epi[s].b[j - STRATA_MAX_KNOTS];
+        if (j < 2 * STRATA_MAX_KNOTS) T.a[s][j] = j < P.epi[s].n ? P.epi[s].a[j] : cell::nanf32();
+        else T.b[s][j - 2 * STRATA_MAX_KNOTS] = P.epi[s].b[j - 2 * STRATA_MAX_KNOTS];
+    }
+    if (threadIdx.x + threadIdx.y * blockDim.x < P.nepi) {
+        const int s = threadIdx.x + threadIdx.y * blockDim.x;
+        int p2 = 1;
+        while (p2 < P.epi[s].n + 1) p2 <<= 1;
+        T.p2[s] = p2;
     }
 }
 
-// Knots of a short table (n <= kShortTable) at or below v, counted against
-// the launch parameters: the loop unrolls, so each knot is a constant-bank
-// operand of one compare.
-constexpr int kShortTable = 8;
-
-__device__ __forceinline__ int short_count(float v, const float* xs, int n) {
-    int k = 0;
-#pragma unroll
-    for (int j = 0; j < kShortTable; j++) k += (j < n && xs[j] <= v) ? 1 : 0;
-    return k;
+// The number of knots at or below v (v not NaN): the reference's forward
+// scan index for strictly increasing knots, found by halving the padded
+// table. "t[j] <= v" holds for a prefix of the knots and never for a NaN
+// pad, so each step keeps the count's invariant.
+__device__ __forceinline__ int knot_count(const float* t, int p2, float v) {
+    int c = 0;
+    for (int step = p2 >> 1; step >= 1; step >>= 1) c += t[c + step - 1] <= v ? step : 0;
+    return c;
 }
 
-// One pointwise stage on v: the count against the parameters when the
-// table is short, the gather from the shared-memory copy.
-__device__ __forceinline__ float epi_stage(const EpiStage& e, const float* ta, const float* tb, float v) {
+// One pointwise stage (Lookup or Reclass, internal/curve/scalar.go:39-114)
+// over a lane's four cells at once, so their loads and arithmetic overlap.
+__device__ __forceinline__ void epi_stage4(const EpiStage& e, const float* ta, const float* tb, int p2,
+                                           float (&v)[4]) {
     const int n = e.n;
-    const int k = n <= kShortTable ? short_count(v, e.a, n) : cell::knots_at_or_below(v, ta, n);
+    int k[4];
+#pragma unroll
+    for (int c = 0; c < 4; c++) k[c] = knot_count(ta, p2, v[c]);
     if (e.op == STRATA_OP_RECLASS) {
-        const float r = tb[k];
-        return v != v ? v : r;
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const float r = tb[k[c]];
+            v[c] = v[c] != v[c] ? v[c] : r;
+        }
+        return;
     }
-    // Lookup, as cell::lookup from its table index on.
-    const int lo = k == 0 ? 0 : k - 1;
-    const int hi = k == n ? n - 1 : k;
-    const float x0 = ta[lo], y0 = tb[lo];
-    const float t = cell::div(cell::sub(v, x0), cell::sub(ta[hi], x0));
-    float r = cell::add(y0, cell::mul(t, cell::sub(tb[hi], y0)));
-    r = v == x0 ? y0 : r;
-    r = k == n ? tb[n - 1] : r;
-    r = k == 0 ? tb[0] : r;
-    return v != v ? v : r;
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        const int lo = k[c] == 0 ? 0 : k[c] - 1;
+        const int hi = k[c] == n ? n - 1 : k[c];
+        const float x0 = ta[lo], y0 = tb[lo];
+        const float t = cell::div(cell::sub(v[c], x0), cell::sub(ta[hi], x0));
+        float r = cell::add(y0, cell::mul(t, cell::sub(tb[hi], y0)));
+        r = v[c] == x0 ? y0 : r;
+        r = k[c] == n ? tb[n - 1] : r;
+        r = k[c] == 0 ? tb[0] : r;
+        v[c] = v[c] != v[c] ? v[c] : r;
+    }
 }
 
-__device__ __forceinline__ float epilogue(const LaunchParams& P, const EpiTables& T, float v) {
+// The epilogue over four cells, stage by stage.
+__device__ __forceinline__ void epilogue4(const LaunchParams& P, const EpiTables& T, float (&v)[4]) {
 #pragma unroll
     for (int i = 0; i < kMaxEpilogue; i++)
-        if (i < P.nepi) v = epi_stage(P.epi[i], T.a[i], T.b[i], v);
-    return v;
+        if (i < P.nepi) epi_stage4(P.epi[i], T.a[i], T.b[i], T.p2[i], v);
 }
 
 }  // namespace strata

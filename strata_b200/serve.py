@@ -1,0 +1,102 @@
+"""Serving: window requests over a device-resident DEM mosaic, with
+continuous batching (strata_server_*).
+
+    srv = serve.Server(mosaic, budget_bytes=120 << 30)
+    t = srv.submit(terrain.slope_stage(opts), x, y, w, h)
+    res = srv.wait(t)        # the window's result (device memory) and its timings
+    res.copy_to(dst)         # into a raster of the window's size
+    srv.release(t)           # frees the outputs and their budget
+
+Requests are admitted in arrival order while their outputs fit the memory
+budget and run in batches as they arrive; batches on the server's streams
+overlap on the device, so a request that arrives while others run joins
+the next batch rather than waiting for the queue to drain. Each window is
+a raster of its own (its border is its edge ring), so a request's result
+is the one strata_process gives for the window view.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from typing import List, Optional
+
+
+
+from . import _lib, engine
+from .raster import Float32Raster
+
+
+@dataclass
+class Result:
+    outputs: List[Float32Raster]  # device rasters owned by the server until release
+    t_submit_ns: int
+    t_start_ns: int
+    t_done_ns: int
+
+    @property
+    def latency_ms(self) -> float:
+        return (self.t_done_ns - self.t_submit_ns) / 1e6
+
+    def copy(self, k: int = 0) -> Float32Raster:
+        """Output k as a device raster of torch tensors the caller owns."""
+        src = self.outputs[k]
+        n = src.width * src.height
+        data = _device_view(src.data, n, "<f4").clone()
+        valid = _device_view(src.valid, (n + 63) // 64, "<i8").clone() if src.valid else None
+        return Float32Raster(data, src.width, src.height, src.width, valid, 0)
+
+
+def _device_view(ptr: int, n: int, typestr: str):
+    """A torch tensor over n elements of device memory at ptr (no copy)."""
+    import torch
+
+    class _Buf:
+        __cuda_array_interface__ = {"shape": (n,), "typestr": typestr, "data": (ptr, False), "version": 3}
+
+    return torch.as_tensor(_Buf(), device="cuda")
+
+
+class Server:
+    def __init__(self, mosaic: Float32Raster, budget_bytes: int = 0, streams: int = 0, max_batch: int = 0,
+                 device: int = 0):
+        self.mosaic = mosaic  # keeps the device buffers alive
+        c = engine.device_context(device)
+        o = _lib.ServerOpts(budget_bytes, streams, max_batch)
+        p = ctypes.c_void_p()
+        _lib.check(_lib.lib().strata_server_create(c, ctypes.byref(engine.c_raster(mosaic)), ctypes.byref(o),
+                                                   ctypes.byref(p)))
+        self._h = p
+
+    def submit(self, stages: engine.StageList, x: int, y: int, w: int, h: int) -> int:
+        t = ctypes.c_uint64()
+        _lib.check(_lib.lib().strata_server_submit(self._h, stages.c_array(), len(stages.stages), x, y, w, h,
+                                                   ctypes.byref(t)))
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = -1) -> Result:
+        r = _lib.ServerResult()
+        _lib.check(_lib.lib().strata_server_wait(self._h, ticket, timeout_ms, ctypes.byref(r)))
+        outs = []
+        for k in range(r.nout):
+            o = r.out[k]
+            outs.append(Float32Raster(o.data, o.width, o.height, o.stride, o.valid if o.valid else None, 0))
+        return Result(outs, r.t_submit_ns, r.t_start_ns, r.t_done_ns)
+
+    def release(self, ticket: int) -> None:
+        _lib.check(_lib.lib().strata_server_release(self._h, ticket))
+
+    def stats(self):
+        b, s, u = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        _lib.check(_lib.lib().strata_server_stats(self._h, ctypes.byref(b), ctypes.byref(s), ctypes.byref(u)))
+        return {"batches": b.value, "served": s.value, "used_bytes": u.value}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            _lib.lib().strata_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
