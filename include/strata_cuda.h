@@ -260,6 +260,26 @@ int strata_batch_info(const strata_batch *batch, strata_stats *stats, int *class
 void strata_batch_destroy(strata_batch *batch);
 
 /*
+ * A batch run that allocates nothing (no counterpart in strata, which has
+ * no batched call). It does what strata_batch_create + strata_batch_run +
+ * strata_batch_destroy do for the same items, with the same results, but
+ * writes the descriptors into a fixed scratch area in the library's static
+ * device memory (one per device, room for STRATA_NOALLOC_BATCH_MAX items;
+ * more is EINVAL) and launches the class kernels directly on the stream
+ * (0 = the context's), so it makes no cudaMalloc or cudaFree call and
+ * builds no graph. The first call on a device looks the scratch area up;
+ * make that call before any stream capture. The scratch is shared by
+ * every call on the device: calls on one stream follow each other in
+ * stream order, but calls on different streams (or different contexts of
+ * one device) that overlap on the device race on it, so a caller
+ * serialises them, e.g. by keeping every call on one stream.
+ * synchronize != 0 waits for the kernels and reports their status.
+ */
+#define STRATA_NOALLOC_BATCH_MAX 64
+int strata_batch_run_noalloc(strata_ctx *ctx, const strata_batch_item *items, int nitems, void *stream,
+                             int synchronize);
+
+/*
  * Serving (no counterpart call in strata, which serves no requests): window
  * requests over a device-resident mosaic, run with continuous batching. A
  * scheduler thread takes queued requests whenever one of `streams` streams

@@ -21,6 +21,7 @@ STAGE_ROTATE180 = 1
 EXEC_ASYNC = 1
 MAX_RADIUS = 8
 MAX_KNOTS = 64
+MAX_NOALLOC_BATCH = 64
 
 c_i32, c_i64, c_f32, c_f64, c_p = ctypes.c_int32, ctypes.c_int64, ctypes.c_float, ctypes.c_double, ctypes.c_void_p
 
@@ -141,6 +142,7 @@ SIGNATURES = [
     ("strata_batch_run", ctypes.c_int, [c_p, c_p, ctypes.c_int]),
     ("strata_batch_info", ctypes.c_int, [c_p, ctypes.POINTER(Stats), ctypes.POINTER(ctypes.c_int)]),
     ("strata_batch_destroy", None, [c_p]),
+    ("strata_batch_run_noalloc", ctypes.c_int, [c_p, ctypes.POINTER(BatchItem), ctypes.c_int, c_p, ctypes.c_int]),
     ("strata_server_create", ctypes.c_int, [c_p, ctypes.POINTER(Raster), ctypes.POINTER(ServerOpts),
                                             ctypes.POINTER(c_p)]),
     ("strata_server_submit", ctypes.c_int, [c_p, ctypes.POINTER(Stage), ctypes.c_int, c_i64, c_i64, c_i64, c_i64,

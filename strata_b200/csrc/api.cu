@@ -1641,6 +1641,182 @@ extern "C" void strata_batch_destroy(strata_batch* B) {
 }
 
 // ---------------------------------------------------------------------------
+// A batch run without allocation: the descriptors go to a fixed scratch
+// area in the module's static device memory instead of a cudaMalloc'd
+// table, and the class kernels launch straight onto the caller's stream
+// (no graph). The scratch is one per device: calls on one stream are
+// ordered by it, calls on different streams that overlap on the device
+// race on it.
+
+namespace {
+
+constexpr size_t kScratchHead = 256;  // the status word, padded so the descriptors stay 256-byte aligned
+constexpr size_t kScratchBytes = kScratchHead + sizeof(strata::BatchItem) * STRATA_NOALLOC_BATCH_MAX;
+static __device__ __align__(256) unsigned char g_batch_scratch[kScratchBytes];
+
+constexpr int kMaxDevices = 64;
+struct ScratchSlot {
+    std::once_flag once;
+    cudaError_t err = cudaSuccess;
+    unsigned char* ptr = nullptr;
+    int sms = 0;
+};
+ScratchSlot g_scratch[kMaxDevices];
+
+// Host staging of the descriptors and the class plan; one call at a time.
+std::mutex g_noalloc_mu;
+strata::BatchItem g_noalloc_items[STRATA_NOALLOC_BATCH_MAX];
+int g_noalloc_order[STRATA_NOALLOC_BATCH_MAX];
+
+// The device address of the scratch area, looked up once per device with
+// that device current.
+int scratch_address(int device, unsigned char** ptr, int* sms) {
+    if (device < 0 || device >= kMaxDevices) return fail(STRATA_EINVAL, "engine: device %d out of range", device);
+    ScratchSlot& s = g_scratch[device];
+    std::call_once(s.once, [&] {
+        s.err = cudaSetDevice(device);
+        if (s.err == cudaSuccess) s.err = cudaGetSymbolAddress((void**)&s.ptr, g_batch_scratch);
+        if (s.err == cudaSuccess) s.err = cudaDeviceGetAttribute(&s.sms, cudaDevAttrMultiProcessorCount, device);
+    });
+    if (s.err != cudaSuccess) return cuda_fail(s.err, "batch scratch address");
+    *ptr = s.ptr;
+    *sms = s.sms;
+    return STRATA_OK;
+}
+
+}  // namespace
+
+extern "C" int strata_batch_run_noalloc(strata_ctx* c, const strata_batch_item* items, int nitems, void* stream,
+                                        int synchronize) {
+    if (!c) return fail(STRATA_EINVAL, "engine: nil context");
+    if (nitems < 1 || !items) return fail(STRATA_EINVAL, "engine: a batch needs at least one raster");
+    if (nitems > STRATA_NOALLOC_BATCH_MAX)
+        return fail(STRATA_EINVAL, "engine: %d rasters exceed the %d a batch without allocation can hold", nitems,
+                    STRATA_NOALLOC_BATCH_MAX);
+    std::lock_guard<std::mutex> lock(c->mu);
+    std::lock_guard<std::mutex> staging(g_noalloc_mu);
+    unsigned char* scratch;
+    int sms, rc;
+    if ((rc = scratch_address(c->device, &scratch, &sms))) return rc;
+    cudaSetDevice(c->device);
+    int* d_status = reinterpret_cast<int*>(scratch);
+    auto* d_items = reinterpret_cast<strata::BatchItem*>(scratch + kScratchHead);
+    strata::BatchItem* host = g_noalloc_items;
+    // Each raster's descriptor, as strata_batch_create plans it.
+    for (int i = 0; i < nitems; i++) {
+        const strata_batch_item& it = items[i];
+        LaunchParams p;
+        int nout = 0;
+        if ((rc = plan_stages(it.stages, it.nstages, p, &nout))) return rc;
+        if ((rc = check_operands(&it.src, 1, it.dst, nout, nout, p.radius))) return rc;
+        if (!it.src.on_device || !it.dst[0].on_device || (nout > 1 && !it.dst[1].on_device))
+            return fail(STRATA_EINVAL, "engine: batch raster %d: the rasters of a batch must be on the device", i);
+        if (p.op == STRATA_OP_LOOKUP || p.op == STRATA_OP_RECLASS)
+            return fail(STRATA_ENOTSUP, "engine: batch raster %d: a pointwise op alone has no batch kernel", i);
+        DevOperand ds, dd[2];
+        if ((rc = stage_in(c, nullptr, it.src, 0, false, &ds))) return rc;
+        for (int k = 0; k < nout; k++)
+            if ((rc = stage_in(c, nullptr, it.dst[k], 0, false, &dd[k]))) return rc;
+        const int64_t W = it.src.width, H = it.src.height;
+        p.src = ds.data;
+        p.src_stride = ds.stride;
+        p.src_x0 = p.src_y0 = 0;
+        p.src_w = W;
+        p.src_h = H;
+        p.dst0 = dd[0].data;
+        p.dst0_stride = dd[0].stride;
+        if (nout > 1) {
+            p.dst1 = dd[1].data;
+            p.dst1_stride = dd[1].stride;
+        }
+        p.dst_x0 = p.dst_y0 = 0;
+        p.width = W;
+        p.height = H;
+        p.out_x0 = p.out_y0 = 0;
+        p.out_x1 = W;
+        p.out_y1 = H;
+        p.status = d_status;
+        strata::BatchItem b;
+        memset(&b, 0, sizeof b);
+        b.p = p;
+        for (int k = 0; k < nout; k++) {
+            if (!it.dst[k].valid) continue;
+            fill_validity(b.v[b.nvalid], ds, it.src.valid != nullptr, dd[k], span_cells(it.dst[k]), W, H, p.radius, 0,
+                          H);
+            b.nvalid++;
+        }
+        b.tw = it.tile_width > 0 ? it.tile_width : 64;
+        b.th = it.tile_height > 0 ? it.tile_height : 32;
+        if (b.tw > 1024 || b.th > 1024 || strata::batch_smem_bytes(p.op, p.radius, b.tw, b.th) > 200 * 1024)
+            return fail(STRATA_EINVAL, "engine: batch raster %d: tile %d x %d is too large", i, b.tw, b.th);
+        b.tiles_x = (W + b.tw - 1) / b.tw;
+        host[i] = b;
+    }
+    // Group by class (op, radius), keeping the callers' order within one:
+    // an insertion sort of the indices, stable and heap-free.
+    int* order = g_noalloc_order;
+    for (int i = 0; i < nitems; i++) {
+        int j = i;
+        const auto key = std::make_pair(host[i].p.op, host[i].p.radius);
+        for (; j > 0 && key < std::make_pair(host[order[j - 1]].p.op, host[order[j - 1]].p.radius); j--)
+            order[j] = order[j - 1];
+        order[j] = i;
+    }
+    // Permute into class order in place (cycle by cycle) and number each
+    // class's work units.
+    for (int i = 0; i < nitems; i++) {
+        if (order[i] < 0) continue;
+        strata::BatchItem t = host[i];
+        int j = i;
+        while (order[j] != i) {
+            const int k = order[j];
+            host[j] = host[k];
+            order[j] = -1;
+            j = k;
+        }
+        host[j] = t;
+        order[j] = -1;
+    }
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+    cudaError_t e = cudaMemsetAsync(d_status, 0, sizeof(int), st);
+    if (e != cudaSuccess) return cuda_fail(e, "batch status");
+    int64_t total = 0;
+    for (int i = 0; i < nitems; i++) {
+        if (i > 0 && (host[i].p.op != host[i - 1].p.op || host[i].p.radius != host[i - 1].p.radius)) total = 0;
+        const int64_t ty = (host[i].p.height + host[i].th - 1) / host[i].th;
+        host[i].tile0 = total;
+        total += host[i].tiles_x * ty;
+    }
+    e = cudaMemcpyAsync(d_items, host, sizeof(strata::BatchItem) * (size_t)nitems, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return cuda_fail(e, "batch descriptors");
+    for (int first = 0; first < nitems;) {
+        const int op = host[first].p.op, radius = host[first].p.radius;
+        int last = first;
+        size_t smem = 0;
+        int64_t units = 0;
+        for (; last < nitems && host[last].p.op == op && host[last].p.radius == radius; last++) {
+            smem = std::max(smem, strata::batch_smem_bytes(op, radius, host[last].tw, host[last].th));
+            units = host[last].tile0 + host[last].tiles_x * ((host[last].p.height + host[last].th - 1) / host[last].th);
+        }
+        const int per_sm = smem > 100 * 1024 ? 1 : (smem > 48 * 1024 ? 2 : 4);
+        const int64_t grid = std::min<int64_t>(units, (int64_t)sms * per_sm);
+        if (!strata::launch_batch_class(op, radius, d_items + first, last - first, units, (int)grid, smem, st)) {
+            cudaGetLastError();
+            return fail(STRATA_ENOTSUP, "engine: an op of the batch has no batch kernel");
+        }
+        if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "batch launch");
+        first = last;
+    }
+    if (!synchronize) return STRATA_OK;
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "batch run");
+    int status = 0;
+    if ((e = cudaMemcpy(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost)) != cudaSuccess)
+        return cuda_fail(e, "batch status");
+    if (status) return fail(status, "engine: a batch kernel reported status %d", status);
+    return STRATA_OK;
+}
+
+// ---------------------------------------------------------------------------
 // Serving: window requests over a resident mosaic, admitted under a memory
 // budget and batched as they arrive (continuous batching). A scheduler
 // thread takes the queued requests whenever one of its streams is free,
