@@ -103,42 +103,54 @@ def focal_ops():
     return ops
 
 
-def workload(name):
+def workload(name, side=None, only=None):
+    """The named workload; side and only (profiling aids) replace its raster
+    side and keep the named ops of its set."""
+    wl = _workload(name, side)
+    if only:
+        keep = set(only.split(","))
+        wl["ops"] = [o for o in wl["ops"] if o[0] in keep]
+        if not wl["ops"]:
+            raise SystemExit(f"no op of {name} is named in {only}")
+    return wl
+
+
+def _workload(name, side=None):
     from strata_b200 import synth
 
     if name == "terrain16k":
-        n, seed, cs = 16384, 0x5EED0002, 10
+        n, seed, cs = side or 16384, 0x5EED0002, 10
         cells = synth.fbm_dem(n, n, seed)
         valid = synth.block_mask(n, n, seed, 0.02)
-        return dict(name="terrain set on 16384x16384 f32 DEM", width=n, height=n, cells=cells, valid=valid,
+        return dict(name=f"terrain set on {n}x{n} f32 DEM", width=n, height=n, cells=cells, valid=valid,
                     ops=terrain_ops(cs), cell_size=cs, mask="2% NoData in 8x8 blocks")
     if name == "slope2k":
-        n, seed, cs = 2048, 0x5EED0001, 30
+        n, seed, cs = side or 2048, 0x5EED0001, 30
         from strata_b200 import terrain
 
-        return dict(name="Slope on 2048x2048 f32 DEM", width=n, height=n, cells=synth.fbm_dem(n, n, seed),
+        return dict(name=f"Slope on {n}x{n} f32 DEM", width=n, height=n, cells=synth.fbm_dem(n, n, seed),
                     valid=synth.block_mask(n, n, seed, 0.02), cell_size=cs, mask="2% NoData in 8x8 blocks",
                     ops=[("slope", lambda: terrain.slope_stage(terrain.SlopeOptions(CellSize=cs)), 1)])
     if name == "slope8k":
-        n, seed, cs = 8192, 0x5EED0001, 30
+        n, seed, cs = side or 8192, 0x5EED0001, 30
         from strata_b200 import terrain
 
-        return dict(name="Slope on 8192x8192 f32 DEM", width=n, height=n, cells=synth.fbm_dem(n, n, seed),
+        return dict(name=f"Slope on {n}x{n} f32 DEM", width=n, height=n, cells=synth.fbm_dem(n, n, seed),
                     valid=synth.block_mask(n, n, seed, 0.02), cell_size=cs, mask="2% NoData in 8x8 blocks",
                     ops=[("slope", lambda: terrain.slope_stage(terrain.SlopeOptions(CellSize=cs)), 1)])
     if name == "pipeline8k":
-        n, seed, cs = 8192, 0x5EED0002, 10
+        n, seed, cs = side or 8192, 0x5EED0002, 10
         from strata_b200 import terrain, transfer
 
-        return dict(name="Slope->Lookup->Reclass on 8192x8192 f32 DEM", width=n, height=n,
+        return dict(name=f"Slope->Lookup->Reclass on {n}x{n} f32 DEM", width=n, height=n,
                     cells=synth.fbm_dem(n, n, seed), valid=synth.block_mask(n, n, seed, 0.02), cell_size=cs,
                     mask="2% NoData in 8x8 blocks",
                     ops=[("slope_lookup_reclass", lambda: terrain.slope_stage(terrain.SlopeOptions(CellSize=cs))
                           .extend(transfer.lookup_stage(SLOPE_XS, SLOPE_YS))
                           .extend(transfer.reclass_stage(BREAKS, VALUES)), 1)])
     if name == "focal8k":
-        n, seed = 8192, 0x5EED0003
-        return dict(name="focal ops on 8192x8192 f32 raster", width=n, height=n, cells=synth.normal_trend(n, n, seed),
+        n, seed = side or 8192, 0x5EED0003
+        return dict(name=f"focal ops on {n}x{n} f32 raster", width=n, height=n, cells=synth.normal_trend(n, n, seed),
                     valid=synth.cell_mask(n, n, seed, 0.05), ops=focal_ops(), cell_size=None,
                     mask="5% random NoData cells")
     raise SystemExit(f"unknown workload {name}")
@@ -242,7 +254,7 @@ def run_ours(args, rank, world, local_rank):
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    wl = workload(args.workload)
+    wl = workload(args.workload, args.side, args.ops)
     W, H = wl["width"], wl["height"]
     n = W * H
     masked = wl["valid"] is not None
@@ -493,7 +505,7 @@ def run_batch(args, rank, world, local_rank):
 
 
 def run_reference(args):
-    wl = workload(args.workload)
+    wl = workload(args.workload, args.side, args.ops)
     threads = os.cpu_count() or 1
     rows = min(wl["height"], max(64, (1 << 22) // wl["width"]))
     for _ in range(args.warmup):
@@ -528,6 +540,8 @@ def main():
                     choices=["terrain16k", "slope2k", "slope8k", "pipeline8k", "focal8k", "batch512"])
     ap.add_argument("--tune-cache", action="store_true", help="keep the batch autotuner's choices in a file")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--side", type=int, default=None, help="raster side override (profiling captures)")
+    ap.add_argument("--ops", default=None, help="comma-separated ops of the workload to keep (profiling captures)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

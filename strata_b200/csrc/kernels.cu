@@ -126,41 +126,14 @@ __global__ void __launch_bounds__(256) pointwise_kernel(const __grid_constant__ 
 // Validity.
 
 
+// One thread per (row, 32-bit word) of the output region: a block of 32
+// words x 8 rows, the rows in a grid-stride loop past 65535 x 8 of them.
 __global__ void __launch_bounds__(256) validity_kernel(const __grid_constant__ ValidityParams v) {
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= v.dst_words) return;
-    const int64_t wi = v.dst_lo_word + i;
-    const int64_t pos = wi * 32 - v.dst_off;  // destination cell index of the word's bit 0
-    uint32_t bits = 0u, ours = 0u;
-    int k = 0;
-    while (k < 32) {
-        const int64_t c = pos + k;
-        if (c < 0) {
-            k = (int)min64(32, (int64_t)k - c);
-            continue;
-        }
-        const int64_t ly = c / v.dst_stride, lx = c - ly * v.dst_stride;
-        const int64_t y = ly + v.dst_y0, x = lx + v.dst_x0;  // global cell
-        if (y >= v.out_y1) break;
-        if (y < v.out_y0 || x >= v.out_x1) {
-            // Past the region in this row: on to the next row's start.
-            k = (int)min64(32, (int64_t)k + (v.dst_stride - lx));
-            continue;
-        }
-        if (x < v.out_x0) {
-            k = (int)min64(32, (int64_t)k + (v.out_x0 - x));
-            continue;
-        }
-        const int len = (int)min64(32 - k, v.out_x1 - x);
-        const uint32_t m = len == 32 ? 0xffffffffu : ((1u << len) - 1u);
-        const uint32_t seg = segment_bits(v, x, y) & m;
-        bits |= seg << k;
-        ours |= m << k;
-        k += len;
-    }
-    if (ours == 0u) return;
-    const uint32_t old = v.dst_bits[wi];
-    v.dst_bits[wi] = (old & ~ours) | bits;
+    const int64_t wpr = (v.out_x1 - v.out_x0 + 31) / 32 + 1;  // words a row of the region can touch
+    const int64_t k = blockIdx.x * 32 + threadIdx.x;
+    if (k >= wpr) return;
+    for (int64_t y = v.out_y0 + blockIdx.y * 8 + threadIdx.y; y < v.out_y1; y += (int64_t)gridDim.y * 8)
+        row_word_validity(v, y, v.out_x0, v.out_x1, k);
 }
 
 template <int OP, int R>
@@ -241,6 +214,7 @@ int64_t launch_data(const LaunchParams& p, cudaStream_t s, int64_t* window_cells
         }
         return blocks;
     }
+    if (focal_eligible(p)) return launch_focal(p, s, window_cells);
     const int64_t tiles = L(p, s);
     if (window_cells) {
         // Each tile reads its cells grown by the radius, clipped to the raster.
@@ -261,9 +235,12 @@ int64_t launch_data(const LaunchParams& p, cudaStream_t s, int64_t* window_cells
 }
 
 void launch_validity(const ValidityParams& v, cudaStream_t s) {
-    if (v.dst_words <= 0) return;
-    const int64_t blocks = (v.dst_words + 255) / 256;
-    validity_kernel<<<(unsigned)blocks, 256, 0, s>>>(v);
+    if (v.dst_words <= 0 || v.out_x1 <= v.out_x0 || v.out_y1 <= v.out_y0) return;
+    const int64_t wpr = (v.out_x1 - v.out_x0 + 31) / 32 + 1;
+    const int64_t rows = v.out_y1 - v.out_y0;
+    const int64_t gy = (rows + 7) / 8;
+    const dim3 grid((unsigned)((wpr + 31) / 32), (unsigned)(gy < 65535 ? gy : 65535));
+    validity_kernel<<<grid, dim3(32, 8), 0, s>>>(v);
 }
 
 }  // namespace strata

@@ -112,6 +112,11 @@ void launch_validity(const ValidityParams& v, cudaStream_t stream);
 // multiple of 4), and its launcher.
 bool march3_eligible(const LaunchParams& p);
 int64_t launch_march3(const LaunchParams& p, cudaStream_t stream);
+// The register-blocked focal kernels (focal.cu) for the windowed ops at
+// radius 2..8 on 16-byte aligned rows; launch_focal returns the blocks
+// launched and sets *window_cells (if given) to the cells they read.
+bool focal_eligible(const LaunchParams& p);
+int64_t launch_focal(const LaunchParams& p, cudaStream_t stream, int64_t* window_cells);
 
 // Tile geometry of the data kernels, for Stats.
 void tile_shape(int op, int radius, int64_t width, int* tw, int* th);

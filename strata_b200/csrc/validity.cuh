@@ -51,36 +51,41 @@ __device__ __forceinline__ uint32_t segment_bits(const ValidityParams& v, int64_
 
 namespace strata {
 
-// The validity of the output cells [x0, x1) x [y0, y1) (global
-// coordinates), written by the nthreads threads of a block, one (row,
-// 32-bit word) pair at a time. A word wholly inside a row of the region
-// holds only the region's cells and is stored; a word the region shares
-// with other cells (a neighbouring tile, another raster) changes only the
-// region's bits, with atomics, so concurrent tiles never lose each
-// other's bits.
+// Word k of output row y's bits over the cells [x0, x1) (global
+// coordinates): k counts the 32-bit words the row segment touches, from the
+// one holding cell x0. A word wholly inside the segment holds only its
+// cells and is stored; a word the segment shares with other cells (a
+// neighbouring tile or row, another raster) changes only the segment's
+// bits, with atomics, so concurrent writers never lose each other's bits.
+__device__ __forceinline__ void row_word_validity(const ValidityParams& v, int64_t y, int64_t x0, int64_t x1,
+                                                  int64_t k) {
+    const int64_t rowbit = v.dst_off + (y - v.dst_y0) * v.dst_stride - v.dst_x0;  // bit of cell (0, y)
+    const int64_t b0 = rowbit + x0, b1 = rowbit + x1;
+    const int64_t w = (b0 >> 5) + k;
+    if (w * 32 >= b1) return;
+    const int64_t lo = b0 > w * 32 ? b0 : w * 32;
+    const int64_t hi = b1 < w * 32 + 32 ? b1 : w * 32 + 32;
+    const int len = (int)(hi - lo), sh = (int)(lo - w * 32);
+    const uint32_t lenmask = len == 32 ? 0xffffffffu : ((1u << len) - 1u);
+    const uint32_t bits = (segment_bits(v, lo - rowbit, y) & lenmask) << sh;
+    const uint32_t m = lenmask << sh;
+    if (m == 0xffffffffu) {
+        v.dst_bits[w] = bits;
+    } else {
+        atomicAnd(&v.dst_bits[w], ~m | bits);
+        atomicOr(&v.dst_bits[w], bits);
+    }
+}
+
+// The validity of the output cells [x0, x1) x [y0, y1), written by the
+// nthreads threads of a block, one (row, word) pair at a time.
 __device__ __forceinline__ void region_validity(const ValidityParams& v, int64_t x0, int64_t y0, int64_t x1,
                                                 int64_t y1, int tid, int nthreads) {
-    const int64_t rows = y1 - y0;
-    const int64_t wpr = (x1 - x0 + 31) / 32 + 1;  // words a row of the region can touch
-    for (int64_t i = tid; i < rows * wpr; i += nthreads) {
-        const int64_t ry = i / wpr, k = i - ry * wpr;
-        const int64_t y = y0 + ry;
-        const int64_t rowbit = v.dst_off + (y - v.dst_y0) * v.dst_stride - v.dst_x0;  // bit of cell (0, y)
-        const int64_t b0 = rowbit + x0, b1 = rowbit + x1;
-        const int64_t w = (b0 >> 5) + k;
-        if (w * 32 >= b1) continue;
-        const int64_t lo = b0 > w * 32 ? b0 : w * 32;
-        const int64_t hi = b1 < w * 32 + 32 ? b1 : w * 32 + 32;
-        const int len = (int)(hi - lo), sh = (int)(lo - w * 32);
-        const uint32_t lenmask = len == 32 ? 0xffffffffu : ((1u << len) - 1u);
-        const uint32_t bits = (segment_bits(v, lo - rowbit, y) & lenmask) << sh;
-        const uint32_t m = lenmask << sh;
-        if (m == 0xffffffffu) {
-            v.dst_bits[w] = bits;
-        } else {
-            atomicAnd(&v.dst_bits[w], ~m | bits);
-            atomicOr(&v.dst_bits[w], bits);
-        }
+    const int wpr = (int)((x1 - x0 + 31) / 32 + 1);  // words a row of the region can touch
+    const int n = (int)(y1 - y0) * wpr;
+    for (int i = tid; i < n; i += nthreads) {
+        const int ry = i / wpr, k = i - ry * wpr;
+        row_word_validity(v, y0 + ry, x0, x1, k);
     }
 }
 

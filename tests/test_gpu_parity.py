@@ -272,6 +272,45 @@ def test_slope_c1_size_against_oracle():
     assert_same_raster(got, want, "slope 2048")
 
 
+FOCAL_LARGE = {
+    "mean_r8": lambda: focal.box_stage(focal.BoxOptions(Radius=8), engine._lib.OP_MEAN),
+    "min_r3": lambda: focal.box_stage(focal.BoxOptions(Radius=3), engine._lib.OP_MIN),
+    "max_r5": lambda: focal.box_stage(focal.BoxOptions(Radius=5), engine._lib.OP_MAX),
+    "gaussian_r8": lambda: focal.separable_stage(focal.SeparableOptions(8, focal.Gaussian(8, 2.5),
+                                                                        synth.uniform_weights(17, 9))),
+    "roughness_r6": lambda: terrain.ruggedness_stage(terrain.RuggednessOptions(Type=3, Radius=6)),
+    "correlate_r8": lambda: focal.weights_stage(focal.WeightsOptions(8, synth.uniform_weights(289, 3)), False),
+    "convolve_r2": lambda: focal.weights_stage(focal.WeightsOptions(2, synth.uniform_weights(25, 4)), True),
+    "riley_r4": lambda: terrain.ruggedness_stage(terrain.RuggednessOptions(Type=0, Radius=4)),
+    "wilson_r7": lambda: terrain.ruggedness_stage(terrain.RuggednessOptions(Type=1, Radius=7)),
+    "tpi_r2": lambda: terrain.ruggedness_stage(terrain.RuggednessOptions(Type=2, Radius=2)),
+    "mean_r8_reclass": lambda: focal.box_stage(focal.BoxOptions(Radius=8), engine._lib.OP_MEAN).extend(
+        transfer.reclass_stage([-0.5, 0.0, 0.5], [1, 2, 3, 4])),
+}
+
+
+@pytest.mark.parametrize("name", sorted(FOCAL_LARGE))
+def test_focal_large_against_oracle(name):
+    """The focal ops at radius 2..8 over a raster wide and tall enough for
+    many column blocks, bands and tiles (5% NoData cells), and over a
+    window view of it at an offset, equal the oracle on every cell and bit."""
+    w, h = 2052, 700
+    seed = 0x5EED0003
+    src = host_raster(poison(synth.normal_trend(w, h, seed), seed, 0.001), synth.cell_mask(w, h, seed, 0.05))
+    want, got = like(src), like(src)
+    run_oracle(FOCAL_LARGE[name](), src, [want], nthreads=8)
+    dsrc, dgot = to_device(src), to_device(got)
+    assert engine.process(FOCAL_LARGE[name](), [dgot], [dsrc]) is None
+    assert_same_raster(to_host(dgot), want, name)
+    # a window view: its own raster, with the parent's stride and bit offsets
+    win = dsrc.Window(36, 21, 1500, 611)
+    wwant = like(to_host(win))
+    run_oracle(FOCAL_LARGE[name](), to_host(win), [wwant], nthreads=8)
+    wgot = to_device(like(to_host(win)))
+    assert engine.process(FOCAL_LARGE[name](), [wgot], [win]) is None
+    assert_same_raster(to_host(wgot), wwant, name + " window")
+
+
 def test_features_equal_separate_calls():
     """terrain.Features (terrain/features.go): every output equals its op run
     alone, with mixed radii (each output its own edge ring), host and device."""
