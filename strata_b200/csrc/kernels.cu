@@ -5,12 +5,8 @@
 // of the raster's border get NaN (internal/exec/halo.go:61-92). Ops whose
 // reference form is separable (ColumnX then RowX,
 // internal/focalrow/focalrow.go:153-315) keep that two-pass order inside
-// the tile, so every cell folds its terms in the reference's order.
-//
-// Validity kernel: one thread owns one 32-bit word of the output mask and
-// writes only the bits of the output's own cells, the AND of the input's
-// bits over each cell's window (internal/stencil/mask.go:43-161), with
-// every other bit of the word preserved.
+// the tile, so every cell folds its terms in the reference's order. The
+// validity of the outputs is written by validity.cu.
 #include "cellops.cuh"
 #include "focalops.cuh"
 #include "launch.h"
@@ -126,16 +122,6 @@ __global__ void __launch_bounds__(256) pointwise_kernel(const __grid_constant__ 
 // Validity.
 
 
-// One thread per (row, 32-bit word) of the output region: a block of 32
-// words x 8 rows, the rows in a grid-stride loop past 65535 x 8 of them.
-__global__ void __launch_bounds__(256) validity_kernel(const __grid_constant__ ValidityParams v) {
-    const int64_t wpr = (v.out_x1 - v.out_x0 + 31) / 32 + 1;  // words a row of the region can touch
-    const int64_t k = blockIdx.x * 32 + threadIdx.x;
-    if (k >= wpr) return;
-    for (int64_t y = v.out_y0 + blockIdx.y * 8 + threadIdx.y; y < v.out_y1; y += (int64_t)gridDim.y * 8)
-        row_word_validity(v, y, v.out_x0, v.out_x1, k);
-}
-
 template <int OP, int R>
 int64_t launch_tiles(const LaunchParams& p0, cudaStream_t s) {
     LaunchParams p = p0;
@@ -234,13 +220,5 @@ int64_t launch_data(const LaunchParams& p, cudaStream_t s, int64_t* window_cells
     return tiles;
 }
 
-void launch_validity(const ValidityParams& v, cudaStream_t s) {
-    if (v.dst_words <= 0 || v.out_x1 <= v.out_x0 || v.out_y1 <= v.out_y0) return;
-    const int64_t wpr = (v.out_x1 - v.out_x0 + 31) / 32 + 1;
-    const int64_t rows = v.out_y1 - v.out_y0;
-    const int64_t gy = (rows + 7) / 8;
-    const dim3 grid((unsigned)((wpr + 31) / 32), (unsigned)(gy < 65535 ? gy : 65535));
-    validity_kernel<<<grid, dim3(32, 8), 0, s>>>(v);
-}
 
 }  // namespace strata
