@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <algorithm>
 #include <cstring>
+#include <limits>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -396,6 +397,167 @@ int check_opts(const strata_exec_opts* o) {
     return STRATA_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Folding a pointwise tail that ends in Reclass into one Reclass table.
+//
+// A Lookup followed by Reclass stages (or Reclass stages alone) maps each
+// cell to a step function of its value: between two lookup knots the
+// interpolation y0 + (v - x0) / (x1 - x0) * (y1 - y0), each step rounded,
+// is monotone in v, so the first Reclass's class index is monotone there
+// and changes at a few float thresholds. Those thresholds, found by
+// bisection over the floats in order, with the classes' values carried
+// through the remaining Reclass stages, form one Reclass table that gives
+// every non-NaN cell the same bits as the stages run one after another
+// (and NaN passes through both). The host arithmetic below is the
+// device's (internal/curve/scalar.go:39-114): IEEE float32 operations
+// rounded to nearest, built without contraction.
+
+float host_lookup(float v, const float* xs, const float* ys, int n) {
+    int k = 0;
+    while (k < n && xs[k] <= v) k++;
+    const int lo = k == 0 ? 0 : k - 1, hi = k == n ? n - 1 : k;
+    const float x0 = xs[lo], y0 = ys[lo];
+    const float t = (v - x0) / (xs[hi] - x0);
+    float r = y0 + t * (ys[hi] - y0);
+    if (v == x0) r = y0;
+    if (k == n) r = ys[n - 1];
+    if (k == 0) r = ys[0];
+    return v != v ? v : r;
+}
+
+int host_class(float v, const float* breaks, int nb) {
+    int k = 0;
+    while (k < nb && breaks[k] <= v) k++;
+    return k;
+}
+
+float host_reclass(float v, const float* breaks, int nb, const float* values) {
+    return v != v ? v : values[host_class(v, breaks, nb)];
+}
+
+// Floats in order as unsigned keys (-0 just below +0), and back.
+uint32_t float_key(float f) {
+    uint32_t b;
+    memcpy(&b, &f, 4);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+float key_float(uint32_t k) {
+    const uint32_t b = (k & 0x80000000u) ? (k & 0x7fffffffu) : ~k;
+    float f;
+    memcpy(&f, &b, 4);
+    return f;
+}
+
+bool moderate(const float* v, int n) {
+    for (int i = 0; i < n; i++)
+        if (!(v[i] >= -1e30f && v[i] <= 1e30f)) return false;
+    return true;
+}
+
+// The fold of p's pointwise stages into one Reclass, if they fold: true
+// and the stage in *out, else false.
+bool fold_stages(const LaunchParams& p, EpiStage* out) {
+    const int n = p.nepi;
+    if (n < 2) return false;
+    const EpiStage* e = p.epi;
+    const bool lookup = e[0].op == STRATA_OP_LOOKUP;
+    const int r1 = lookup ? 1 : 0;  // the first Reclass
+    for (int i = r1; i < n; i++)
+        if (e[i].op != STRATA_OP_RECLASS) return false;
+    if (lookup && (!moderate(e[0].a, e[0].n) || !moderate(e[0].b, e[0].n))) return false;
+    if (lookup)
+        for (int i = 0; i + 1 < e[0].n; i++)
+            if (!std::isfinite(e[0].a[i + 1] - e[0].a[i]) || !std::isfinite(e[0].b[i + 1] - e[0].b[i])) return false;
+    // The value of class c of the first Reclass after the later ones.
+    auto carry = [&](int c) {
+        float v = e[r1].b[c];
+        for (int i = r1 + 1; i < n; i++) v = host_reclass(v, e[i].a, e[i].n, e[i].b);
+        return v;
+    };
+    auto cls = [&](float v) {
+        const float u = lookup ? host_lookup(v, e[0].a, e[0].b, e[0].n) : v;
+        return host_class(u, e[r1].a, e[r1].n);
+    };
+    float brk[STRATA_MAX_KNOTS] = {}, val[STRATA_MAX_KNOTS + 1] = {};
+    int nb = 0;
+    bool fits = true;
+    auto same = [](float a, float b) { return memcmp(&a, &b, 4) == 0; };
+    auto step_to = [&](float at, float v) {
+        if (same(v, val[nb])) return;
+        if (nb == STRATA_MAX_KNOTS) {
+            fits = false;
+            return;
+        }
+        brk[nb++] = at;
+        val[nb] = v;
+    };
+    // The pieces on which the class index is monotone: between the
+    // lookup's knots (or, with no Lookup, between the first Reclass's
+    // breaks, where it is constant).
+    const float* knots = lookup ? e[0].a : e[r1].a;
+    const int nk = lookup ? e[0].n : e[r1].n;
+    const float ninf = -std::numeric_limits<float>::infinity();
+    int c = cls(ninf);
+    val[0] = carry(c);
+    for (int k = 0; k < nk && fits; k++) {
+        uint32_t lo = float_key(knots[k]);
+        const uint32_t end = k + 1 < nk ? float_key(knots[k + 1]) : float_key(std::numeric_limits<float>::infinity()) + 1;
+        c = cls(knots[k]);
+        step_to(knots[k], carry(c));
+        // the next change of class inside [lo, end): bisect the monotone index
+        while (fits && lo + 1 < end && cls(key_float(end - 1)) != c) {
+            uint32_t a = lo, b = end - 1;  // cls(a) == c, cls(b) != c
+            while (b - a > 1) {
+                const uint32_t m = a + (b - a) / 2;
+                (cls(key_float(m)) == c ? a : b) = m;
+            }
+            c = cls(key_float(b));
+            step_to(key_float(b), carry(c));
+            lo = b;
+        }
+    }
+    if (!fits) return false;
+    memset(out, 0, sizeof *out);
+    out->op = STRATA_OP_RECLASS;
+    out->n = nb;
+    memcpy(out->a, brk, sizeof(float) * nb);
+    memcpy(out->b, val, sizeof(float) * (nb + 1));
+    return true;
+}
+
+// Replaces p's pointwise stages by their fold when they fold, remembering
+// the last few folds of the calling thread (a fold bisects the floats, a
+// cached one is a table compare).
+void fold_tail(LaunchParams& p) {
+    if (p.nepi < 2) return;
+    struct Entry {
+        int nepi = 0;
+        EpiStage in[strata::kMaxEpilogue];
+        bool folds = false;
+        EpiStage out;
+    };
+    thread_local Entry cache[4];
+    thread_local int next = 0;
+    const size_t bytes = sizeof(EpiStage) * (size_t)p.nepi;
+    for (const Entry& c : cache)
+        if (c.nepi == p.nepi && memcmp(c.in, p.epi, bytes) == 0) {
+            if (c.folds) {
+                p.epi[0] = c.out;
+                p.nepi = 1;
+            }
+            return;
+        }
+    Entry& c = cache[next];
+    next = (next + 1) % 4;
+    c.nepi = p.nepi;
+    memcpy(c.in, p.epi, bytes);
+    c.folds = fold_stages(p, &c.out);
+    if (c.folds) {
+        p.epi[0] = c.out;
+        p.nepi = 1;
+    }
+}
+
 // Resolves stages into launch parameters (op, radius, epilogue).
 int plan_stages(const strata_stage* stages, int nstages, LaunchParams& p, int* nout) {
     if (!stages || nstages < 1) return fail(STRATA_EINVAL, "engine: nil kernel");
@@ -424,6 +586,7 @@ int plan_stages(const strata_stage* stages, int nstages, LaunchParams& p, int* n
         }
     }
     p.nepi = epi;
+    fold_tail(p);
     *nout = s0.op == STRATA_OP_GRADIENT ? 2 : 1;
     return STRATA_OK;
 }

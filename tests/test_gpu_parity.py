@@ -145,6 +145,84 @@ def test_lookup_and_reclass():
     run_matrix(lambda: transfer.reclass_stage(BREAKS, VALUES), cells)
 
 
+def _near(vals, ulps=40):
+    """Every float within ulps of each value, stepping through the floats
+    in order (-0 next to +0)."""
+    out = []
+    for v in np.asarray(vals, np.float32):
+        if not np.isfinite(v):
+            continue
+        b = int(np.array([v], np.float32).view(np.uint32)[0])
+        key = (b | 0x80000000) if b < 0x80000000 else (~b & 0xFFFFFFFF)
+        keys = np.arange(key - ulps, key + ulps + 1, dtype=np.int64).clip(0x00800000, 0xFF7FFFFF)
+        bits = np.where(keys >= 0x80000000, keys & 0x7FFFFFFF, ~keys & 0xFFFFFFFF)
+        out.append(bits.astype(np.uint32).view(np.float32))
+    return np.concatenate(out) if out else np.zeros(0, np.float32)
+
+
+def _tail_cells(xs, ys, breaks, seed):
+    """Cells on and around every knot, every break's preimage under the
+    lookup (where the class changes), ±0, infinities, NaN and random floats."""
+    rng = np.random.default_rng(seed)
+    pre = []
+    for k in range(len(xs) - 1):
+        x0, x1, y0, y1 = float(xs[k]), float(xs[k + 1]), float(ys[k]), float(ys[k + 1])
+        if y1 != y0:
+            for b in breaks:
+                t = (float(b) - y0) / (y1 - y0)
+                if 0 <= t <= 1:
+                    pre.append(x0 + t * (x1 - x0))
+    vals = np.concatenate([_near(xs), _near(pre), _near(breaks), _near([0.0], 8),
+                           np.array([np.inf, -np.inf, np.nan, 1e30, -1e30], np.float32),
+                           rng.standard_normal(4000).astype(np.float32) * float(np.abs(xs).max() + 1),
+                           rng.integers(0, 2**32, 2000, dtype=np.uint64).astype(np.uint32).view(np.float32)])
+    w = 257
+    h = (len(vals) + w - 1) // w
+    cells = np.full(w * h, 1.5, np.float32)
+    cells[:len(vals)] = vals
+    return cells.reshape(h, w)
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_folded_pointwise_tail_edges(seed):
+    """A Lookup followed by Reclass stages (and Reclass stages alone) runs as
+    one folded Reclass table on the device; on cells at and around every
+    knot, every class threshold, ±0, ±inf and NaN it equals the oracle's
+    stages run one after another, bit for bit."""
+    rng = np.random.default_rng(100 + seed)
+    nk = int(rng.integers(2, 9))
+    xs = np.sort(rng.choice(np.arange(-50, 50), nk, replace=False)).astype(np.float32) * np.float32(0.37)
+    ys = (rng.standard_normal(nk) * 10).astype(np.float32)  # segments rise and fall
+    nb = int(rng.integers(1, 7))
+    breaks = np.sort(rng.choice(np.arange(-30, 30), nb, replace=False)).astype(np.float32) * np.float32(0.71)
+    values = (rng.standard_normal(nb + 1) * 3).astype(np.float32)
+    if seed % 2:
+        values[int(rng.integers(nb + 1))] = np.nan  # a NoData class
+    breaks2 = np.sort(values[np.isfinite(values)])[:2] + np.float32(0.25)
+    breaks2 = np.unique(breaks2)
+    values2 = np.arange(len(breaks2) + 1, dtype=np.float32) * 10
+    chains = {
+        "lookup_reclass": lambda: transfer.lookup_stage(xs, ys).extend(transfer.reclass_stage(breaks, values)),
+        "lookup_reclass_reclass": lambda: transfer.lookup_stage(xs, ys).extend(
+            transfer.reclass_stage(breaks, values)).extend(transfer.reclass_stage(breaks2, values2)),
+        "reclass_reclass": lambda: transfer.reclass_stage(breaks, values).extend(
+            transfer.reclass_stage(breaks2, values2)),
+    }
+    cells = _tail_cells(xs, ys, breaks, seed)
+    h, w = cells.shape
+    for name, make in chains.items():
+        for device in (False, True):
+            lay = dict(src=dict(stride=None, offset=0, valid=synth.cell_mask(w, h, seed, 0.05)),
+                       dst=dict(stride=None, offset=0, masked=True))
+            check_case(make(), cells, 1, device, lay, f"{name} seed={seed} device={device}")
+    # after a stencil, in the marching kernel's epilogue
+    dem = dem_cells(300, 200, seed) * np.float32(0.05)
+    lay = dict(src=dict(stride=None, offset=0, valid=None), dst=dict(stride=None, offset=0, masked=False))
+    check_case(terrain.slope_stage(terrain.SlopeOptions(CellSize=1)).extend(
+        transfer.lookup_stage(xs, ys)).extend(transfer.reclass_stage(breaks, values)), dem, 1, True, lay,
+        f"slope+tail seed={seed}")
+
+
 def test_pipeline_slope_lookup_reclass():
     """The fused Slope -> Lookup -> Reclass pass equals the oracle's three
     stages, which equal three separate calls (internal/exec/pipeline.go)."""
