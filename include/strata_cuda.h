@@ -236,9 +236,12 @@ int strata_process_chunked(strata_ctx *ctx, const strata_stage *stages, int nsta
  * edge and validity rules of strata_process per raster. strata_batch_create
  * checks every item as strata_process would, groups the rasters by op
  * class, uploads their descriptors and captures one persistent kernel per
- * class into a CUDA graph; strata_batch_run replays it with one launch
- * (synchronize != 0 waits for it). tile_width / tile_height pick an item's
- * output tile (0 = 64 x 32); the Python autotuner chooses them per class.
+ * class (and one per validity radius) into a CUDA graph on parallel
+ * branches; strata_batch_run replays it with one launch (synchronize != 0
+ * waits for it). tile_height picks the rows of an item's work units (0 =
+ * the kernel's default, at most 1024; the windowed focal ops at radius > 1
+ * use fixed tiles); tile_width is not used, the kernels fix the units'
+ * width. The Python autotuner chooses tile_height per class.
  * The rasters must stay allocated, and the batch be run on one stream at a
  * time, until strata_batch_destroy.
  */

@@ -1,5 +1,5 @@
 """Batches: many device-resident rasters of mixed sizes and ops in one
-CUDA-graph launch, with tile shapes from an autotuner.
+CUDA-graph launch, with band heights from an autotuner.
 
     items = [batch.Item(terrain.slope_stage(opts), src, [dst]), ...]
     b = batch.Batch(items)          # plans, uploads descriptors, captures the graph
@@ -7,9 +7,13 @@ CUDA-graph launch, with tile shapes from an autotuner.
 
 Each item is one pipeline over one raster, with strata_process's edge and
 validity rules, so a raster's result is the same alone and in a batch.
-The tile shape of each op class comes from the Autotuner: it times the
-candidate shapes on a probe raster of the class once per device and
-caches the winner (in memory, and in a JSON file when a path is given).
+A raster's work units are bands of rows (512 columns wide for the
+marching kernels, a band of 512 column results for the separable focal
+ops; the windowed focal ops use fixed tiles). The band height of each op
+class comes from the Autotuner: it times the candidate heights on a probe
+raster of the class once per device and caches the winner (in memory, and
+in a JSON file when a path is given). An item's tile is (width, height):
+the width is fixed by the kernel and not used, the height is the band.
 """
 from __future__ import annotations
 
@@ -26,10 +30,10 @@ import numpy as np
 from . import _lib, engine
 from .raster import Float32Raster, StrataPanic
 
-# Candidate output tiles (width, height): wide tiles read fewer halo
-# columns per cell, tall ones fewer halo rows; the best depends on the
-# radius and on how the op's cost compares with its loads.
-CANDIDATES: List[Tuple[int, int]] = [(64, 32), (128, 16), (32, 64), (128, 32), (64, 64), (256, 16)]
+# Candidate bands (rows per work unit), as (width, height) tiles whose
+# width the kernels fix: short bands spread a raster over more blocks,
+# tall ones re-read fewer halo rows per cell.
+CANDIDATES: List[Tuple[int, int]] = [(512, 16), (512, 32), (512, 64), (512, 128), (512, 256)]
 
 
 @dataclass
@@ -98,7 +102,7 @@ class Batch:
 
 
 class Autotuner:
-    """Picks each op class's tile shape by timing the candidates on a probe
+    """Picks each op class's band height by timing the candidates on a probe
     raster of the class (probe x probe cells, seeded), once per device;
     results are cached in memory and, with a path, in a JSON file keyed by
     the device name."""

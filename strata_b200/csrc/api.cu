@@ -1625,9 +1625,89 @@ extern "C" int strata_process_features(strata_ctx* c, const strata_stage* stages
 // once (descriptors uploaded, one persistent kernel per op class captured
 // in a CUDA graph) and run with one graph launch.
 
+namespace {
+
+bool aligned16_host(const void* q) { return ((uintptr_t)q & 15) == 0; }
+
+// Checks batch item i as strata_process would and resolves it into a
+// planned-to-be descriptor (its requested band in b.th). Allocates nothing.
+int fill_batch_item(strata_ctx* c, const strata_batch_item& it, int i, strata::BatchItem& b, int* nout_out) {
+    LaunchParams p;
+    int nout = 0, rc;
+    if ((rc = plan_stages(it.stages, it.nstages, p, &nout))) return rc;
+    if ((rc = check_operands(&it.src, 1, it.dst, nout, nout, p.radius))) return rc;
+    if (!it.src.on_device || !it.dst[0].on_device || (nout > 1 && !it.dst[1].on_device))
+        return fail(STRATA_EINVAL, "engine: batch raster %d: the rasters of a batch must be on the device", i);
+    if (p.op == STRATA_OP_LOOKUP || p.op == STRATA_OP_RECLASS)
+        return fail(STRATA_ENOTSUP, "engine: batch raster %d: a pointwise op alone has no batch kernel", i);
+    if (it.tile_height < 0 || it.tile_height > 1024)
+        return fail(STRATA_EINVAL, "engine: batch raster %d: band of %d rows (0 to 1024)", i, it.tile_height);
+    DevOperand ds, dd[2];
+    if ((rc = stage_in(c, nullptr, it.src, 0, false, &ds))) return rc;
+    for (int k = 0; k < nout; k++)
+        if ((rc = stage_in(c, nullptr, it.dst[k], 0, false, &dd[k]))) return rc;
+    const int64_t W = it.src.width, H = it.src.height;
+    p.src = ds.data;
+    p.src_stride = ds.stride;
+    p.src_x0 = p.src_y0 = 0;
+    p.src_w = W;
+    p.src_h = H;
+    p.dst0 = dd[0].data;
+    p.dst0_stride = dd[0].stride;
+    if (nout > 1) {
+        p.dst1 = dd[1].data;
+        p.dst1_stride = dd[1].stride;
+    }
+    p.dst_x0 = p.dst_y0 = 0;
+    p.width = W;
+    p.height = H;
+    p.out_x0 = p.out_y0 = 0;
+    p.out_x1 = W;
+    p.out_y1 = H;
+    memset(&b, 0, sizeof b);
+    b.p = p;
+    for (int k = 0; k < nout; k++) {
+        if (!it.dst[k].valid) continue;
+        fill_validity(b.v[b.nvalid], ds, it.src.valid != nullptr, dd[k], span_cells(it.dst[k]), W, H, p.radius, 0, H);
+        b.nvalid++;
+    }
+    b.th = it.tile_height;
+    b.vec = aligned16_host(p.src) && aligned16_host(p.dst0) && !(p.src_stride & 3) && !(p.dst0_stride & 3) &&
+            (nout < 2 || (aligned16_host(p.dst1) && !(p.dst1_stride & 3)));
+    *nout_out = nout;
+    return STRATA_OK;
+}
+
+// Launches planned classes on stream st, each data class and the validity
+// on branches of their own (forked from and joined back to st, so a
+// capture of st records them as parallel graph nodes).
+int launch_planned(const strata::BatchClass* cls, int nc, const strata::BatchItem* d_items,
+                   const strata::ValidityClass* vcls, int nvc, const strata::ValidityItem* d_vitems, cudaStream_t st,
+                   cudaStream_t* branch, int nbranch, cudaEvent_t* ev) {
+    cudaError_t e = cudaEventRecord(ev[0], st);
+    for (int k = 0; k < nbranch && e == cudaSuccess; k++) e = cudaStreamWaitEvent(branch[k], ev[0], 0);
+    if (e != cudaSuccess) return cuda_fail(e, "batch fork");
+    for (int i = 0; i < nc; i++)
+        if (!strata::launch_batch_class(cls[i], d_items, branch[i % nbranch]))
+            return fail(STRATA_ENOTSUP, "engine: an op of the batch has no batch kernel");
+    for (int i = 0; i < nvc; i++) strata::launch_batch_validity(vcls[i], d_vitems, branch[(nc + i) % nbranch]);
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "batch launch");
+    for (int k = 0; k < nbranch && e == cudaSuccess; k++) {
+        e = cudaEventRecord(ev[1 + k], branch[k]);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(st, ev[1 + k], 0);
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "batch join");
+    return STRATA_OK;
+}
+
+constexpr int kBranches = 4;
+
+}  // namespace
+
 struct strata_batch {
     strata_ctx* ctx = nullptr;
-    strata::BatchItem* d_items = nullptr;  // the descriptors, on the device
+    strata::BatchItem* d_items = nullptr;       // the descriptors, on the device
+    strata::ValidityItem* d_vitems = nullptr;  // the validity descriptors
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int classes = 0;
@@ -1642,131 +1722,71 @@ extern "C" int strata_batch_create(strata_ctx* c, const strata_batch_item* items
     std::lock_guard<std::mutex> lock(c->mu);
     cudaSetDevice(c->device);
     std::vector<strata::BatchItem> host((size_t)nitems);
-    std::vector<std::pair<std::pair<int, int>, int>> keyed;  // ((op, radius), item)
     int64_t cells = 0, in_bytes = 0, out_bytes = 0;
     for (int i = 0; i < nitems; i++) {
-        const strata_batch_item& it = items[i];
-        LaunchParams p;
         int nout = 0, rc;
-        if ((rc = plan_stages(it.stages, it.nstages, p, &nout))) return rc;
-        if ((rc = check_operands(&it.src, 1, it.dst, nout, nout, p.radius))) return rc;
-        if (!it.src.on_device || !it.dst[0].on_device || (nout > 1 && !it.dst[1].on_device))
-            return fail(STRATA_EINVAL, "engine: batch raster %d: the rasters of a batch must be on the device", i);
-        if (p.op == STRATA_OP_LOOKUP || p.op == STRATA_OP_RECLASS)
-            return fail(STRATA_ENOTSUP, "engine: batch raster %d: a pointwise op alone has no batch kernel", i);
-        DevOperand ds, dd[2];
-        if ((rc = stage_in(c, nullptr, it.src, 0, false, &ds))) return rc;
-        for (int k = 0; k < nout; k++)
-            if ((rc = stage_in(c, nullptr, it.dst[k], 0, false, &dd[k]))) return rc;
-        const int64_t W = it.src.width, H = it.src.height;
-        p.src = ds.data;
-        p.src_stride = ds.stride;
-        p.src_x0 = p.src_y0 = 0;
-        p.src_w = W;
-        p.src_h = H;
-        p.dst0 = dd[0].data;
-        p.dst0_stride = dd[0].stride;
-        if (nout > 1) {
-            p.dst1 = dd[1].data;
-            p.dst1_stride = dd[1].stride;
-        }
-        p.dst_x0 = p.dst_y0 = 0;
-        p.width = W;
-        p.height = H;
-        p.out_x0 = p.out_y0 = 0;
-        p.out_x1 = W;
-        p.out_y1 = H;
-        p.status = c->d_status;
-        strata::BatchItem& b = host[(size_t)i];
-        memset(&b, 0, sizeof b);
-        b.p = p;
-        for (int k = 0; k < nout; k++) {
-            if (!it.dst[k].valid) continue;
-            fill_validity(b.v[b.nvalid], ds, it.src.valid != nullptr, dd[k], span_cells(it.dst[k]), W, H, p.radius, 0,
-                          H);
-            b.nvalid++;
-        }
-        b.tw = it.tile_width > 0 ? it.tile_width : 64;
-        b.th = it.tile_height > 0 ? it.tile_height : 32;
-        if (b.tw > 1024 || b.th > 1024 || strata::batch_smem_bytes(p.op, p.radius, b.tw, b.th) > 200 * 1024)
-            return fail(STRATA_EINVAL, "engine: batch raster %d: tile %d x %d is too large", i, b.tw, b.th);
-        b.tiles_x = (W + b.tw - 1) / b.tw;
-        keyed.push_back({{p.op, p.radius}, i});
-        cells += W * H;
-        in_bytes += W * H * 4;
-        out_bytes += W * H * 4 * nout;
+        if ((rc = fill_batch_item(c, items[i], i, host[(size_t)i], &nout))) return rc;
+        host[(size_t)i].p.status = c->d_status;
+        const int64_t n = items[i].src.width * items[i].src.height;
+        cells += n;
+        in_bytes += n * 4;
+        out_bytes += n * 4 * nout;
     }
-    // Group by class; each class's rasters get consecutive work units.
-    std::stable_sort(keyed.begin(), keyed.end(),
-                     [](const auto& a, const auto& b) { return a.first < b.first; });
-    std::vector<strata::BatchItem> ordered;
-    ordered.reserve((size_t)nitems);
-    struct Class {
-        int op, radius;
-        int first, count;
-        int64_t total;
-        size_t smem;
-    };
-    std::vector<Class> classes;
+    std::vector<int> order((size_t)nitems);
+    std::vector<strata::BatchClass> cls((size_t)nitems);
     int64_t window = 0;
-    for (size_t i = 0; i < keyed.size();) {
-        Class cl{keyed[i].first.first, keyed[i].first.second, (int)ordered.size(), 0, 0, 0};
-        for (; i < keyed.size() && keyed[i].first == std::make_pair(cl.op, cl.radius); i++) {
-            strata::BatchItem b = host[(size_t)keyed[i].second];
-            const int64_t ty = (b.p.height + b.th - 1) / b.th;
-            b.tile0 = cl.total;
-            cl.total += b.tiles_x * ty;
-            cl.smem = std::max(cl.smem, strata::batch_smem_bytes(cl.op, cl.radius, b.tw, b.th));
-            window += (int64_t)(b.tw + 2 * cl.radius) * (b.th + 2 * cl.radius) * b.tiles_x * ty;
-            ordered.push_back(b);
-            cl.count++;
-        }
-        classes.push_back(cl);
-    }
+    const int nc = strata::batch_plan(host.data(), nitems, order.data(), cls.data(), &window);
+    if (nc < 0) return fail(STRATA_ENOTSUP, "engine: an op of the batch has no batch kernel");
+    std::vector<strata::ValidityItem> vitems((size_t)(2 * nitems));
+    strata::ValidityClass vcls[STRATA_MAX_RADIUS + 1];
+    int nvc = 0;
+    const int nv = strata::batch_plan_validity(host.data(), nitems, vitems.data(), vcls, &nvc);
+
     auto* B = new strata_batch;
     B->ctx = c;
-    B->classes = (int)classes.size();
+    B->classes = nc;
     B->cells = cells;
     B->in_bytes = in_bytes;
     B->out_bytes = out_bytes;
     B->window = window;
-    cudaError_t e = cudaMalloc(&B->d_items, sizeof(strata::BatchItem) * ordered.size());
+    for (int i = 0; i < nc; i++) B->tiles += cls[(size_t)i].total;
+    cudaError_t e = cudaMalloc(&B->d_items, sizeof(strata::BatchItem) * (size_t)nitems);
     if (e == cudaSuccess)
-        e = cudaMemcpy(B->d_items, ordered.data(), sizeof(strata::BatchItem) * ordered.size(), cudaMemcpyHostToDevice);
+        e = cudaMemcpy(B->d_items, host.data(), sizeof(strata::BatchItem) * (size_t)nitems, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && nv > 0) e = cudaMalloc(&B->d_vitems, sizeof(strata::ValidityItem) * (size_t)nv);
+    if (e == cudaSuccess && nv > 0)
+        e = cudaMemcpy(B->d_vitems, vitems.data(), sizeof(strata::ValidityItem) * (size_t)nv, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
         strata_batch_destroy(B);
         return cuda_fail(e, "batch descriptors");
     }
-    int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
-    // Capture every class's persistent kernel into one graph.
-    cudaStream_t cap;
-    if ((e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking)) != cudaSuccess) {
-        strata_batch_destroy(B);
-        return cuda_fail(e, "capture stream");
+    // Capture every class's persistent kernel into one graph, the classes
+    // on parallel branches.
+    cudaStream_t cap = nullptr, br[kBranches] = {};
+    cudaEvent_t ev[1 + kBranches] = {};
+    e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
+    for (int k = 0; k < kBranches && e == cudaSuccess; k++) e = cudaStreamCreateWithFlags(&br[k], cudaStreamNonBlocking);
+    for (int k = 0; k < 1 + kBranches && e == cudaSuccess; k++) e = cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming);
+    int rc = STRATA_OK;
+    if (e == cudaSuccess) e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        rc = launch_planned(cls.data(), nc, B->d_items, vcls, nvc, B->d_vitems, cap, br, kBranches, ev);
+        cudaError_t e2 = cudaStreamEndCapture(cap, &B->graph);
+        if (rc == STRATA_OK && e2 == cudaSuccess) e2 = cudaGraphInstantiate(&B->exec, B->graph, 0);
+        if (rc == STRATA_OK && e2 != cudaSuccess) rc = cuda_fail(e2, "batch graph");
+    } else {
+        rc = cuda_fail(e, "batch capture");
     }
-    e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
-    bool ok = e == cudaSuccess;
-    for (const Class& cl : classes) {
-        if (!ok) break;
-        // Enough blocks to fill the GPU at the class's occupancy, never
-        // more than its work units.
-        const int per_sm = cl.smem > 100 * 1024 ? 1 : (cl.smem > 48 * 1024 ? 2 : 4);
-        const int64_t grid = std::min<int64_t>(cl.total, (int64_t)sms * per_sm);
-        B->tiles += cl.total;
-        ok = strata::launch_batch_class(cl.op, cl.radius, B->d_items + cl.first, cl.count, cl.total, (int)grid,
-                                        cl.smem, cap);
-    }
-    cudaError_t e2 = cudaStreamEndCapture(cap, &B->graph);
-    if (ok && e2 == cudaSuccess) e2 = cudaGraphInstantiate(&B->exec, B->graph, 0);
-    cudaStreamDestroy(cap);
-    if (!ok || e2 != cudaSuccess) {
+    for (int k = 0; k < 1 + kBranches; k++)
+        if (ev[k]) cudaEventDestroy(ev[k]);
+    for (int k = 0; k < kBranches; k++)
+        if (br[k]) cudaStreamDestroy(br[k]);
+    if (cap) cudaStreamDestroy(cap);
+    if (rc != STRATA_OK) {
         cudaGetLastError();
         strata_batch_destroy(B);
-        return ok ? cuda_fail(e2, "batch graph") : fail(STRATA_ENOTSUP, "engine: an op of the batch has no batch kernel");
+        return rc;
     }
-    B->tiles = 0;
-    for (const Class& cl : classes) B->tiles += cl.total;
     *out = B;
     return STRATA_OK;
 }
@@ -1800,21 +1820,24 @@ extern "C" void strata_batch_destroy(strata_batch* B) {
     if (B->exec) cudaGraphExecDestroy(B->exec);
     if (B->graph) cudaGraphDestroy(B->graph);
     if (B->d_items) cudaFree(B->d_items);
+    if (B->d_vitems) cudaFree(B->d_vitems);
     delete B;
 }
 
 // ---------------------------------------------------------------------------
 // A batch run without allocation: the descriptors go to a fixed scratch
-// area in the module's static device memory instead of a cudaMalloc'd
-// table, and the class kernels launch straight onto the caller's stream
+// area in the module's static device memory instead of cudaMalloc'd
+// tables, and the class kernels launch straight onto the caller's stream
 // (no graph). The scratch is one per device: calls on one stream are
 // ordered by it, calls on different streams that overlap on the device
 // race on it.
 
 namespace {
 
-constexpr size_t kScratchHead = 256;  // the status word, padded so the descriptors stay 256-byte aligned
-constexpr size_t kScratchBytes = kScratchHead + sizeof(strata::BatchItem) * STRATA_NOALLOC_BATCH_MAX;
+constexpr size_t kScratchHead = 256;  // the status word, padded so the tables stay 256-byte aligned
+constexpr size_t kItemBytes = sizeof(strata::BatchItem) * STRATA_NOALLOC_BATCH_MAX;
+constexpr size_t kScratchBytes = kScratchHead + kItemBytes + sizeof(strata::ValidityItem) * 2 * STRATA_NOALLOC_BATCH_MAX;
+static_assert(kItemBytes % 16 == 0, "the validity table starts on a 16-byte boundary");
 static __device__ __align__(256) unsigned char g_batch_scratch[kScratchBytes];
 
 constexpr int kMaxDevices = 64;
@@ -1822,28 +1845,27 @@ struct ScratchSlot {
     std::once_flag once;
     cudaError_t err = cudaSuccess;
     unsigned char* ptr = nullptr;
-    int sms = 0;
 };
 ScratchSlot g_scratch[kMaxDevices];
 
-// Host staging of the descriptors and the class plan; one call at a time.
+// Host staging of the descriptors and the plan; one call at a time.
 std::mutex g_noalloc_mu;
 strata::BatchItem g_noalloc_items[STRATA_NOALLOC_BATCH_MAX];
+strata::ValidityItem g_noalloc_vitems[2 * STRATA_NOALLOC_BATCH_MAX];
 int g_noalloc_order[STRATA_NOALLOC_BATCH_MAX];
+strata::BatchClass g_noalloc_classes[STRATA_NOALLOC_BATCH_MAX];
 
 // The device address of the scratch area, looked up once per device with
 // that device current.
-int scratch_address(int device, unsigned char** ptr, int* sms) {
+int scratch_address(int device, unsigned char** ptr) {
     if (device < 0 || device >= kMaxDevices) return fail(STRATA_EINVAL, "engine: device %d out of range", device);
     ScratchSlot& s = g_scratch[device];
     std::call_once(s.once, [&] {
         s.err = cudaSetDevice(device);
         if (s.err == cudaSuccess) s.err = cudaGetSymbolAddress((void**)&s.ptr, g_batch_scratch);
-        if (s.err == cudaSuccess) s.err = cudaDeviceGetAttribute(&s.sms, cudaDevAttrMultiProcessorCount, device);
     });
     if (s.err != cudaSuccess) return cuda_fail(s.err, "batch scratch address");
     *ptr = s.ptr;
-    *sms = s.sms;
     return STRATA_OK;
 }
 
@@ -1859,117 +1881,36 @@ extern "C" int strata_batch_run_noalloc(strata_ctx* c, const strata_batch_item* 
     std::lock_guard<std::mutex> lock(c->mu);
     std::lock_guard<std::mutex> staging(g_noalloc_mu);
     unsigned char* scratch;
-    int sms, rc;
-    if ((rc = scratch_address(c->device, &scratch, &sms))) return rc;
+    int rc;
+    if ((rc = scratch_address(c->device, &scratch))) return rc;
     cudaSetDevice(c->device);
     int* d_status = reinterpret_cast<int*>(scratch);
     auto* d_items = reinterpret_cast<strata::BatchItem*>(scratch + kScratchHead);
+    auto* d_vitems = reinterpret_cast<strata::ValidityItem*>(scratch + kScratchHead + kItemBytes);
     strata::BatchItem* host = g_noalloc_items;
-    // Each raster's descriptor, as strata_batch_create plans it.
     for (int i = 0; i < nitems; i++) {
-        const strata_batch_item& it = items[i];
-        LaunchParams p;
         int nout = 0;
-        if ((rc = plan_stages(it.stages, it.nstages, p, &nout))) return rc;
-        if ((rc = check_operands(&it.src, 1, it.dst, nout, nout, p.radius))) return rc;
-        if (!it.src.on_device || !it.dst[0].on_device || (nout > 1 && !it.dst[1].on_device))
-            return fail(STRATA_EINVAL, "engine: batch raster %d: the rasters of a batch must be on the device", i);
-        if (p.op == STRATA_OP_LOOKUP || p.op == STRATA_OP_RECLASS)
-            return fail(STRATA_ENOTSUP, "engine: batch raster %d: a pointwise op alone has no batch kernel", i);
-        DevOperand ds, dd[2];
-        if ((rc = stage_in(c, nullptr, it.src, 0, false, &ds))) return rc;
-        for (int k = 0; k < nout; k++)
-            if ((rc = stage_in(c, nullptr, it.dst[k], 0, false, &dd[k]))) return rc;
-        const int64_t W = it.src.width, H = it.src.height;
-        p.src = ds.data;
-        p.src_stride = ds.stride;
-        p.src_x0 = p.src_y0 = 0;
-        p.src_w = W;
-        p.src_h = H;
-        p.dst0 = dd[0].data;
-        p.dst0_stride = dd[0].stride;
-        if (nout > 1) {
-            p.dst1 = dd[1].data;
-            p.dst1_stride = dd[1].stride;
-        }
-        p.dst_x0 = p.dst_y0 = 0;
-        p.width = W;
-        p.height = H;
-        p.out_x0 = p.out_y0 = 0;
-        p.out_x1 = W;
-        p.out_y1 = H;
-        p.status = d_status;
-        strata::BatchItem b;
-        memset(&b, 0, sizeof b);
-        b.p = p;
-        for (int k = 0; k < nout; k++) {
-            if (!it.dst[k].valid) continue;
-            fill_validity(b.v[b.nvalid], ds, it.src.valid != nullptr, dd[k], span_cells(it.dst[k]), W, H, p.radius, 0,
-                          H);
-            b.nvalid++;
-        }
-        b.tw = it.tile_width > 0 ? it.tile_width : 64;
-        b.th = it.tile_height > 0 ? it.tile_height : 32;
-        if (b.tw > 1024 || b.th > 1024 || strata::batch_smem_bytes(p.op, p.radius, b.tw, b.th) > 200 * 1024)
-            return fail(STRATA_EINVAL, "engine: batch raster %d: tile %d x %d is too large", i, b.tw, b.th);
-        b.tiles_x = (W + b.tw - 1) / b.tw;
-        host[i] = b;
+        if ((rc = fill_batch_item(c, items[i], i, host[i], &nout))) return rc;
+        host[i].p.status = d_status;
     }
-    // Group by class (op, radius), keeping the callers' order within one:
-    // an insertion sort of the indices, stable and heap-free.
-    int* order = g_noalloc_order;
-    for (int i = 0; i < nitems; i++) {
-        int j = i;
-        const auto key = std::make_pair(host[i].p.op, host[i].p.radius);
-        for (; j > 0 && key < std::make_pair(host[order[j - 1]].p.op, host[order[j - 1]].p.radius); j--)
-            order[j] = order[j - 1];
-        order[j] = i;
-    }
-    // Permute into class order in place (cycle by cycle) and number each
-    // class's work units.
-    for (int i = 0; i < nitems; i++) {
-        if (order[i] < 0) continue;
-        strata::BatchItem t = host[i];
-        int j = i;
-        while (order[j] != i) {
-            const int k = order[j];
-            host[j] = host[k];
-            order[j] = -1;
-            j = k;
-        }
-        host[j] = t;
-        order[j] = -1;
-    }
+    const int nc = strata::batch_plan(host, nitems, g_noalloc_order, g_noalloc_classes, nullptr);
+    if (nc < 0) return fail(STRATA_ENOTSUP, "engine: an op of the batch has no batch kernel");
+    strata::ValidityClass vcls[STRATA_MAX_RADIUS + 1];
+    int nvc = 0;
+    const int nv = strata::batch_plan_validity(host, nitems, g_noalloc_vitems, vcls, &nvc);
     cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
     cudaError_t e = cudaMemsetAsync(d_status, 0, sizeof(int), st);
-    if (e != cudaSuccess) return cuda_fail(e, "batch status");
-    int64_t total = 0;
-    for (int i = 0; i < nitems; i++) {
-        if (i > 0 && (host[i].p.op != host[i - 1].p.op || host[i].p.radius != host[i - 1].p.radius)) total = 0;
-        const int64_t ty = (host[i].p.height + host[i].th - 1) / host[i].th;
-        host[i].tile0 = total;
-        total += host[i].tiles_x * ty;
-    }
-    e = cudaMemcpyAsync(d_items, host, sizeof(strata::BatchItem) * (size_t)nitems, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_items, host, sizeof(strata::BatchItem) * (size_t)nitems, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && nv > 0)
+        e = cudaMemcpyAsync(d_vitems, g_noalloc_vitems, sizeof(strata::ValidityItem) * (size_t)nv,
+                            cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return cuda_fail(e, "batch descriptors");
-    for (int first = 0; first < nitems;) {
-        const int op = host[first].p.op, radius = host[first].p.radius;
-        int last = first;
-        size_t smem = 0;
-        int64_t units = 0;
-        for (; last < nitems && host[last].p.op == op && host[last].p.radius == radius; last++) {
-            smem = std::max(smem, strata::batch_smem_bytes(op, radius, host[last].tw, host[last].th));
-            units = host[last].tile0 + host[last].tiles_x * ((host[last].p.height + host[last].th - 1) / host[last].th);
-        }
-        const int per_sm = smem > 100 * 1024 ? 1 : (smem > 48 * 1024 ? 2 : 4);
-        const int64_t grid = std::min<int64_t>(units, (int64_t)sms * per_sm);
-        if (!strata::launch_batch_class(op, radius, d_items + first, last - first, units, (int)grid, smem, st)) {
-            cudaGetLastError();
+    for (int i = 0; i < nc; i++)
+        if (!strata::launch_batch_class(g_noalloc_classes[i], d_items, st))
             return fail(STRATA_ENOTSUP, "engine: an op of the batch has no batch kernel");
-        }
-        if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "batch launch");
-        first = last;
-    }
+    for (int i = 0; i < nvc; i++) strata::launch_batch_validity(vcls[i], d_vitems, st);
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "batch launch");
     if (!synchronize) return STRATA_OK;
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "batch run");
     int status = 0;
@@ -2022,6 +1963,10 @@ struct Slot {
     cudaEvent_t done = nullptr;
     strata::BatchItem* d_items = nullptr;
     strata::BatchItem* h_items = nullptr;  // page-locked staging
+    strata::ValidityItem* d_vitems = nullptr;
+    strata::ValidityItem* h_vitems = nullptr;  // page-locked staging
+    std::vector<int> order;
+    std::vector<strata::BatchClass> classes;
     std::vector<Request*> reqs;
     bool busy = false;
 };
@@ -2051,67 +1996,56 @@ struct strata_server {
 namespace {
 
 // Launches one batch of admitted requests on slot s (scheduler thread,
-// with the server lock held).
+// with the server lock held): each request a raster of the batch, planned
+// and run by the batch kernels, its validity alongside.
 int launch_batch(strata_server* S, Slot& s) {
     cudaStream_t st = s.stream;
-    std::vector<std::pair<std::pair<int, int>, int>> keyed;
-    for (int i = 0; i < (int)s.reqs.size(); i++) keyed.push_back({{s.reqs[i]->p.op, s.reqs[i]->p.radius}, i});
-    std::stable_sort(keyed.begin(), keyed.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
-    struct Class {
-        int op, radius, first, count;
-        int64_t total;
-        size_t smem;
-    };
-    std::vector<Class> classes;
-    int n = 0;
-    for (size_t i = 0; i < keyed.size();) {
-        Class cl{keyed[i].first.first, keyed[i].first.second, n, 0, 0, 0};
-        for (; i < keyed.size() && keyed[i].first == std::make_pair(cl.op, cl.radius); i++) {
-            Request* r = s.reqs[(size_t)keyed[i].second];
-            strata::BatchItem& b = s.h_items[n++];
-            memset(&b, 0, sizeof b);
-            b.p = r->p;
-            b.tw = 64;
-            b.th = 32;
-            b.tiles_x = (r->w + b.tw - 1) / b.tw;
-            b.tile0 = cl.total;
-            cl.total += b.tiles_x * ((r->h + b.th - 1) / b.th);
-            for (int k = 0; k < r->nout; k++) {
-                if (!r->out_bits[k]) continue;
-                ValidityParams& v = b.v[b.nvalid++];
-                memset(&v, 0, sizeof v);
-                if (S->mosaic.valid) {
-                    v.src_bits = S->dm.bits;
-                    v.src_off = S->dm.bit_off + r->y * S->dm.stride + r->x;
-                    v.src_stride = S->dm.stride;
-                    v.src_lo_word = S->dm.lo_word;
-                    v.src_hi_word = S->dm.hi_word;
-                }
-                v.dst_bits = r->out_bits[k];
-                v.dst_off = 0;
-                v.dst_stride = r->w;
-                v.out_x1 = r->w;
-                v.out_y1 = r->h;
-                v.width = r->w;
-                v.height = r->h;
-                v.radius = r->p.radius;
-                v.dst_words = (r->w * r->h + 31) / 32;
+    const int n = (int)s.reqs.size();
+    for (int i = 0; i < n; i++) {
+        Request* r = s.reqs[(size_t)i];
+        strata::BatchItem& b = s.h_items[i];
+        memset(&b, 0, sizeof b);
+        b.p = r->p;
+        for (int k = 0; k < r->nout; k++) {
+            if (!r->out_bits[k]) continue;
+            ValidityParams& v = b.v[b.nvalid++];
+            memset(&v, 0, sizeof v);
+            if (S->mosaic.valid) {
+                v.src_bits = S->dm.bits;
+                v.src_off = S->dm.bit_off + r->y * S->dm.stride + r->x;
+                v.src_stride = S->dm.stride;
+                v.src_lo_word = S->dm.lo_word;
+                v.src_hi_word = S->dm.hi_word;
             }
-            cl.smem = std::max(cl.smem, strata::batch_smem_bytes(cl.op, cl.radius, b.tw, b.th));
-            cl.count++;
+            v.dst_bits = r->out_bits[k];
+            v.dst_off = 0;
+            v.dst_stride = r->w;
+            v.out_x1 = r->w;
+            v.out_y1 = r->h;
+            v.width = r->w;
+            v.height = r->h;
+            v.radius = r->p.radius;
+            v.dst_words = (r->w * r->h + 31) / 32;
         }
-        classes.push_back(cl);
+        const LaunchParams& p = b.p;
+        b.vec = aligned16_host(p.src) && aligned16_host(p.dst0) && !(p.src_stride & 3) && !(p.dst0_stride & 3) &&
+                (r->nout < 2 || (aligned16_host(p.dst1) && !(p.dst1_stride & 3)));
     }
+    const int nc = strata::batch_plan(s.h_items, n, s.order.data(), s.classes.data(), nullptr);
+    if (nc < 0) return fail(STRATA_ENOTSUP, "engine: an op of the request has no batch kernel");
+    strata::ValidityClass vcls[STRATA_MAX_RADIUS + 1];
+    int nvc = 0;
+    const int nv = strata::batch_plan_validity(s.h_items, n, s.h_vitems, vcls, &nvc);
     cudaError_t e = cudaMemcpyAsync(s.d_items, s.h_items, sizeof(strata::BatchItem) * (size_t)n,
                                     cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && nv > 0)
+        e = cudaMemcpyAsync(s.d_vitems, s.h_vitems, sizeof(strata::ValidityItem) * (size_t)nv, cudaMemcpyHostToDevice,
+                            st);
     if (e != cudaSuccess) return cuda_fail(e, "serve descriptors");
-    for (const Class& cl : classes) {
-        const int per_sm = cl.smem > 48 * 1024 ? 2 : 4;
-        const int64_t grid = std::min<int64_t>(cl.total, (int64_t)S->sms * per_sm);
-        if (!strata::launch_batch_class(cl.op, cl.radius, s.d_items + cl.first, cl.count, cl.total, (int)grid, cl.smem,
-                                        st))
+    for (int i = 0; i < nc; i++)
+        if (!strata::launch_batch_class(s.classes[(size_t)i], s.d_items, st))
             return fail(STRATA_ENOTSUP, "engine: an op of the request has no batch kernel");
-    }
+    for (int i = 0; i < nvc; i++) strata::launch_batch_validity(vcls[i], s.d_vitems, st);
     e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaEventRecord(s.done, st);
     if (e != cudaSuccess) return cuda_fail(e, "serve launch");
@@ -2223,6 +2157,12 @@ extern "C" int strata_server_create(strata_ctx* c, const strata_raster* mosaic, 
         if (e == cudaSuccess) e = cudaMalloc(&s.d_items, sizeof(strata::BatchItem) * (size_t)S->max_batch);
         if (e == cudaSuccess)
             e = cudaHostAlloc(&s.h_items, sizeof(strata::BatchItem) * (size_t)S->max_batch, cudaHostAllocDefault);
+        if (e == cudaSuccess) e = cudaMalloc(&s.d_vitems, sizeof(strata::ValidityItem) * 2 * (size_t)S->max_batch);
+        if (e == cudaSuccess)
+            e = cudaHostAlloc(&s.h_vitems, sizeof(strata::ValidityItem) * 2 * (size_t)S->max_batch,
+                              cudaHostAllocDefault);
+        s.order.resize((size_t)S->max_batch);
+        s.classes.resize((size_t)S->max_batch);
     }
     if (e != cudaSuccess) {
         strata_server_destroy(S);
@@ -2353,6 +2293,8 @@ extern "C" void strata_server_destroy(strata_server* S) {
         if (s.done) cudaEventDestroy(s.done);
         if (s.d_items) cudaFree(s.d_items);
         if (s.h_items) cudaFreeHost(s.h_items);
+        if (s.d_vitems) cudaFree(s.d_vitems);
+        if (s.h_vitems) cudaFreeHost(s.h_vitems);
         if (s.stream) cudaStreamDestroy(s.stream);
     }
     cudaStreamSynchronize(S->ctx->stream);

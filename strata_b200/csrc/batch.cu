@@ -1,182 +1,283 @@
 // batch.cu - many rasters of mixed sizes and ops in one CUDA-graph launch.
 //
-// A batch groups its rasters by op class (op and radius). Each class runs
-// one persistent kernel: its blocks walk the work units of every raster of
-// the class (output tiles, gridDim apart), so a class of many small
-// rasters costs one launch rather than one per raster, and the classes'
-// kernels sit side by side in one captured graph that replays with one
-// launch. Each raster carries its own tile shape (the autotuner's choice
-// for its class) and its own descriptor: the block stages the descriptor
-// of the raster it works on in shared memory, loads the tile with its
-// halo, computes it with the same cell functions as the single-raster
-// kernels (so every cell has the same bits), and writes the tile's
-// validity with word-safe updates.
-#include "cellops.cuh"
-#include "focalops.cuh"
+// A batch groups its rasters by op class (op, radius, and the kind and
+// epilogue where the kernel is specialised on them). Each class runs one
+// persistent kernel whose blocks walk the work units of every raster of
+// the class, gridDim apart, so a class of many small rasters costs one
+// launch rather than one per raster; the classes' kernels sit side by
+// side in one captured graph that replays with one launch. A unit has the
+// shape of the single-raster kernels' blocks, and the block runs the same
+// body on it, so every cell has the same bits:
+//   * radius-1 ops: 512 columns (a warp's march down 128 of them) by a band
+//     of rows (march.cuh);
+//   * separable ops and roughness at radius 2..8: a band of 512 column
+//     results (focal.cuh, in batch_focal.cu);
+//   * correlation and the other ruggedness kinds at radius 2..8: a tile of
+//     128 columns (focal.cuh, in batch_focal.cu).
+// Each raster keeps its own descriptor (the block stages it in shared
+// memory when it reaches the raster's units) and its own band height (the
+// autotuner's choice for its class). The validity of every masked output
+// runs in persistent kernels of its own, one per radius, a warp a unit of
+// 1024 cells by a band of rows (validity.cuh).
+#include <algorithm>
+
+#include "batch.cuh"
 #include "launch.h"
-#include "ops3.cuh"
+#include "march.cuh"
 #include "validity.cuh"
 
 namespace strata {
+
+// Launchers of the classes whose kernels batch_focal.cu holds.
+bool launch_batch_focal(const BatchClass& c, const BatchItem* d_items, cudaStream_t s);
+// Unit width and height of the focal families for radius r (band: the
+// requested rows, 0 for the default).
+void batch_focal_shape(int op, int radius, int kind, int band, int* tw, int* th);
+
 namespace {
 
-constexpr int kBatchThreads = 256;
-
-template <int OP, int R>
-constexpr bool kColPass = OP == STRATA_OP_SEPARABLE || OP == STRATA_OP_MEAN || OP == STRATA_OP_MIN ||
-                          OP == STRATA_OP_MAX || (OP == STRATA_OP_RUGGEDNESS && R > 1);
-
-template <int OP, int R>
-__global__ void __launch_bounds__(kBatchThreads) batch_kernel(const BatchItem* __restrict__ items, int nitems,
-                                                              int64_t total) {
-    extern __shared__ __align__(16) float sm[];
-    __shared__ LaunchParams P;
-    __shared__ ValidityParams V[2];
-    const int tid = threadIdx.x;
+template <int OP, int KIND, bool EPI>
+__global__ void __launch_bounds__(kBatchThreads) batch_march_kernel(const BatchItem* __restrict__ items, int n,
+                                                                    int64_t total) {
+    __shared__ __align__(16) LaunchParams P;
+    EpiTables* T = EpiSmem<EPI>::get();
+    const int warp = threadIdx.x >> 5;
     int cur = -1;
-    int tw = 0, th = 0, nvalid = 0;
-    int64_t tiles_x = 1, tile0 = 0;
     for (int64_t u = blockIdx.x; u < total; u += gridDim.x) {
-        // The raster of unit u: the last whose first unit is at or before u.
-        int lo = 0, hi = nitems - 1;
+        const int it = batch_item_of(items, n, u);
+        if (it != cur) {  // the same for the whole block
+            __syncthreads();
+            batch_stage_params(items[it], P);
+            __syncthreads();
+            if constexpr (EPI) {
+                stage_epilogue(P, *T);
+                __syncthreads();
+            }
+            cur = it;
+        }
+        const BatchUnit b = batch_unit(items[it], P, u);
+        const int64_t xs = b.x + 128 * warp;
+        if (xs < P.out_x1) march_warp<OP, KIND, EPI>(P, T, xs, b.y0, b.rows, b.vec);
+    }
+}
+
+constexpr int kValidityWarps = 8;
+
+template <int R>
+__global__ void __launch_bounds__(32 * kValidityWarps) batch_validity_kernel(const ValidityItem* __restrict__ items,
+                                                                             int n, int64_t total) {
+    const int64_t warps = (int64_t)gridDim.x * kValidityWarps;
+    for (int64_t u = (int64_t)blockIdx.x * kValidityWarps + (threadIdx.x >> 5); u < total; u += warps) {
+        int lo = 0, hi = n - 1;
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
-            if (items[mid].tile0 <= u) lo = mid;
+            if (items[mid].unit0 <= u) lo = mid;
             else hi = mid - 1;
         }
-        if (lo != cur) {
-            __syncthreads();  // the last tile is done with the previous descriptor
-            const int4* s = reinterpret_cast<const int4*>(&items[lo].p);
-            int4* d = reinterpret_cast<int4*>(&P);
-            for (int i = tid; i < (int)(sizeof(LaunchParams) / 16); i += kBatchThreads) d[i] = s[i];
-            const int4* sv = reinterpret_cast<const int4*>(&items[lo].v[0]);
-            int4* dv = reinterpret_cast<int4*>(&V[0]);
-            for (int i = tid; i < (int)(2 * sizeof(ValidityParams) / 16); i += kBatchThreads) dv[i] = sv[i];
-            tw = items[lo].tw;
-            th = items[lo].th;
-            tiles_x = items[lo].tiles_x;
-            tile0 = items[lo].tile0;
-            nvalid = items[lo].nvalid;
-            cur = lo;
-        }
-        __syncthreads();
-        const int64_t t = u - tile0;
-        const int64_t x0 = P.out_x0 + (t % tiles_x) * tw;
-        const int64_t y0 = P.out_y0 + (t / tiles_x) * th;
-        const int64_t x1 = min(x0 + tw, P.out_x1), y1 = min(y0 + th, P.out_y1);
-        const int SW = tw + 2 * R, SH = th + 2 * R;
-        float* tile = sm;
-        for (int i = tid; i < SW * SH; i += kBatchThreads) {
-            const int sy = i / SW, sx = i - sy * SW;
-            const int64_t bx = x0 - R + sx - P.src_x0, by = y0 - R + sy - P.src_y0;
-            float v = 0.0f;
-            if (bx >= 0 && bx < P.src_w && by >= 0 && by < P.src_h) v = P.src[by * P.src_stride + bx];
-            tile[i] = v;
-        }
-        __syncthreads();
-        float* colr = sm + SW * SH;     // column results: th rows of SW
-        float* colr2 = colr + th * SW;  // roughness keeps the minima here
-        if constexpr (kColPass<OP, R>) {
-            for (int i = tid; i < th * SW; i += kBatchThreads) {
-                const int oy = i / SW, sx = i - oy * SW;
-                const float* top = &tile[oy * SW + sx];
-                if constexpr (OP == STRATA_OP_RUGGEDNESS) {
-                    colr[i] = column_fold<STRATA_OP_MAX, R>(P, top, SW);
-                    colr2[i] = column_fold<STRATA_OP_MIN, R>(P, top, SW);
-                } else {
-                    colr[i] = column_fold<OP, R>(P, top, SW);
-                }
-            }
-            __syncthreads();
-        }
-        const int64_t W = P.width, H = P.height;
-        for (int i = tid; i < tw * th; i += kBatchThreads) {
-            const int oy = i / tw, ox = i - oy * tw;
-            const int64_t gx = x0 + ox, gy = y0 + oy;
-            if (gx >= x1 || gy >= y1) continue;
-            const bool interior = gx >= R && gx < W - R && gy >= R && gy < H - R;
-            float o0 = cell::nanf32(), o1 = cell::nanf32();
-            if (interior) {
-                const float* c = &tile[(oy + R) * SW + ox + R];
-                if constexpr (OP == STRATA_OP_RUGGEDNESS && R > 1) {
-                    if (P.kind == STRATA_RUG_ROUGHNESS)
-                        o0 = cell::sub(row_fold<STRATA_OP_MAX, R>(P, &colr[oy * SW + ox]),
-                                       row_fold<STRATA_OP_MIN, R>(P, &colr2[oy * SW + ox]));
-                    else
-                        o0 = rugged_window<R>(c, SW, P.kind);
-                } else if constexpr (kColPass<OP, R>) {
-                    o0 = row_fold<OP, R>(P, &colr[oy * SW + ox]);
-                } else if constexpr (OP == STRATA_OP_CORRELATE && R > 1) {
-                    o0 = correlate<R>(P, c, SW);
-                } else {
-                    const float z[9] = {c[-SW - 1], c[-SW], c[-SW + 1], c[-1], c[0], c[1],
-                                        c[SW - 1], c[SW], c[SW + 1]};
-                    apply3<OP>(P, z, o0, o1);
-                }
-                if (P.nepi) o0 = epilogue(P, o0);
-            }
-            const int64_t dx = gx - P.dst_x0, dy = gy - P.dst_y0;
-            P.dst0[dy * P.dst0_stride + dx] = o0;
-            if constexpr (OP == STRATA_OP_GRADIENT) P.dst1[dy * P.dst1_stride + dx] = o1;
-        }
-        for (int k = 0; k < nvalid; k++) region_validity(V[k], x0, y0, x1, y1, tid, kBatchThreads);
+        const ValidityItem& I = items[lo];
+        const int64_t t = u - I.unit0;
+        const int64_t band = t / I.strips, strip = t - band * I.strips;
+        const int64_t y0 = I.v.out_y0 + band * I.band;
+        const int64_t r = I.v.out_y1 - y0;
+        validity_strip<R>(I.v, I.v.out_x0 + strip * kStripCells, y0, r < I.band ? (int)r : I.band);
     }
 }
 
-template <int OP, int R>
-void launch_class(const BatchItem* items, int nitems, int64_t total, int grid, size_t smem, cudaStream_t s) {
-    if (smem > 48 * 1024)
-        cudaFuncSetAttribute(batch_kernel<OP, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    batch_kernel<OP, R><<<grid, kBatchThreads, smem, s>>>(items, nitems, total);
+// Blocks that fill the GPU once at the kernel's occupancy (per_sm, looked
+// up once per kernel by its launcher), never more than the units.
+int persistent_grid(int per_sm, int64_t total) {
+    static int sms[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) dev = 0;
+    if (!sms[dev]) {
+        int n = 148;
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        sms[dev] = n;
+    }
+    const int64_t g = (int64_t)sms[dev] * per_sm;
+    return (int)(total < g ? total : g);
 }
 
-using ClassLauncher = void (*)(const BatchItem*, int, int64_t, int, size_t, cudaStream_t);
+template <class K>
+int occupancy(K kernel, int threads) {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, 0) != cudaSuccess || n < 1) n = 1;
+    return n;
+}
 
-template <int OP>
-ClassLauncher pick(int r) {
-    switch (r) {
-    case 1: return launch_class<OP, 1>;
-    case 2: return launch_class<OP, 2>;
-    case 3: return launch_class<OP, 3>;
-    case 4: return launch_class<OP, 4>;
-    case 5: return launch_class<OP, 5>;
-    case 6: return launch_class<OP, 6>;
-    case 7: return launch_class<OP, 7>;
-    case 8: return launch_class<OP, 8>;
+template <int OP, int KIND, bool EPI>
+bool launch_march_class(const BatchClass& c, const BatchItem* d, cudaStream_t s) {
+    static const int per_sm = occupancy(batch_march_kernel<OP, KIND, EPI>, kBatchThreads);
+    batch_march_kernel<OP, KIND, EPI><<<persistent_grid(per_sm, c.total), kBatchThreads, 0, s>>>(
+        d + c.first, c.count, c.total);
+    return true;
+}
+
+template <int OP, int KIND>
+bool launch_march_epi(const BatchClass& c, const BatchItem* d, cudaStream_t s) {
+    return c.epi ? launch_march_class<OP, KIND, true>(c, d, s) : launch_march_class<OP, KIND, false>(c, d, s);
+}
+
+template <int R>
+void launch_validity_class(const ValidityClass& c, const ValidityItem* d, cudaStream_t s) {
+    static const int per_sm = occupancy(batch_validity_kernel<R>, 32 * kValidityWarps);
+    batch_validity_kernel<R><<<persistent_grid(per_sm, (c.total + kValidityWarps - 1) / kValidityWarps),
+                               32 * kValidityWarps, 0, s>>>(d + c.first, c.count, c.total);
+}
+
+// The class of an item: its family (0 march, 1 separable, 2 windowed),
+// and the kind and epilogue flag its kernel is specialised on.
+struct Key {
+    int family, op, radius, kind, epi;
+    bool operator<(const Key& o) const {
+        if (family != o.family) return family < o.family;
+        if (op != o.op) return op < o.op;
+        if (radius != o.radius) return radius < o.radius;
+        if (kind != o.kind) return kind < o.kind;
+        return epi < o.epi;
     }
-    return nullptr;
+    bool operator==(const Key& o) const {
+        return family == o.family && op == o.op && radius == o.radius && kind == o.kind && epi == o.epi;
+    }
+};
+
+Key key_of(const LaunchParams& p) {
+    Key k{0, p.op, p.radius, 0, 0};
+    if (p.radius <= 1) {
+        k.radius = 1;
+        if (p.op == STRATA_OP_SLOPE || p.op == STRATA_OP_ASPECT) k.kind = p.kind ? 1 : 0;
+        k.epi = p.nepi > 0;
+    } else if (p.op == STRATA_OP_CORRELATE || (p.op == STRATA_OP_RUGGEDNESS && p.kind != STRATA_RUG_ROUGHNESS)) {
+        k.family = 2;
+        k.kind = p.op == STRATA_OP_RUGGEDNESS ? p.kind : 0;
+    } else {
+        k.family = 1;
+        k.kind = p.op == STRATA_OP_RUGGEDNESS ? p.kind : 0;
+    }
+    return k;
 }
 
 }  // namespace
 
-size_t batch_smem_bytes(int op, int radius, int tw, int th) {
-    const int SW = tw + 2 * radius, SH = th + 2 * radius;
-    int floats = SW * SH;
-    const bool colpass = op == STRATA_OP_SEPARABLE || op == STRATA_OP_MEAN || op == STRATA_OP_MIN ||
-                         op == STRATA_OP_MAX || (op == STRATA_OP_RUGGEDNESS && radius > 1);
-    if (colpass) floats += th * SW * (op == STRATA_OP_RUGGEDNESS ? 2 : 1);
-    return (size_t)floats * 4;
+int batch_plan(BatchItem* items, int n, int* order, BatchClass* cls, int64_t* window_cells) {
+    // Each item's unit shape.
+    int64_t window = 0;
+    for (int i = 0; i < n; i++) {
+        BatchItem& b = items[i];
+        const LaunchParams& p = b.p;
+        if (p.radius < 1 && !(p.op >= STRATA_OP_GRADIENT && p.op <= STRATA_OP_CURVATURE)) return -1;
+        const Key k = key_of(p);
+        if (k.family == 0) {
+            b.tw = 512;
+            b.th = b.th > 0 ? b.th : 32;
+        } else {
+            batch_focal_shape(p.op, p.radius, p.kind, b.th, &b.tw, &b.th);
+        }
+        const int64_t w = p.out_x1 - p.out_x0, h = p.out_y1 - p.out_y0;
+        b.tiles_x = (w + b.tw - 1) / b.tw;
+        const int r = k.radius;
+        window += b.tiles_x * ((h + b.th - 1) / b.th) * (int64_t)(b.tw + 2 * r) * (b.th + 2 * r);
+    }
+    if (window_cells) *window_cells = window;
+    // Stable insertion sort of the indices by class, then the items
+    // permuted into that order in place, cycle by cycle.
+    for (int i = 0; i < n; i++) {
+        const Key ki = key_of(items[i].p);
+        int j = i;
+        for (; j > 0 && ki < key_of(items[order[j - 1]].p); j--) order[j] = order[j - 1];
+        order[j] = i;
+    }
+    for (int i = 0; i < n; i++) {
+        if (order[i] < 0) continue;
+        BatchItem t = items[i];
+        int j = i;
+        while (order[j] != i) {
+            const int k = order[j];
+            items[j] = items[k];
+            order[j] = -1;
+            j = k;
+        }
+        items[j] = t;
+        order[j] = -1;
+    }
+    int nc = 0;
+    for (int i = 0; i < n;) {
+        const Key k = key_of(items[i].p);
+        BatchClass& c = cls[nc++];
+        c.op = k.op;
+        c.radius = k.radius;
+        c.kind = k.kind;
+        c.epi = k.epi;
+        c.first = i;
+        c.count = 0;
+        c.total = 0;
+        for (; i < n && key_of(items[i].p) == k; i++) {
+            BatchItem& b = items[i];
+            b.tile0 = c.total;
+            c.total += b.tiles_x * ((b.p.out_y1 - b.p.out_y0 + b.th - 1) / b.th);
+            c.count++;
+        }
+    }
+    return nc;
 }
 
-bool launch_batch_class(int op, int radius, const BatchItem* items, int nitems, int64_t total, int grid,
-                        size_t smem, cudaStream_t s) {
-    ClassLauncher L = nullptr;
-    switch (op) {
-    case STRATA_OP_GRADIENT: L = launch_class<STRATA_OP_GRADIENT, 1>; break;
-    case STRATA_OP_SLOPE: L = launch_class<STRATA_OP_SLOPE, 1>; break;
-    case STRATA_OP_ASPECT: L = launch_class<STRATA_OP_ASPECT, 1>; break;
-    case STRATA_OP_HILLSHADE: L = launch_class<STRATA_OP_HILLSHADE, 1>; break;
-    case STRATA_OP_CURVATURE: L = launch_class<STRATA_OP_CURVATURE, 1>; break;
-    case STRATA_OP_RUGGEDNESS: L = pick<STRATA_OP_RUGGEDNESS>(radius); break;
-    case STRATA_OP_CORRELATE: L = pick<STRATA_OP_CORRELATE>(radius); break;
-    case STRATA_OP_SEPARABLE: L = pick<STRATA_OP_SEPARABLE>(radius); break;
-    case STRATA_OP_MEAN: L = pick<STRATA_OP_MEAN>(radius); break;
-    case STRATA_OP_MIN: L = pick<STRATA_OP_MIN>(radius); break;
-    case STRATA_OP_MAX: L = pick<STRATA_OP_MAX>(radius); break;
+int batch_plan_validity(const BatchItem* items, int n, ValidityItem* vitems, ValidityClass* vcls, int* nvcls) {
+    constexpr int kBand = 32;
+    int nv = 0, nc = 0;
+    for (int r = 0; r <= STRATA_MAX_RADIUS; r++) {
+        ValidityClass c{r, nv, 0, 0};
+        for (int i = 0; i < n; i++)
+            for (int k = 0; k < items[i].nvalid; k++) {
+                const ValidityParams& v = items[i].v[k];
+                if (v.radius != r || v.dst_words <= 0 || v.out_x1 <= v.out_x0 || v.out_y1 <= v.out_y0) continue;
+                ValidityItem& it = vitems[nv++];
+                memset(&it, 0, sizeof it);
+                it.v = v;
+                it.band = kBand;
+                it.strips = (v.out_x1 - v.out_x0 + kStripCells - 1) / kStripCells;
+                it.unit0 = c.total;
+                c.total += it.strips * ((v.out_y1 - v.out_y0 + kBand - 1) / kBand);
+                c.count++;
+            }
+        if (c.count) vcls[nc++] = c;
     }
-    if (!L) return false;
-    L(items, nitems, total, grid, smem, s);
-    return true;
+    *nvcls = nc;
+    return nv;
+}
+
+bool launch_batch_class(const BatchClass& c, const BatchItem* d, cudaStream_t s) {
+    if (c.radius > 1 || c.op == STRATA_OP_LOOKUP || c.op == STRATA_OP_RECLASS) return launch_batch_focal(c, d, s);
+    switch (c.op) {
+    case STRATA_OP_GRADIENT: return launch_march_class<STRATA_OP_GRADIENT, 0, false>(c, d, s);
+    case STRATA_OP_SLOPE:
+        return c.kind ? launch_march_epi<STRATA_OP_SLOPE, 1>(c, d, s) : launch_march_epi<STRATA_OP_SLOPE, 0>(c, d, s);
+    case STRATA_OP_ASPECT:
+        return c.kind ? launch_march_epi<STRATA_OP_ASPECT, 1>(c, d, s) : launch_march_epi<STRATA_OP_ASPECT, 0>(c, d, s);
+    case STRATA_OP_HILLSHADE: return launch_march_epi<STRATA_OP_HILLSHADE, 0>(c, d, s);
+    case STRATA_OP_CURVATURE: return launch_march_epi<STRATA_OP_CURVATURE, 0>(c, d, s);
+    case STRATA_OP_RUGGEDNESS: return launch_march_epi<STRATA_OP_RUGGEDNESS, 0>(c, d, s);
+    case STRATA_OP_CORRELATE: return launch_march_epi<STRATA_OP_CORRELATE, 0>(c, d, s);
+    case STRATA_OP_SEPARABLE: return launch_march_epi<STRATA_OP_SEPARABLE, 0>(c, d, s);
+    case STRATA_OP_MEAN: return launch_march_epi<STRATA_OP_MEAN, 0>(c, d, s);
+    case STRATA_OP_MIN: return launch_march_epi<STRATA_OP_MIN, 0>(c, d, s);
+    case STRATA_OP_MAX: return launch_march_epi<STRATA_OP_MAX, 0>(c, d, s);
+    }
+    return false;
+}
+
+void launch_batch_validity(const ValidityClass& c, const ValidityItem* d, cudaStream_t s) {
+    switch (c.radius) {
+    case 0: launch_validity_class<0>(c, d, s); break;
+    case 1: launch_validity_class<1>(c, d, s); break;
+    case 2: launch_validity_class<2>(c, d, s); break;
+    case 3: launch_validity_class<3>(c, d, s); break;
+    case 4: launch_validity_class<4>(c, d, s); break;
+    case 5: launch_validity_class<5>(c, d, s); break;
+    case 6: launch_validity_class<6>(c, d, s); break;
+    case 7: launch_validity_class<7>(c, d, s); break;
+    case 8: launch_validity_class<8>(c, d, s); break;
+    }
 }
 
 }  // namespace strata

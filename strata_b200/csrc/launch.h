@@ -78,25 +78,58 @@ struct alignas(16) ValidityParams {
 };
 
 // One raster of a batch (batch.cu): its launch parameters, the validity
-// of its masked outputs, and where its work units (tiles of tw x th
-// output cells, tiles_x across) start among its class's.
+// of its masked outputs, and its work units: tiles of tw x th output cells,
+// tiles_x across, numbered from tile0 among its class's.
 struct alignas(16) BatchItem {
     LaunchParams p;
     ValidityParams v[2];
     int64_t tile0;
     int64_t tiles_x;
-    int tw, th;
+    int tw, th;  // th: the requested band (rows a unit) before planning, 0 for the default
     int nvalid;  // masked outputs: v[0 .. nvalid)
+    int vec;     // 1: the rows of src and dst start on 16-byte boundaries where units load and store
+};
+
+// One masked output of a batch raster: its units are warp strips of 1024
+// cells across and band rows, numbered from unit0 among its class's.
+struct alignas(16) ValidityItem {
+    ValidityParams v;
+    int64_t unit0;
+    int64_t strips;
+    int band;
     int pad;
 };
 
-// Shared memory a batch kernel block needs for a tw x th tile of this op.
-size_t batch_smem_bytes(int op, int radius, int tw, int th);
-// Launches the persistent kernel of one op class over items[0 .. nitems)
-// (device memory), total work units, on grid blocks. False if the op has
-// no batch kernel.
-bool launch_batch_class(int op, int radius, const BatchItem* items, int nitems, int64_t total, int grid, size_t smem,
-                        cudaStream_t stream);
+// A class of batch rasters, run by one persistent kernel: the items
+// [first, first + count) of the planned table, total work units.
+struct BatchClass {
+    int op, radius, kind, epi;  // the kernel's specialisation
+    int first, count;
+    int64_t total;
+};
+
+// A class of batch validity items (one radius).
+struct ValidityClass {
+    int radius;
+    int first, count;
+    int64_t total;
+};
+
+// Plans a batch in place (host): orders items[0 .. n) into classes (stable
+// within a class), sets each item's unit geometry (tw, tiles_x, th from
+// the requested band) and numbering, and writes the classes to cls
+// (capacity n). order: n ints of scratch. Returns the number of classes,
+// or -1 if an item has no batch kernel. *window_cells (if given) gets the
+// input cells the units read.
+int batch_plan(BatchItem* items, int n, int* order, BatchClass* cls, int64_t* window_cells);
+// The validity items of planned items (at most 2n, into vitems) grouped by
+// radius into vcls (capacity 9); returns the number of validity items and
+// sets *nvcls.
+int batch_plan_validity(const BatchItem* items, int n, ValidityItem* vitems, ValidityClass* vcls, int* nvcls);
+// Launches a class's persistent kernel over its items (device memory) on
+// stream; false if the class has no kernel.
+bool launch_batch_class(const BatchClass& c, const BatchItem* d_items, cudaStream_t stream);
+void launch_batch_validity(const ValidityClass& c, const ValidityItem* d_vitems, cudaStream_t stream);
 
 // Launches the data kernel of stages (the first any op, the rest pointwise
 // epilogues) over whole rasters. Returns the number of thread-block tiles

@@ -34,88 +34,13 @@
 #include <cuda.h>
 
 #include "launch.h"
+#include "march.cuh"
 #include "ops3.cuh"
 
 namespace strata {
 namespace {
 
 using namespace cell;
-
-constexpr int kWarps = 4;  // warps per block, side by side: 512 columns
-constexpr unsigned kFull = 0xffffffffu;
-
-struct Row6 {
-    float v[6];  // columns x-1 .. x+4 around the lane's four
-};
-
-// hornDX's horizontal difference of one row for the four cells.
-__device__ __forceinline__ void hdiff(const Row6& r, float (&h)[4]) {
-#pragma unroll
-    for (int i = 0; i < 4; i++) h[i] = sub(r.v[i + 2], r.v[i]);
-}
-
-// The shared-memory copy of the epilogue's tables, for kernels with one.
-template <bool EPI>
-struct EpiSmem {
-    __device__ static EpiTables* get() {
-        __shared__ EpiTables t;
-        return &t;
-    }
-};
-template <>
-struct EpiSmem<false> {
-    __device__ static EpiTables* get() { return nullptr; }
-};
-
-template <int OP>
-constexpr bool kIsHorn = OP == STRATA_OP_GRADIENT || OP == STRATA_OP_SLOPE || OP == STRATA_OP_ASPECT ||
-                         OP == STRATA_OP_HILLSHADE;
-
-// One output row of four cells from the window rows a (top), b, c
-// (bottom) and, for Horn ops, their horizontal differences.
-template <int OP, int KIND, bool EPI>
-__device__ __forceinline__ void row_compute(const LaunchParams& P, const EpiTables* T, const Row6& a, const Row6& b,
-                                            const Row6& c,
-                                            const float (&ha)[4], const float (&hb)[4], const float (&hc)[4],
-                                            bool rowin, const bool (&colin)[4], float (&o0)[4], float (&o1)[4]) {
-    const float nan = nanf32();
-    if constexpr (kIsHorn<OP>) {
-        // hornDY's vertical differences: bottom row minus top row.
-        float v[6];
-#pragma unroll
-        for (int j = 0; j < 6; j++) v[j] = sub(c.v[j], a.v[j]);
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-            const float dx = add(add(ha[i], hc[i]), add(hb[i], hb[i]));
-            const float dy = add(add(v[i], v[i + 2]), add(v[i + 1], v[i + 1]));
-            const float gx = mul(dx, P.k[0]);
-            const float gy = mul(dy, P.k[1]);
-            const bool in = rowin && colin[i];
-            if constexpr (OP == STRATA_OP_GRADIENT) {
-                o0[i] = in ? gx : nan;
-                o1[i] = in ? gy : nan;
-            } else {
-                float r;
-                if constexpr (OP == STRATA_OP_SLOPE) r = slope(gx, gy, P.k[2], KIND != 0);
-                else if constexpr (OP == STRATA_OP_ASPECT) r = aspect(gx, gy, P.k[2], KIND != 0);
-                else r = shade(gx, gy, P.k[2], P.k[3], P.k[4]);
-                o0[i] = in ? r : nan;
-            }
-        }
-        // The epilogue maps NaN to itself, so the edge ring stays NaN.
-        if constexpr (EPI && OP != STRATA_OP_GRADIENT) epilogue4(P, *T, o0);
-    } else {
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-            const float z[9] = {a.v[i], a.v[i + 1], a.v[i + 2], b.v[i], b.v[i + 1],
-                                b.v[i + 2], c.v[i], c.v[i + 1], c.v[i + 2]};
-            float r0 = nan, r1 = nan;
-            apply3<OP>(P, z, r0, r1);
-            o0[i] = (rowin && colin[i]) ? r0 : nan;
-        }
-        if constexpr (EPI) epilogue4(P, *T, o0);
-    }
-}
 
 // What every marching kernel works out first: the warp's columns, rows and
 // interior tests, and where its outputs go.
