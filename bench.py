@@ -545,8 +545,6 @@ def run_serve(args, rank, world, local_rank):
     """Serving: window requests over a resident mosaic, batched as they
     arrive (continuous batching), against the same requests run one at a
     time through engine.process."""
-    import threading
-
     import torch
 
     from strata_b200 import engine, focal, serve, terrain
@@ -596,40 +594,29 @@ def run_serve(args, rank, world, local_rank):
     mean_cells = float(np.mean([w * h for _o, _x, _y, w, h in reqs]))
     rate = 0.6 * capacity / mean_cells  # requests per second
     gaps = np.random.default_rng(seed + 1).exponential(1.0 / rate, len(reqs))
-    lat, tickets, lock = [], [], threading.Lock()
-
-    def submitter():
-        t = time.perf_counter()
-        for (o, x, y, w, h), g in zip(reqs, gaps):
-            t += g
-            left = t - time.perf_counter()
-            if left > 3e-4:
-                time.sleep(left - 2e-4)
-            while time.perf_counter() < t:
-                pass
-            tk = srv.submit(ops[o][1], x, y, w, h)
-            with lock:
-                tickets.append(tk)
-
-    switch = sys.getswitchinterval()
-    sys.setswitchinterval(1e-4)  # arrivals on time while the other thread waits
-    th = threading.Thread(target=submitter)
+    due = np.cumsum(gaps)
+    # One thread submits each request at its arrival time and, in between,
+    # polls the oldest outstanding one; the latencies are the server's own
+    # submit-to-done times, so polling late does not lengthen them.
+    lat, pending = [], []
+    nxt = 0
     t0 = time.perf_counter()
-    th.start()
-    done = 0
-    while done < len(reqs):
-        with lock:
-            tk = tickets[done] if done < len(tickets) else None
-        if tk is None:
-            time.sleep(1e-4)
+    while nxt < len(reqs) or pending:
+        now = time.perf_counter() - t0
+        if nxt < len(reqs) and now >= due[nxt]:
+            o, x, y, w, h = reqs[nxt]
+            pending.append(srv.submit(ops[o][1], x, y, w, h))
+            nxt += 1
             continue
-        r = srv.wait(tk)
-        lat.append(r.latency_ms)
-        srv.release(tk)
-        done += 1
-    th.join()
+        if pending:
+            r = srv.poll(pending[0])
+            if r is not None:
+                lat.append(r.latency_ms)
+                srv.release(pending.pop(0))
+                continue
+        if nxt < len(reqs) and due[nxt] - now > 5e-4:
+            time.sleep(2e-4)
     open_s = time.perf_counter() - t0
-    sys.setswitchinterval(switch)
     st = srv.stats()
     srv.close()
 

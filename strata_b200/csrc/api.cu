@@ -2052,6 +2052,8 @@ int launch_batch(strata_server* S, Slot& s) {
     return STRATA_OK;
 }
 
+constexpr int64_t kCoalesceNs = 100000;  // how long a short queue waits for company while a batch runs
+
 void scheduler(strata_server* S) {
     cudaSetDevice(S->ctx->device);
     std::unique_lock<std::mutex> lk(S->mu);
@@ -2074,8 +2076,15 @@ void scheduler(strata_server* S) {
             S->done_cv.notify_all();
         }
         // Admit queued requests onto a free stream, in arrival order, while
-        // their outputs fit the budget.
+        // their outputs fit the budget. While another batch runs, a short
+        // queue waits up to kCoalesceNs for more requests to join it, so
+        // that batches grow with the load; an idle server launches at once.
+        bool running = false;
+        for (Slot& s : S->slots) running = running || s.busy;
+        const bool hold = running && !S->queue.empty() && (int)S->queue.size() < S->max_batch / 4 &&
+                          now_ns() - S->queue.front()->t_submit < kCoalesceNs;
         for (Slot& s : S->slots) {
+            if (hold) break;
             if (s.busy || S->queue.empty()) continue;
             while (!S->queue.empty() && (int)s.reqs.size() < S->max_batch) {
                 Request* r = S->queue.front();

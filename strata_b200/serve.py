@@ -82,6 +82,17 @@ class Server:
             outs.append(Float32Raster(o.data, o.width, o.height, o.stride, o.valid if o.valid else None, 0))
         return Result(outs, r.t_submit_ns, r.t_start_ns, r.t_done_ns)
 
+    def poll(self, ticket: int) -> Optional[Result]:
+        """The request's result if it is done, else None (no waiting)."""
+        r = _lib.ServerResult()
+        rc = _lib.lib().strata_server_wait(self._h, ticket, 0, ctypes.byref(r))
+        if rc == _lib.ETIMEDOUT:
+            return None
+        _lib.check(rc)
+        outs = [Float32Raster(r.out[k].data, r.out[k].width, r.out[k].height, r.out[k].stride,
+                              r.out[k].valid if r.out[k].valid else None, 0) for k in range(r.nout)]
+        return Result(outs, r.t_submit_ns, r.t_start_ns, r.t_done_ns)
+
     def release(self, ticket: int) -> None:
         _lib.check(_lib.lib().strata_server_release(self._h, ticket))
 
