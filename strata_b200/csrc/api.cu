@@ -103,8 +103,10 @@ struct strata_ctx {
         size_t n = 0;
     };
     std::vector<Buf> bufs;
-    // Page-locked staging for mask merges.
-    std::vector<uint64_t> host_words;
+    // Page-locked staging of the first and last mask words of host
+    // destinations (two a destination), merged into the caller's words.
+    uint64_t* h_edges = nullptr;
+    size_t n_edges = 0;
     // A device word kernels set when a bounded wait runs out, and its
     // page-locked host copy.
     int* d_status = nullptr;
@@ -171,6 +173,7 @@ extern "C" void strata_ctx_destroy(strata_ctx* c) {
         if (b.p) cudaFree(b.p);
     if (c->d_status) cudaFree(c->d_status);
     if (c->h_status) cudaFreeHost(c->h_status);
+    if (c->h_edges) cudaFreeHost(c->h_edges);
     if (c->stream) cudaStreamDestroy(c->stream);
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     delete c;
@@ -657,6 +660,57 @@ void mask_words(int64_t off, int64_t cells, int64_t* w0, int64_t* n) {
     *n = ((off + cells + 63) >> 6) - *w0;
 }
 
+// Page-locked room for the edge words of n destinations.
+int ensure_edges(strata_ctx* c, size_t n) {
+    if (c->n_edges >= 2 * n) return STRATA_OK;
+    if (c->h_edges) cudaFreeHost(c->h_edges);
+    c->h_edges = nullptr;
+    c->n_edges = 0;
+    const size_t want = std::max<size_t>(2 * n, 64);
+    cudaError_t e = cudaHostAlloc(&c->h_edges, want * 8, cudaHostAllocDefault);
+    if (e != cudaSuccess) return cuda_fail(e, "mask staging");
+    c->n_edges = want;
+    return STRATA_OK;
+}
+
+// Starts the copy of a host destination's mask back on stream s: the words
+// wholly inside the raster's bit span straight into the caller's words,
+// the first and last (which other rasters may share) into edge[0..1] for
+// merge_edges once the stream is done.
+cudaError_t mask_back(const strata_raster& r, const DevOperand& d, uint64_t* edge, cudaStream_t s) {
+    const int64_t n = d.nwords64;
+    const uint64_t* dev = reinterpret_cast<const uint64_t*>(d.bits);
+    cudaError_t e = cudaSuccess;
+    if (n > 2) e = cudaMemcpyAsync(r.valid + d.host_w0 + 1, dev + 1, (size_t)(n - 2) * 8, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(edge, dev, 8, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && n > 1) e = cudaMemcpyAsync(edge + 1, dev + n - 1, 8, cudaMemcpyDeviceToHost, s);
+    return e;
+}
+
+// Merges the edge words mask_back fetched: only the raster's own bits of
+// them change.
+void merge_edges(const strata_raster& r, const DevOperand& d, const uint64_t* edge) {
+    const int64_t lo = r.valid_offset, hi = r.valid_offset + span_cells(r);
+    auto merge = [&](int64_t k, uint64_t v) {
+        const int64_t w = d.host_w0 + k;
+        uint64_t own = ~0ull;
+        if (w * 64 < lo) own &= ~0ull << (lo - w * 64);
+        if ((w + 1) * 64 > hi) own &= (hi - w * 64) >= 64 ? ~0ull : ((1ull << (hi - w * 64)) - 1);
+        r.valid[w] = (r.valid[w] & ~own) | (v & own);
+    };
+    merge(0, edge[0]);
+    if (d.nwords64 > 1) merge(d.nwords64 - 1, edge[1]);
+}
+
+// A destination's cells back to the host: one linear copy when its rows
+// are contiguous, else a 2-D copy that leaves the gap cells alone.
+cudaError_t data_back(const strata_raster& r, const DevOperand& d, cudaStream_t s) {
+    if (r.stride == r.width)
+        return cudaMemcpyAsync(r.data, d.data, (size_t)(r.width * r.height) * 4, cudaMemcpyDeviceToHost, s);
+    return cudaMemcpy2DAsync(r.data, (size_t)r.stride * 4, d.data, (size_t)r.stride * 4, (size_t)r.width * 4,
+                             (size_t)r.height, cudaMemcpyDeviceToHost, s);
+}
+
 int stage_in(strata_ctx* c, cudaStream_t st, const strata_raster& r, int slot, bool copy_data, DevOperand* d) {
     d->stride = r.stride;
     int64_t cells = span_cells(r);
@@ -701,23 +755,14 @@ int stage_in(strata_ctx* c, cudaStream_t st, const strata_raster& r, int slot, b
 // bits).
 int stage_out(strata_ctx* c, cudaStream_t st, const strata_raster& r, const DevOperand& d) {
     if (r.on_device) return STRATA_OK;
-    cudaError_t e = cudaMemcpy2DAsync(r.data, (size_t)r.stride * 4, d.data, (size_t)r.stride * 4, (size_t)r.width * 4,
-                                      (size_t)r.height, cudaMemcpyDeviceToHost, st);
+    cudaError_t e = data_back(r, d, st);
     if (e != cudaSuccess) return cuda_fail(e, "copy to host");
     if (r.valid) {
-        c->host_words.resize((size_t)d.nwords64);
-        e = cudaMemcpyAsync(c->host_words.data(), d.bits, (size_t)d.nwords64 * 8, cudaMemcpyDeviceToHost, st);
-        if (e != cudaSuccess) return cuda_fail(e, "copy mask to host");
-        e = cudaStreamSynchronize(st);
-        if (e != cudaSuccess) return cuda_fail(e, "copy mask to host");
-        int64_t lo = r.valid_offset, hi = r.valid_offset + span_cells(r);  // bits of the raster's span
-        for (int64_t k = 0; k < d.nwords64; k++) {
-            int64_t w = d.host_w0 + k;
-            uint64_t own = ~0ull;
-            if (w * 64 < lo) own &= ~0ull << (lo - w * 64);
-            if ((w + 1) * 64 > hi) own &= (hi - w * 64) >= 64 ? ~0ull : ((1ull << (hi - w * 64)) - 1);
-            r.valid[w] = (r.valid[w] & ~own) | (c->host_words[(size_t)k] & own);
-        }
+        int rc;
+        if ((rc = ensure_edges(c, 1))) return rc;
+        if ((e = mask_back(r, d, c->h_edges, st)) != cudaSuccess) return cuda_fail(e, "copy mask to host");
+        if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "copy mask to host");
+        merge_edges(r, d, c->h_edges);
     }
     return STRATA_OK;
 }
@@ -1472,23 +1517,6 @@ extern "C" int strata_process_chunked(strata_ctx* c, const strata_stage* stages,
 // call. A host input crosses to the device once; each output's copy back
 // runs on a second stream while the next pipeline computes.
 
-namespace {
-
-// Mask bits of a host destination merged into the caller's words: the
-// words the raster's span shares with other rasters keep their other bits.
-void merge_mask(const strata_raster& r, const DevOperand& d, const std::vector<uint64_t>& words) {
-    int64_t lo = r.valid_offset, hi = r.valid_offset + span_cells(r);
-    for (int64_t k = 0; k < d.nwords64; k++) {
-        int64_t w = d.host_w0 + k;
-        uint64_t own = ~0ull;
-        if (w * 64 < lo) own &= ~0ull << (lo - w * 64);
-        if ((w + 1) * 64 > hi) own &= (hi - w * 64) >= 64 ? ~0ull : ((1ull << (hi - w * 64)) - 1);
-        r.valid[w] = (r.valid[w] & ~own) | (words[(size_t)k] & own);
-    }
-}
-
-}  // namespace
-
 extern "C" int strata_process_features(strata_ctx* c, const strata_stage* stages, const int32_t* counts,
                                        int nfeatures, const strata_raster* src, const strata_raster* dst,
                                        int ndst, const strata_exec_opts* opts, strata_stats* stats) {
@@ -1525,7 +1553,7 @@ extern "C" int strata_process_features(strata_ctx* c, const strata_stage* stages
     std::vector<DevOperand> dd((size_t)ndst);
     for (int i = 0; i < ndst; i++)
         if ((rc = stage_in(c, st, dst[i], 2 + 2 * i, false, &dd[(size_t)i]))) return rc;
-    std::vector<std::vector<uint64_t>> words((size_t)ndst);
+    if ((rc = ensure_edges(c, (size_t)ndst))) return rc;
     std::vector<cudaEvent_t> events;
     auto cleanup = [&] {
         for (auto e : events) cudaEventDestroy(e);
@@ -1587,13 +1615,8 @@ extern "C" int strata_process_features(strata_ctx* c, const strata_stage* stages
         for (int i = o; i < o + nouts[(size_t)f]; i++) {
             if (dst[i].on_device) continue;
             const DevOperand& d = dd[(size_t)i];
-            e = cudaMemcpy2DAsync(dst[i].data, (size_t)dst[i].stride * 4, d.data, (size_t)dst[i].stride * 4,
-                                  (size_t)W * 4, (size_t)H, cudaMemcpyDeviceToHost, cs);
-            if (e == cudaSuccess && dst[i].valid) {
-                words[(size_t)i].resize((size_t)d.nwords64);
-                e = cudaMemcpyAsync(words[(size_t)i].data(), d.bits, (size_t)d.nwords64 * 8,
-                                    cudaMemcpyDeviceToHost, cs);
-            }
+            e = data_back(dst[i], d, cs);
+            if (e == cudaSuccess && dst[i].valid) e = mask_back(dst[i], d, c->h_edges + 2 * i, cs);
             if (e != cudaSuccess) {
                 cleanup();
                 return cuda_fail(e, "copy to host");
@@ -1608,7 +1631,7 @@ extern "C" int strata_process_features(strata_ctx* c, const strata_stage* stages
     if (!(all_device && opts && (opts->flags & STRATA_EXEC_ASYNC)))
         if ((rc = take_status(c, st))) return rc;
     for (int i = 0; i < ndst; i++)
-        if (!dst[i].on_device && dst[i].valid) merge_mask(dst[i], dd[(size_t)i], words[(size_t)i]);
+        if (!dst[i].on_device && dst[i].valid) merge_edges(dst[i], dd[(size_t)i], c->h_edges + 2 * i);
     if (stats) {
         const int64_t cells = W * H;
         stats->cells += cells;
