@@ -166,17 +166,17 @@ template <int R>
 constexpr int kSepOut = kSepCols - 2 * kHalo<R>;  // output columns per block
 
 // The fold of one column (FOLD is MEAN, MIN, MAX or SEPARABLE), top to
-// bottom over ring slots (u + k) % D; u is a constant once the caller's
-// row loop is unrolled, so the ring stays in registers.
-template <int FOLD, int R>
-__device__ __forceinline__ float col_fold(const LaunchParams& P, const float (&ring)[2 * R + 1][4], int i, int u) {
+// bottom over ring slots (u + k) % RS, k = 0 .. 2R; u is a constant once
+// the caller's row loop is unrolled, so the ring stays in registers.
+template <int FOLD, int R, int RS>
+__device__ __forceinline__ float col_fold(const LaunchParams& P, const float (&ring)[RS][4], int i, int u) {
     constexpr int D = 2 * R + 1;
     float a;
-    if constexpr (FOLD == STRATA_OP_SEPARABLE) a = mul(P.w[17], ring[u % D][i]);
-    else a = ring[u % D][i];
+    if constexpr (FOLD == STRATA_OP_SEPARABLE) a = mul(P.w[17], ring[u % RS][i]);
+    else a = ring[u % RS][i];
 #pragma unroll
     for (int k = 1; k < D; k++) {
-        const float v = ring[(u + k) % D][i];
+        const float v = ring[(u + k) % RS][i];
         if constexpr (FOLD == STRATA_OP_SEPARABLE) a = add(a, mul(P.w[17 + k], v));
         else if constexpr (FOLD == STRATA_OP_MEAN) a = add(a, v);
         else if constexpr (FOLD == STRATA_OP_MIN) a = go_min(a, v);
@@ -184,6 +184,15 @@ __device__ __forceinline__ float col_fold(const LaunchParams& P, const float (&r
     }
     return a;
 }
+
+// Rows the separable march's loop body covers: all 2R+1 (the ring slot of
+// each row a constant, no moves) while that code stays small, else 4 with
+// the ring's last 2R rows moved down after every 4 (the loop body would
+// otherwise outgrow the instruction cache).
+template <int R>
+constexpr int kSepUnroll = R >= 5 ? 4 : 2 * R + 1;
+template <int R>
+constexpr int kSepRing = kSepUnroll<R> == 2 * R + 1 ? 2 * R + 1 : 2 * R + kSepUnroll<R>;
 
 // Term c (0 .. 2R) of a fold across column results, left to right: the
 // first term starts the fold.
@@ -234,7 +243,9 @@ __device__ __forceinline__ void sep_body(const LaunchParams& P, int64_t X0, int6
     StageWalk src(P, X0 - HL + 4 * tid, y0 - R, rows + 2 * R, &stg[0][4 * tid], vec);
 #pragma unroll
     for (int k = 0; k < kStageRows - 1; k++) src.issue();
-    float ring[D][4];
+    constexpr int U = kSepUnroll<R>;
+    constexpr int RS = kSepRing<R>;
+    float ring[RS][4];
     int taken = 0;
 #pragma unroll
     for (int k = 0; k < 2 * R; k++) {
@@ -248,14 +259,14 @@ __device__ __forceinline__ void sep_body(const LaunchParams& P, int64_t X0, int6
     const bool writer = tid < OW / 4 && X0 + 4 * tid < P.out_x1;
     OutWalk dst(P, X0 + 4 * tid, y0, R, vec);
     int buf = 0;
-    for (int yb = 0; yb < rows; yb += D) {
+    for (int yb = 0; yb < rows; yb += U) {
 #pragma unroll
-        for (int u = 0; u < D; u++) {
+        for (int u = 0; u < U; u++) {
             if (yb + u >= rows) break;
             {
                 const float4 v = src.take(taken++);
                 src.issue();
-                float* slot = ring[(u + 2 * R) % D];
+                float* slot = ring[(u + 2 * R) % RS];
                 slot[0] = v.x;
                 slot[1] = v.y;
                 slot[2] = v.z;
@@ -264,8 +275,8 @@ __device__ __forceinline__ void sep_body(const LaunchParams& P, int64_t X0, int6
             float c0[4], c1[4];
 #pragma unroll
             for (int i = 0; i < 4; i++) {
-                c0[i] = col_fold<F0, R>(P, ring, i, u);
-                if constexpr (NF == 2) c1[i] = col_fold<F1, R>(P, ring, i, u);
+                c0[i] = col_fold<F0, R, RS>(P, ring, i, u);
+                if constexpr (NF == 2) c1[i] = col_fold<F1, R, RS>(P, ring, i, u);
             }
             *reinterpret_cast<float4*>(&tb[buf][0][4 * tid]) = make_float4(c0[0], c0[1], c0[2], c0[3]);
             if constexpr (NF == 2)
@@ -303,6 +314,13 @@ __device__ __forceinline__ void sep_body(const LaunchParams& P, int64_t X0, int6
             }
             dst.step();
             buf ^= 1;
+        }
+        if constexpr (RS != D) {
+            // The window's last 2R rows move down to the ring's first slots.
+#pragma unroll
+            for (int k = 0; k < 2 * R; k++)
+#pragma unroll
+                for (int i = 0; i < 4; i++) ring[k][i] = ring[k + U][i];
         }
     }
     cp_async_wait<0>();
