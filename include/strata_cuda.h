@@ -319,6 +319,28 @@ int strata_server_submit(strata_server *srv, const strata_stage *stages, int nst
 /* Waits up to timeout_ms (< 0: without limit) for a request; STRATA_ETIMEDOUT if it is not done by then. */
 int strata_server_wait(strata_server *srv, uint64_t ticket, int64_t timeout_ms, strata_server_result *result);
 int strata_server_release(strata_server *srv, uint64_t ticket);
+
+/*
+ * The same calls for many requests at once, for clients that hold several
+ * requests together (one lock, one scheduler wake-up, one call across a
+ * language boundary instead of one per request). submit_many checks every
+ * request first and queues none if one is invalid; tickets[i] is request
+ * i's ticket, in arrival order. wait_many waits for the tickets in order
+ * (results may be NULL) and returns the first failure; release_many
+ * releases in order and stops at the first failure, the earlier tickets
+ * released.
+ */
+typedef struct {
+    const strata_stage *stages;
+    int32_t nstages;
+    int32_t reserved;
+    int64_t x, y, w, h;
+} strata_server_request;
+
+int strata_server_submit_many(strata_server *srv, const strata_server_request *reqs, int n, uint64_t *tickets);
+int strata_server_wait_many(strata_server *srv, const uint64_t *tickets, int n, int64_t timeout_ms,
+                            strata_server_result *results);
+int strata_server_release_many(strata_server *srv, const uint64_t *tickets, int n);
 int strata_server_stats(strata_server *srv, int64_t *batches, int64_t *served, int64_t *used_bytes);
 void strata_server_destroy(strata_server *srv);
 

@@ -75,6 +75,11 @@ class ServerResult(ctypes.Structure):
                 ("t_start_ns", c_i64), ("t_done_ns", c_i64)]
 
 
+class ServerRequest(ctypes.Structure):
+    _fields_ = [("stages", ctypes.POINTER(Stage)), ("nstages", c_i32), ("reserved", c_i32), ("x", c_i64),
+                ("y", c_i64), ("w", c_i64), ("h", c_i64)]
+
+
 class GradientOptions(ctypes.Structure):
     _fields_ = [("cell_size", c_f64), ("cell_size_y", c_f64), ("z_factor", c_f64),
                 ("fit_radius", c_i32), ("reserved", c_i32)]
@@ -149,6 +154,11 @@ SIGNATURES = [
                                             ctypes.POINTER(ctypes.c_uint64)]),
     ("strata_server_wait", ctypes.c_int, [c_p, ctypes.c_uint64, c_i64, ctypes.POINTER(ServerResult)]),
     ("strata_server_release", ctypes.c_int, [c_p, ctypes.c_uint64]),
+    ("strata_server_submit_many", ctypes.c_int, [c_p, ctypes.POINTER(ServerRequest), ctypes.c_int,
+                                                 ctypes.POINTER(ctypes.c_uint64)]),
+    ("strata_server_wait_many", ctypes.c_int, [c_p, ctypes.POINTER(ctypes.c_uint64), ctypes.c_int, c_i64,
+                                               ctypes.POINTER(ServerResult)]),
+    ("strata_server_release_many", ctypes.c_int, [c_p, ctypes.POINTER(ctypes.c_uint64), ctypes.c_int]),
     ("strata_server_stats", ctypes.c_int, [c_p, ctypes.POINTER(c_i64), ctypes.POINTER(c_i64),
                                            ctypes.POINTER(c_i64)]),
     ("strata_server_destroy", None, [c_p]),

@@ -2205,25 +2205,30 @@ extern "C" int strata_server_create(strata_ctx* c, const strata_raster* mosaic, 
     return STRATA_OK;
 }
 
-extern "C" int strata_server_submit(strata_server* S, const strata_stage* stages, int nstages, int64_t x, int64_t y,
-                                    int64_t w, int64_t h, uint64_t* ticket) {
-    if (!S || !ticket) return fail(STRATA_EINVAL, "engine: nil server");
+namespace {
+
+// A checked, planned request for window (x, y, w, h) of the mosaic, with
+// its own copies of the stages and their tables (the caller's may go
+// away); nullptr and the failure recorded if the request is invalid.
+Request* prepare_request(strata_server* S, const strata_stage* stages, int nstages, int64_t x, int64_t y, int64_t w,
+                         int64_t h, int* rc_out) {
     const strata_raster& M = S->mosaic;
-    if (w <= 0 || h <= 0 || x < 0 || y < 0 || x + w > M.width || y + h > M.height)
-        return fail(STRATA_EINVAL, "raster: window %lld×%lld at (%lld, %lld) outside %lld×%lld raster", (long long)w,
-                    (long long)h, (long long)x, (long long)y, (long long)M.width, (long long)M.height);
+    if (w <= 0 || h <= 0 || x < 0 || y < 0 || x + w > M.width || y + h > M.height) {
+        *rc_out = fail(STRATA_EINVAL, "raster: window %lld×%lld at (%lld, %lld) outside %lld×%lld raster",
+                       (long long)w, (long long)h, (long long)x, (long long)y, (long long)M.width,
+                       (long long)M.height);
+        return nullptr;
+    }
     auto* r = new Request;
     r->x = x;
     r->y = y;
     r->w = w;
     r->h = h;
-    // Keep the stages and their tables: the caller's may go away.
     r->stages.assign(stages, stages + (nstages > 0 ? nstages : 0));
     for (auto& st : r->stages)
         for (int k = 0; k < 4; k++)
             if (st.table[k] && st.table_len[k] > 0) {
-                int n = st.table_len[k] + (st.op == STRATA_OP_RECLASS && k == 1 ? 0 : 0);
-                r->tables.emplace_back(st.table[k], st.table[k] + n);
+                r->tables.emplace_back(st.table[k], st.table[k] + st.table_len[k]);
                 st.table[k] = r->tables.back().data();
             }
     int rc = plan_stages(r->stages.data(), (int)r->stages.size(), r->p, &r->nout);
@@ -2231,7 +2236,8 @@ extern "C" int strata_server_submit(strata_server* S, const strata_stage* stages
         rc = fail(STRATA_ENOTSUP, "engine: a pointwise op alone has no batch kernel");
     if (rc) {
         delete r;
-        return rc;
+        *rc_out = rc;
+        return nullptr;
     }
     LaunchParams& p = r->p;
     p.src = S->dm.data + y * S->dm.stride + x;
@@ -2244,19 +2250,38 @@ extern "C" int strata_server_submit(strata_server* S, const strata_stage* stages
     p.out_y1 = h;
     p.status = S->ctx->d_status;
     r->bytes = (size_t)(w * h) * 4 * (size_t)r->nout + (M.valid ? (size_t)((w * h + 63) / 64) * 8 * r->nout : 0);
-    std::lock_guard<std::mutex> lk(S->mu);
+    *rc_out = STRATA_OK;
+    return r;
+}
+
+// Queues a prepared request (server lock held) and returns its ticket.
+uint64_t enqueue(strata_server* S, Request* r) {
     r->ticket = S->next_ticket++;
     r->t_submit = now_ns();
     S->all[r->ticket] = r;
     S->queue.push_back(r);
-    *ticket = r->ticket;
-    S->cv.notify_one();
+    return r->ticket;
+}
+
+// Frees a finished request's outputs and its budget (server lock held).
+int release_locked(strata_server* S, uint64_t ticket) {
+    auto it = S->all.find(ticket);
+    if (it == S->all.end()) return fail(STRATA_EINVAL, "engine: unknown ticket %llu", (unsigned long long)ticket);
+    Request* r = it->second;
+    if (r->status > 0) return fail(STRATA_EINVAL, "engine: request %llu is still running", (unsigned long long)ticket);
+    for (int k = 0; k < 2; k++) {
+        if (r->out[k]) cudaFreeAsync(r->out[k], S->ctx->stream);
+        if (r->out_bits[k]) cudaFreeAsync(r->out_bits[k], S->ctx->stream);
+    }
+    if (r->t_start) S->used -= r->bytes;
+    S->all.erase(it);
+    delete r;
     return STRATA_OK;
 }
 
-extern "C" int strata_server_wait(strata_server* S, uint64_t ticket, int64_t timeout_ms, strata_server_result* res) {
-    if (!S) return fail(STRATA_EINVAL, "engine: nil server");
-    std::unique_lock<std::mutex> lk(S->mu);
+// Waits for a request (server lock held by lk) and describes its result.
+int wait_locked(strata_server* S, std::unique_lock<std::mutex>& lk, uint64_t ticket, int64_t timeout_ms,
+                strata_server_result* res) {
     auto it = S->all.find(ticket);
     if (it == S->all.end()) return fail(STRATA_EINVAL, "engine: unknown ticket %llu", (unsigned long long)ticket);
     Request* r = it->second;
@@ -2283,23 +2308,74 @@ extern "C" int strata_server_wait(strata_server* S, uint64_t ticket, int64_t tim
     return r->status < 0 ? fail(r->status, "engine: request %llu failed", (unsigned long long)ticket) : STRATA_OK;
 }
 
+}  // namespace
+
+extern "C" int strata_server_submit(strata_server* S, const strata_stage* stages, int nstages, int64_t x, int64_t y,
+                                    int64_t w, int64_t h, uint64_t* ticket) {
+    if (!S || !ticket) return fail(STRATA_EINVAL, "engine: nil server");
+    int rc;
+    Request* r = prepare_request(S, stages, nstages, x, y, w, h, &rc);
+    if (!r) return rc;
+    std::lock_guard<std::mutex> lk(S->mu);
+    *ticket = enqueue(S, r);
+    S->cv.notify_one();
+    return STRATA_OK;
+}
+
+extern "C" int strata_server_submit_many(strata_server* S, const strata_server_request* reqs, int n,
+                                         uint64_t* tickets) {
+    if (!S || (n > 0 && (!reqs || !tickets))) return fail(STRATA_EINVAL, "engine: nil server");
+    if (n < 0) return fail(STRATA_EINVAL, "engine: %d requests", n);
+    std::vector<Request*> prepared((size_t)n);
+    for (int i = 0; i < n; i++) {
+        int rc;
+        const strata_server_request& q = reqs[i];
+        prepared[(size_t)i] = prepare_request(S, q.stages, q.nstages, q.x, q.y, q.w, q.h, &rc);
+        if (!prepared[(size_t)i]) {
+            for (int j = 0; j < i; j++) delete prepared[(size_t)j];
+            return rc;
+        }
+    }
+    std::lock_guard<std::mutex> lk(S->mu);
+    for (int i = 0; i < n; i++) tickets[i] = enqueue(S, prepared[(size_t)i]);
+    S->cv.notify_one();
+    return STRATA_OK;
+}
+
+extern "C" int strata_server_wait(strata_server* S, uint64_t ticket, int64_t timeout_ms, strata_server_result* res) {
+    if (!S) return fail(STRATA_EINVAL, "engine: nil server");
+    std::unique_lock<std::mutex> lk(S->mu);
+    return wait_locked(S, lk, ticket, timeout_ms, res);
+}
+
+extern "C" int strata_server_wait_many(strata_server* S, const uint64_t* tickets, int n, int64_t timeout_ms,
+                                       strata_server_result* results) {
+    if (!S || (n > 0 && !tickets)) return fail(STRATA_EINVAL, "engine: nil server");
+    std::unique_lock<std::mutex> lk(S->mu);
+    for (int i = 0; i < n; i++) {
+        const int rc = wait_locked(S, lk, tickets[i], timeout_ms, results ? results + i : nullptr);
+        if (rc) return rc;
+    }
+    return STRATA_OK;
+}
+
 extern "C" int strata_server_release(strata_server* S, uint64_t ticket) {
     if (!S) return fail(STRATA_EINVAL, "engine: nil server");
     std::lock_guard<std::mutex> lk(S->mu);
-    auto it = S->all.find(ticket);
-    if (it == S->all.end()) return fail(STRATA_EINVAL, "engine: unknown ticket %llu", (unsigned long long)ticket);
-    Request* r = it->second;
-    if (r->status > 0) return fail(STRATA_EINVAL, "engine: request %llu is still running", (unsigned long long)ticket);
     cudaSetDevice(S->ctx->device);
-    for (int k = 0; k < 2; k++) {
-        if (r->out[k]) cudaFreeAsync(r->out[k], S->ctx->stream);
-        if (r->out_bits[k]) cudaFreeAsync(r->out_bits[k], S->ctx->stream);
-    }
-    if (r->t_start) S->used -= r->bytes;
-    S->all.erase(it);
-    delete r;
+    const int rc = release_locked(S, ticket);
     S->cv.notify_one();
-    return STRATA_OK;
+    return rc;
+}
+
+extern "C" int strata_server_release_many(strata_server* S, const uint64_t* tickets, int n) {
+    if (!S || (n > 0 && !tickets)) return fail(STRATA_EINVAL, "engine: nil server");
+    std::lock_guard<std::mutex> lk(S->mu);
+    cudaSetDevice(S->ctx->device);
+    int rc = STRATA_OK;
+    for (int i = 0; i < n && rc == STRATA_OK; i++) rc = release_locked(S, tickets[i]);
+    S->cv.notify_one();
+    return rc;
 }
 
 extern "C" int strata_server_stats(strata_server* S, int64_t* batches, int64_t* served, int64_t* used_bytes) {

@@ -18,7 +18,7 @@ from __future__ import annotations
 
 import ctypes
 from dataclasses import dataclass
-from typing import List, Optional
+from typing import List, Optional, Sequence
 
 
 
@@ -72,6 +72,42 @@ class Server:
         _lib.check(_lib.lib().strata_server_submit(self._h, stages.c_array(), len(stages.stages), x, y, w, h,
                                                    ctypes.byref(t)))
         return t.value
+
+    def submit_many(self, requests) -> List[int]:
+        """Submits (stages, x, y, w, h) requests in one call; their tickets,
+        in order. Checks every request first and submits none if one is
+        invalid."""
+        requests = list(requests)
+        n = len(requests)
+        arr = (_lib.ServerRequest * n)()
+        keep = []
+        for i, (stages, x, y, w, h) in enumerate(requests):
+            st = stages.c_array()
+            keep.append(st)
+            arr[i].stages = ctypes.cast(st, ctypes.POINTER(_lib.Stage))
+            arr[i].nstages = len(stages.stages)
+            arr[i].x, arr[i].y, arr[i].w, arr[i].h = x, y, w, h
+        t = (ctypes.c_uint64 * n)()
+        _lib.check(_lib.lib().strata_server_submit_many(self._h, arr, n, t))
+        return list(t)
+
+    def wait_many(self, tickets: Sequence[int], timeout_ms: int = -1) -> List[Result]:
+        """Waits for every ticket, in order; their results."""
+        n = len(tickets)
+        t = (ctypes.c_uint64 * n)(*tickets)
+        res = (_lib.ServerResult * n)()
+        _lib.check(_lib.lib().strata_server_wait_many(self._h, t, n, timeout_ms, res))
+        return [self._result(res[i]) for i in range(n)]
+
+    def release_many(self, tickets: Sequence[int]) -> None:
+        n = len(tickets)
+        _lib.check(_lib.lib().strata_server_release_many(self._h, (ctypes.c_uint64 * n)(*tickets), n))
+
+    @staticmethod
+    def _result(r) -> Result:
+        outs = [Float32Raster(r.out[k].data, r.out[k].width, r.out[k].height, r.out[k].stride,
+                              r.out[k].valid if r.out[k].valid else None, 0) for k in range(r.nout)]
+        return Result(outs, r.t_submit_ns, r.t_start_ns, r.t_done_ns)
 
     def wait(self, ticket: int, timeout_ms: int = -1) -> Result:
         r = _lib.ServerResult()

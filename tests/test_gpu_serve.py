@@ -86,3 +86,26 @@ def test_unmasked_mosaic_and_bad_window():
     with pytest.raises(engine.StrataPanic, match="outside"):
         srv.submit(OPS[0](), 250, 0, 100, 10)
     srv.close()
+
+
+def test_submit_many_equals_alone_and_is_all_or_nothing():
+    """Requests submitted, waited for and released in groups give each
+    window the result strata_process gives it alone; a group with an
+    invalid request queues none of its requests."""
+    W, H = 900, 700
+    m = to_device(_mosaic(W, H))
+    srv = serve.Server(m, streams=2, max_batch=8)
+    rng = np.random.default_rng(9)
+    reqs = _requests(rng, W, H, 30)
+    tickets = srv.submit_many([(OPS[op](), x, y, w, h) for op, x, y, w, h in reqs])
+    assert len(tickets) == len(reqs) and len(set(tickets)) == len(reqs)
+    results = srv.wait_many(tickets, timeout_ms=60000)
+    for res, (op, x, y, w, h) in zip(results, reqs):
+        assert_same_raster(to_host(res.copy()), _alone(m, op, x, y, w, h), f"group request op={op} at ({x}, {y})")
+    srv.release_many(tickets)
+    st = srv.stats()
+    assert st["served"] == len(reqs) and st["used_bytes"] == 0
+    with pytest.raises(engine.StrataPanic, match="outside"):
+        srv.submit_many([(OPS[0](), 0, 0, 10, 10), (OPS[1](), W - 5, 0, 10, 10)])
+    assert srv.stats()["served"] == len(reqs)
+    srv.close()
