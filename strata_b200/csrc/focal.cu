@@ -20,8 +20,9 @@
 // once per M x 4 x (2R+1) terms.
 //
 // Both kernels leave cells within the radius of the raster's border NaN
-// (internal/exec/halo.go:61-92) and need 16-byte aligned rows (the
-// launcher checks, else the general tile kernel runs).
+// (internal/exec/halo.go:61-92). They load and store whole float4s where
+// the rows are 16-byte aligned at the kernel's columns, and single cells
+// otherwise (the launcher decides per call).
 #include <cuda_runtime.h>
 
 #include "cellops.cuh"
@@ -35,26 +36,36 @@ namespace {
 
 template <int OP, int R>
 __global__ void __launch_bounds__(kSepThreads, (OP == STRATA_OP_SEPARABLE || OP == STRATA_OP_RUGGEDNESS) && R >= 6 ? 3 : 4)
-    sep_march_kernel(const __grid_constant__ LaunchParams P, int colblocks, int strip) {
+    sep_march_kernel(const __grid_constant__ LaunchParams P, int colblocks, int strip, int vec) {
     __shared__ __align__(16) SepSmem<OP> sm;
     const int cb = (int)(blockIdx.x % (unsigned)colblocks);
     const int sb = (int)(blockIdx.x / (unsigned)colblocks);
     const int64_t X0 = P.out_x0 + (int64_t)cb * kSepOut<R>;
     const int64_t y0 = P.out_y0 + (int64_t)sb * strip;
     const int rows = (int)((y0 + strip < P.out_y1 ? y0 + strip : P.out_y1) - y0);
-    sep_body<OP, R>(P, X0, y0, rows, true, sm);
+    sep_body<OP, R>(P, X0, y0, rows, vec != 0, sm);
 }
 
 template <int OP, int R, int KIND>
-__global__ void __launch_bounds__(kWinThreads) window_kernel(const __grid_constant__ LaunchParams P, int tiles_x) {
+__global__ void __launch_bounds__(kWinThreads) window_kernel(const __grid_constant__ LaunchParams P, int tiles_x,
+                                                             int vec) {
     __shared__ __align__(16) float tile[kWinTileFloats<OP, R, KIND>];
     const int64_t x0 = P.out_x0 + (int64_t)(blockIdx.x % (unsigned)tiles_x) * kWinTW;
     const int64_t y0 = P.out_y0 + (int64_t)(blockIdx.x / (unsigned)tiles_x) * (4 * kWinM<OP, KIND>);
-    window_body<OP, R, KIND>(P, x0, y0, true, tile);
+    window_body<OP, R, KIND>(P, x0, y0, vec != 0, tile);
 }
 
 // ---------------------------------------------------------------------------
 // Launchers.
+
+bool aligned16(const void* q) { return ((uintptr_t)q & 15) == 0; }
+
+// Whether the rows of source and destination start on 16-byte boundaries
+// at the columns the kernels load and store (then whole float4s).
+int focal_vec(const LaunchParams& p) {
+    return !(p.src_stride & 3) && !(p.dst0_stride & 3) && !((p.out_x0 - p.src_x0) & 3) &&
+           !((p.out_x0 - p.dst_x0) & 3) && aligned16(p.src) && aligned16(p.dst0);
+}
 
 int sm_count() {
     int dev = 0, n = 148;
@@ -82,7 +93,8 @@ int64_t launch_sep(const LaunchParams& p, cudaStream_t s, int64_t* window_cells)
     int64_t strip = (h + bands - 1) / bands;
     if (strip < 16) strip = 16;
     bands = (h + strip - 1) / strip;
-    sep_march_kernel<OP, R><<<(unsigned)(colblocks * bands), kSepThreads, 0, s>>>(p, (int)colblocks, (int)strip);
+    sep_march_kernel<OP, R><<<(unsigned)(colblocks * bands), kSepThreads, 0, s>>>(p, (int)colblocks, (int)strip,
+                                                                                  focal_vec(p));
     if (window_cells) {
         // each block reads its 512 columns over its band and R rows above and below, clipped to the raster
         int64_t wx = 0, wy = 0;
@@ -105,7 +117,7 @@ int64_t launch_window(const LaunchParams& p, cudaStream_t s, int64_t* window_cel
     constexpr int TH = 4 * kWinM<OP, KIND>;
     const int64_t w = p.out_x1 - p.out_x0, h = p.out_y1 - p.out_y0;
     const int64_t tiles_x = (w + kWinTW - 1) / kWinTW, tiles_y = (h + TH - 1) / TH;
-    window_kernel<OP, R, KIND><<<(unsigned)(tiles_x * tiles_y), kWinThreads, 0, s>>>(p, (int)tiles_x);
+    window_kernel<OP, R, KIND><<<(unsigned)(tiles_x * tiles_y), kWinThreads, 0, s>>>(p, (int)tiles_x, focal_vec(p));
     if (window_cells) {
         int64_t wx = 0, wy = 0;
         for (int64_t i = 0; i < tiles_x; i++) {
@@ -140,8 +152,6 @@ int64_t launch_radius(const LaunchParams& p, cudaStream_t s, int64_t* wc) {
     return -1;
 }
 
-bool aligned16(const void* q) { return ((uintptr_t)q & 15) == 0; }
-
 }  // namespace
 
 bool focal_eligible(const LaunchParams& p) {
@@ -157,9 +167,6 @@ bool focal_eligible(const LaunchParams& p) {
     }
     const int64_t w = p.out_x1 - p.out_x0, h = p.out_y1 - p.out_y0;
     if (w <= 0 || h <= 0) return false;
-    if ((p.src_stride & 3) || (p.dst0_stride & 3)) return false;
-    if (((p.out_x0 - p.src_x0) & 3) || ((p.out_x0 - p.dst_x0) & 3)) return false;
-    if (!aligned16(p.src) || !aligned16(p.dst0)) return false;
     // 32-bit block, row and column arithmetic inside the kernels.
     const int64_t blocks = ((w + 127) / 128) * ((h + 15) / 16);
     return blocks < ((int64_t)1 << 31) && p.height < ((int64_t)1 << 30) && p.width < ((int64_t)1 << 30) &&

@@ -200,6 +200,15 @@ int64_t launch_data(const LaunchParams& p, cudaStream_t s, int64_t* window_cells
         }
         return blocks;
     }
+    if (march_any_eligible(p)) {
+        const int64_t blocks = launch_march_any(p, s);
+        if (window_cells) {
+            const int64_t w = p.out_x1 - p.out_x0, segs = (w + 127) / 128;
+            const int64_t rows = (p.out_y1 - p.out_y0) + 2 * (blocks / ((segs + 3) / 4));
+            *window_cells = (w + 2 * segs) * (rows < p.height ? rows : p.height);
+        }
+        return blocks;
+    }
     if (focal_eligible(p)) return launch_focal(p, s, window_cells);
     const int64_t tiles = L(p, s);
     if (window_cells) {

@@ -145,9 +145,14 @@ void launch_validity(const ValidityParams& v, cudaStream_t stream);
 // multiple of 4), and its launcher.
 bool march3_eligible(const LaunchParams& p);
 int64_t launch_march3(const LaunchParams& p, cudaStream_t stream);
+// The same march for any alignment and stride, with per-cell loads and
+// stores (march3.cu march_any_kernel).
+bool march_any_eligible(const LaunchParams& p);
+int64_t launch_march_any(const LaunchParams& p, cudaStream_t stream);
 // The register-blocked focal kernels (focal.cu) for the windowed ops at
-// radius 2..8 on 16-byte aligned rows; launch_focal returns the blocks
-// launched and sets *window_cells (if given) to the cells they read.
+// radius 2..8 (vector loads and stores where rows are 16-byte aligned,
+// per-cell ones otherwise); launch_focal returns the blocks launched and
+// sets *window_cells (if given) to the cells they read.
 bool focal_eligible(const LaunchParams& p);
 int64_t launch_focal(const LaunchParams& p, cudaStream_t stream, int64_t* window_cells);
 

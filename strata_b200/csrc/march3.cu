@@ -30,7 +30,8 @@
 //
 // The launcher takes these paths only when every row of the source and
 // destination starts on a 16-byte boundary at the region's first column
-// and the region is a multiple of 4 wide; otherwise the tile kernel runs.
+// and the region is a multiple of 4 wide; otherwise march_any_kernel runs
+// the same march with per-cell loads and stores (march.cuh march_warp).
 #include <cuda.h>
 
 #include "launch.h"
@@ -400,6 +401,45 @@ int64_t launch_epi(const LaunchParams& p, cudaStream_t s) {
     return p.nepi ? launch_march<OP, KIND, true>(p, s) : launch_march<OP, KIND, false>(p, s);
 }
 
+// Rasters whose rows are not 16-byte aligned where the march loads and
+// stores (a window at any origin, any stride or width): the same march,
+// a warp per 128 columns of a strip, with per-cell loads and stores
+// (march.cuh march_warp).
+template <int OP, int KIND, bool EPI>
+__global__ void __launch_bounds__(kWarps * 32) march_any_kernel(const __grid_constant__ LaunchParams P, int strip,
+                                                                int col_blocks) {
+    EpiTables* T = EpiSmem<EPI>::get();
+    if constexpr (EPI) {
+        stage_epilogue(P, *T);
+        __syncthreads();
+    }
+    const int warp = threadIdx.x >> 5;
+    const int cb = blockIdx.x % col_blocks;
+    const int sb = blockIdx.x / col_blocks;
+    const int64_t xs = P.out_x0 + (int64_t)(cb * kWarps + warp) * 128;
+    if (xs >= P.out_x1) return;  // warp-uniform
+    const int64_t y0 = P.out_y0 + (int64_t)sb * strip;
+    const int rows = (int)min((int64_t)strip, P.out_y1 - y0);
+    march_warp<OP, KIND, EPI>(P, T, xs, y0, rows, false);
+}
+
+template <int OP, int KIND, bool EPI>
+int64_t launch_any(const LaunchParams& p, cudaStream_t s) {
+    const int64_t w = p.out_x1 - p.out_x0, h = p.out_y1 - p.out_y0;
+    const int64_t segs = (w + 127) / 128;
+    const int64_t col_blocks = (segs + kWarps - 1) / kWarps;
+    int64_t strip = segs > 0 ? (h * segs) / (148 * 48 * 4) : h;
+    strip = strip < 8 ? 8 : (strip > 64 ? 64 : strip);
+    const int64_t blocks = col_blocks * ((h + strip - 1) / strip);
+    march_any_kernel<OP, KIND, EPI><<<(unsigned)blocks, kWarps * 32, 0, s>>>(p, (int)strip, (int)col_blocks);
+    return blocks;
+}
+
+template <int OP, int KIND>
+int64_t launch_any_epi(const LaunchParams& p, cudaStream_t s) {
+    return p.nepi ? launch_any<OP, KIND, true>(p, s) : launch_any<OP, KIND, false>(p, s);
+}
+
 }  // namespace
 
 bool march3_eligible(const LaunchParams& p) {
@@ -413,6 +453,36 @@ bool march3_eligible(const LaunchParams& p) {
     const int64_t col_blocks = ((w + 127) / 128 + kWarps - 1) / kWarps;
     const int64_t blocks = col_blocks * ((p.out_y1 - p.out_y0 + 7) / 8);
     return blocks < ((int64_t)1 << 31) && p.height < ((int64_t)1 << 30) && p.src_h < ((int64_t)1 << 30);
+}
+
+bool march_any_eligible(const LaunchParams& p) {
+    if (p.radius > 1 || p.op < STRATA_OP_GRADIENT || p.op > STRATA_OP_MAX) return false;
+    const int64_t w = p.out_x1 - p.out_x0;
+    if (w <= 0) return false;
+    // 32-bit block, row and column arithmetic inside the kernel.
+    const int64_t col_blocks = ((w + 127) / 128 + kWarps - 1) / kWarps;
+    const int64_t blocks = col_blocks * ((p.out_y1 - p.out_y0 + 7) / 8);
+    return blocks < ((int64_t)1 << 31) && p.height < ((int64_t)1 << 30) && p.src_h < ((int64_t)1 << 30) &&
+           p.src_w < ((int64_t)1 << 30) && p.width < ((int64_t)1 << 30);
+}
+
+int64_t launch_march_any(const LaunchParams& p, cudaStream_t s) {
+    switch (p.op) {
+    case STRATA_OP_GRADIENT: return launch_any<STRATA_OP_GRADIENT, 0, false>(p, s);
+    case STRATA_OP_SLOPE:
+        return p.kind ? launch_any_epi<STRATA_OP_SLOPE, 1>(p, s) : launch_any_epi<STRATA_OP_SLOPE, 0>(p, s);
+    case STRATA_OP_ASPECT:
+        return p.kind ? launch_any_epi<STRATA_OP_ASPECT, 1>(p, s) : launch_any_epi<STRATA_OP_ASPECT, 0>(p, s);
+    case STRATA_OP_HILLSHADE: return launch_any_epi<STRATA_OP_HILLSHADE, 0>(p, s);
+    case STRATA_OP_CURVATURE: return launch_any_epi<STRATA_OP_CURVATURE, 0>(p, s);
+    case STRATA_OP_RUGGEDNESS: return launch_any_epi<STRATA_OP_RUGGEDNESS, 0>(p, s);
+    case STRATA_OP_CORRELATE: return launch_any_epi<STRATA_OP_CORRELATE, 0>(p, s);
+    case STRATA_OP_SEPARABLE: return launch_any_epi<STRATA_OP_SEPARABLE, 0>(p, s);
+    case STRATA_OP_MEAN: return launch_any_epi<STRATA_OP_MEAN, 0>(p, s);
+    case STRATA_OP_MIN: return launch_any_epi<STRATA_OP_MIN, 0>(p, s);
+    case STRATA_OP_MAX: return launch_any_epi<STRATA_OP_MAX, 0>(p, s);
+    }
+    return -1;
 }
 
 int64_t launch_march3(const LaunchParams& p, cudaStream_t s) {

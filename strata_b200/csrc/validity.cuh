@@ -177,23 +177,43 @@ __device__ __forceinline__ void validity_strip(const ValidityParams& v, int64_t 
         colin = mlo & mhi;
     }
     const bool masked = v.src_bits != nullptr;
-    // Source bit of cell (c0 - R) in row y0 - R, advanced a row at a time.
-    int64_t sb = v.src_off + (y0 - R - v.src_y0) * v.src_stride + (c0 - R - v.src_x0);
-    auto hrow = [&]() -> uint32_t {
-        uint32_t h = 0xffffffffu;
-        if (masked) {
-            const int64_t w = floor_div32(sb);
-            const int sh = (int)(sb - w * 32);
-            const uint32_t a0 = src_word(v, w), a1 = src_word(v, w + 1), a2 = src_word(v, w + 2);
-            const uint64_t win = (uint64_t)__funnelshift_r(a0, a1, sh) | ((uint64_t)__funnelshift_r(a1, a2, sh) << 32);
-            h = erode<D>(win);
-        }
-        sb += v.src_stride;
-        return h;
+    // The source rows' words, loaded 2R+1 rows ahead of their use so that
+    // a warp keeps that many rows of loads in flight: slot m % (2R+1) holds
+    // the words of source row y0 - R + m until row m is eroded.
+    struct Raw {
+        uint32_t a0, a1, a2;
+        int sh;
     };
+    int64_t lb = v.src_off + (y0 - R - v.src_y0) * v.src_stride + (c0 - R - v.src_x0);  // next row's bit
+    auto load = [&]() -> Raw {
+        Raw r;
+        const int64_t w = floor_div32(lb);
+        r.sh = (int)(lb - w * 32);
+        r.a0 = src_word(v, w);
+        r.a1 = src_word(v, w + 1);
+        r.a2 = src_word(v, w + 2);
+        lb += v.src_stride;
+        return r;
+    };
+    auto eroded = [&](const Raw& r) -> uint32_t {
+        const uint64_t win =
+            (uint64_t)__funnelshift_r(r.a0, r.a1, r.sh) | ((uint64_t)__funnelshift_r(r.a1, r.a2, r.sh) << 32);
+        return erode<D>(win);
+    };
+    Raw pa[D];
+    if (masked) {
+#pragma unroll
+        for (int j = 0; j < D; j++) pa[j] = load();
+    }
     uint32_t ring[D];
 #pragma unroll
-    for (int k = 0; k < 2 * R; k++) ring[k] = hrow();
+    for (int k = 0; k < 2 * R; k++) {
+        ring[k] = 0xffffffffu;
+        if (masked) {
+            ring[k] = eroded(pa[k]);
+            pa[k] = load();
+        }
+    }
     // Destination bit of cell cw in row y0, advanced a row at a time.
     int64_t db = v.dst_off + (y0 - v.dst_y0) * v.dst_stride + (cw - v.dst_x0);
     int64_t y = y0;
@@ -201,7 +221,12 @@ __device__ __forceinline__ void validity_strip(const ValidityParams& v, int64_t 
 #pragma unroll
         for (int u = 0; u < D; u++) {
             if (yb + u >= rows) break;
-            ring[(u + 2 * R) % D] = hrow();
+            const int slot = (u + 2 * R) % D;
+            ring[slot] = 0xffffffffu;
+            if (masked) {
+                ring[slot] = eroded(pa[slot]);
+                pa[slot] = load();
+            }
             uint32_t e = 0xffffffffu;
 #pragma unroll
             for (int k = 0; k < D; k++) e &= ring[k];
