@@ -27,7 +27,6 @@
 
 #include "cellops.cuh"
 #include "focal.cuh"
-#include "focalops.cuh"
 #include "launch.h"
 #include "ops3.cuh"
 

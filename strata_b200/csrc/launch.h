@@ -156,7 +156,5 @@ int64_t launch_march_any(const LaunchParams& p, cudaStream_t stream);
 bool focal_eligible(const LaunchParams& p);
 int64_t launch_focal(const LaunchParams& p, cudaStream_t stream, int64_t* window_cells);
 
-// Tile geometry of the data kernels, for Stats.
-void tile_shape(int op, int radius, int64_t width, int* tw, int* th);
 
 }  // namespace strata

@@ -26,7 +26,7 @@
 // the window's top, middle and bottom row, so each row's difference is
 // computed once and used by three output rows. The operations and their
 // order per cell are the reference's, so the bits are too. The other ops
-// evaluate apply3 (ops3.cuh), shared with the general tile kernel.
+// evaluate apply3 (ops3.cuh), shared with the batch kernels' march.
 //
 // The launcher takes these paths only when every row of the source and
 // destination starts on a 16-byte boundary at the region's first column
