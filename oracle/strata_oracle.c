@@ -721,6 +721,15 @@ int orc_process(const orc_stage *stages, int nstages, const orc_raster *src,
     if (st->op < ORC_GRADIENT || st->op > ORC_RECLASS) return -1;
     for (int i = 1; i < nstages; i++)
         if (stages[i].op != ORC_LOOKUP && stages[i].op != ORC_RECLASS) return -1;
+    /* Pointwise tables: Lookup's knots and values pair up (at least one);
+     * Reclass has one value more than breaks (zero breaks allowed). */
+    for (int i = 0; i < nstages; i++) {
+        const orc_stage *p = &stages[i];
+        if (p->op != ORC_LOOKUP && p->op != ORC_RECLASS) continue;
+        const int n0 = p->table_len[0], n1 = p->table_len[1];
+        if (p->op == ORC_LOOKUP ? (n0 < 1 || n1 != n0) : (n0 < 0 || n1 != n0 + 1)) return -1;
+        if ((n0 > 0 && !p->table[0]) || !p->table[1]) return -1;
+    }
     if (ndst != (st->op == ORC_GRADIENT ? 2 : 1)) return -1;
     if (src->valid)
         for (int d = 0; d < ndst; d++)

@@ -144,8 +144,38 @@ __device__ __forceinline__ void epi_stage4(const EpiStage& e, const float* ta, c
     }
 }
 
+// Breaks of a lone Reclass stage that the select chain below takes; the
+// folded Lookup -> Reclass tail of a slope classification has a handful.
+constexpr int kChainBreaks = 8;
+
+// A lone Reclass over four cells as a chain of selects against its breaks
+// in increasing order: the last break at or below v names the class, which
+// is the search's count for strictly increasing, NaN-free breaks (the host
+// checks both), and a NaN cell stays NaN. A break costs a compare and a
+// select per cell, with no dependent table loads; the guard on the break
+// count is uniform and shared by the four cells.
+__device__ __forceinline__ void reclass_chain4(const EpiStage& e, float (&v)[4]) {
+    const int n = e.n;
+    float r[4];
+#pragma unroll
+    for (int c = 0; c < 4; c++) r[c] = e.b[0];
+#pragma unroll
+    for (int j = 0; j < kChainBreaks; j++) {
+        if (j >= n) break;
+        const float t = e.a[j], y = e.b[j + 1];
+#pragma unroll
+        for (int c = 0; c < 4; c++) r[c] = v[c] >= t ? y : r[c];
+    }
+#pragma unroll
+    for (int c = 0; c < 4; c++) v[c] = v[c] != v[c] ? v[c] : r[c];
+}
+
 // The epilogue over four cells, stage by stage.
 __device__ __forceinline__ void epilogue4(const LaunchParams& P, const EpiTables& T, float (&v)[4]) {
+    if (P.nepi == 1 && P.epi[0].op == STRATA_OP_RECLASS && P.epi[0].n <= kChainBreaks) {
+        reclass_chain4(P.epi[0], v);
+        return;
+    }
 #pragma unroll
     for (int i = 0; i < kMaxEpilogue; i++)
         if (i < P.nepi) epi_stage4(P.epi[i], T.a[i], T.b[i], T.p2[i], v);

@@ -66,14 +66,17 @@ def _orc_dict(r: Float32Raster):
 def oracle_stage(st: _lib.Stage):
     """The oracle stage equal to a product stage (Convolve's rotation, which
     focal/correlate.go:80-86 applies on the host, applied here)."""
+    # Tables keep their slots: an empty one (a Reclass with no breaks) is
+    # an empty array ahead of the later ones.
     tables = []
     for i in range(4):
         n = st.table_len[i]
         if st.table[i] and n > 0:
-            a = np.ctypeslib.as_array((np.ctypeslib.ctypes.c_float * n).from_address(st.table[i])).copy()
-            tables.append(a)
+            tables.append(np.ctypeslib.as_array((np.ctypeslib.ctypes.c_float * n).from_address(st.table[i])).copy())
         else:
-            break
+            tables.append(np.zeros(0, np.float32))
+    while tables and tables[-1].size == 0:
+        tables.pop()
     if st.op == _lib.OP_CORRELATE and st.flags & _lib.STAGE_ROTATE180:
         tables[0] = tables[0][::-1].copy()
     return orc.stage(st.op, st.radius, st.kind, list(st.k), tables)

@@ -223,6 +223,35 @@ def test_folded_pointwise_tail_edges(seed):
         f"slope+tail seed={seed}")
 
 
+@pytest.mark.parametrize("nb", [0, 1, 2, 4, 7, 8, 9, 20])
+def test_stencil_reclass_on_output_values(nb):
+    """A lone Reclass after a stencil, with breaks drawn from the stencil's
+    own outputs so that cells fall exactly on them, and a break at +0 or -0
+    under a flat patch (slope exactly 0): up to 8 breaks take the select
+    chain of the marching kernels' epilogue, more take the table search,
+    and both equal the oracle bit for bit on aligned and strided layouts,
+    masked or not, host or device operands."""
+    w, h = 300, 200
+    dem = dem_cells(w, h, 40 + nb)
+    dem[50:80, 40:90] = np.float32(1234.5)
+    slope = lambda: terrain.slope_stage(terrain.SlopeOptions(CellSize=10))
+    src = host_raster(dem)
+    ref = like(src, masked=False)
+    run_oracle(slope(), src, [ref])
+    vals = np.unique(ref.data[np.isfinite(ref.data)])
+    assert vals[0] == 0 and len(vals) > nb
+    rng = np.random.default_rng(nb)
+    picked = np.sort(rng.choice(vals[vals > 0], max(nb - 1, 0), replace=False))
+    zero = np.float32(-0.0) if nb % 2 else np.float32(0.0)
+    breaks = np.concatenate([[zero], picked]).astype(np.float32)[:nb]
+    values = (rng.standard_normal(nb + 1) * 5).astype(np.float32)
+    values[int(rng.integers(nb + 1))] = np.nan
+    make = lambda: slope().extend(transfer.reclass_stage(breaks, values))
+    for masked, device in itertools.product((False, True), (False, True)):
+        for li, lay in enumerate(layouts(w, h, nb, masked)):
+            check_case(make(), dem, 1, device, lay, f"nb={nb} masked={masked} device={device} layout={li}")
+
+
 def test_pipeline_slope_lookup_reclass():
     """The fused Slope -> Lookup -> Reclass pass equals the oracle's three
     stages, which equal three separate calls (internal/exec/pipeline.go)."""

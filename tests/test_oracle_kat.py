@@ -334,3 +334,23 @@ def test_validity_erosion_matches_naive():
             for xx in range(w):
                 want = (r <= xx < w - r and r <= yy < h - r and valid[yy - r:yy + r + 1, xx - r:xx + r + 1].all())
                 assert bool(got[off + yy * stride + xx]) == want
+
+
+def test_reclass_without_breaks():
+    """Zero breaks: every cell takes the one value, NaN stays NaN."""
+    out = pointwise(orc.stage(orc.RECLASS, 0, 0, [], [np.zeros(0, np.float32), fs(["0x40e00000"])]),
+                    ["0x7fc00000", "0xbf800000", "0x80000000", "0x7f800000"])
+    assert np.isnan(out[0]) and (out[1:] == np.float32(7)).all()
+
+
+def test_pointwise_tables_checked():
+    """Mismatched or missing Lookup / Reclass tables are an invalid call,
+    not a read past them."""
+    src = raster([1, 2, 3], 3, 1)
+    bad = [orc.stage(orc.RECLASS, 0, 0, [], [fs(["0x3f800000"])]),
+           orc.stage(orc.RECLASS, 0, 0, [], [fs(["0x3f800000"]), fs(["0x3f800000"])]),
+           orc.stage(orc.LOOKUP, 0, 0, [], [fs(["0x3f800000", "0x40000000"]), fs(["0x3f800000"])]),
+           orc.stage(orc.LOOKUP, 0, 0, [], [])]
+    for st in bad:
+        with pytest.raises(ValueError):
+            run([st], src)
