@@ -173,6 +173,140 @@ __device__ __forceinline__ float zt_curvature(float z1, float z2, float z3, floa
     return sub(0.0f, div(num, add(d, d)));
 }
 
+// ---------------------------------------------------------------------------
+// Two cells per instruction. PTX add/sub/mul.rn.f32x2 (sm_100a) round each
+// half exactly as __fadd_rn / __fsub_rn / __fmul_rn round it, subnormals
+// kept (no .ftz), so a pair of cells taken through these has the scalar
+// functions' bits in half the issue slots. The halves live in an aligned
+// register pair: packing is free for fresh results and for neighbours
+// loaded side by side, and reading a half back is free.
+//
+// One rule: a packed product never feeds a packed add or subtract. The
+// assembler fuses that pair into one packed fused multiply-add (a single
+// rounding) whatever the rounding modifiers and --fmad say, where a packed
+// product summed half by half (add_p / sub_p), or scalar products summed
+// packed, keep both roundings; a device check of 2^23 pairs per form
+// showed the fused pair off in 5-18% of them and the split forms exact.
+
+struct F2 {
+    uint64_t r;
+};
+__device__ __forceinline__ F2 pk(float lo, float hi) {
+    F2 p;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(p.r) : "f"(lo), "f"(hi));
+    return p;
+}
+__device__ __forceinline__ F2 splat(float v) { return pk(v, v); }
+__device__ __forceinline__ float lo(F2 p) { return __uint_as_float((uint32_t)p.r); }
+__device__ __forceinline__ float hi(F2 p) { return __uint_as_float((uint32_t)(p.r >> 32)); }
+__device__ __forceinline__ F2 add2(F2 a, F2 b) {
+    F2 d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d.r) : "l"(a.r), "l"(b.r));
+    return d;
+}
+__device__ __forceinline__ F2 sub2(F2 a, F2 b) {
+    F2 d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d.r) : "l"(a.r), "l"(b.r));
+    return d;
+}
+__device__ __forceinline__ F2 mul2(F2 a, F2 b) {
+    F2 d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d.r) : "l"(a.r), "l"(b.r));
+    return d;
+}
+// prod + b and prod - b for a packed product prod, half by half.
+__device__ __forceinline__ F2 add_p(F2 prod, F2 b) { return pk(add(lo(prod), lo(b)), add(hi(prod), hi(b))); }
+__device__ __forceinline__ F2 sub_p(F2 prod, F2 b) { return pk(sub(lo(prod), lo(b)), sub(hi(prod), hi(b))); }
+
+// atan32 over a pair: the same steps, the halves apart only for the
+// argument reduction and the division.
+__device__ __forceinline__ F2 atan32x2(F2 x) {
+    const F2 xm = sub2(x, splat(1.0f)), xp = add2(x, splat(1.0f));
+    const float xs[2] = {lo(x), hi(x)}, xms[2] = {lo(xm), hi(xm)}, xps[2] = {lo(xp), hi(xp)};
+    float t[2], y0[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        float num = xs[h], den = 1.0f;
+        y0[h] = 0.0f;
+        if (xs[h] > kTanPi8) {
+            num = xms[h];
+            den = xps[h];
+            y0[h] = kPi4;
+        }
+        if (xs[h] > kTan3Pi8) {
+            num = -1.0f;
+            den = xs[h];
+            y0[h] = kPi2;
+        }
+        t[h] = div(num, den);
+    }
+    const F2 tt = pk(t[0], t[1]);
+    const F2 z = mul2(tt, tt);
+    F2 p = sub_p(mul2(splat(kC4), z), splat(kC3));
+    p = add_p(mul2(p, z), splat(kC2));
+    p = sub_p(mul2(p, z), splat(kC1));
+    return add2(pk(y0[0], y0[1]), add_p(mul2(mul2(p, z), tt), tt));
+}
+
+// slope over a pair of gradients.
+__device__ __forceinline__ F2 slope2(F2 gx, F2 gy, F2 scale, bool take_atan) {
+    const F2 s = add_p(mul2(gx, gx), mul2(gy, gy));
+    const F2 m = pk(sqrt64of32(lo(s)), sqrt64of32(hi(s)));
+    return mul2(take_atan ? atan32x2(m) : m, scale);
+}
+
+// aspect over a pair of gradients (atan2f32's steps inline).
+__device__ __forceinline__ F2 aspect2(F2 gx, F2 gy, float flat, bool trig) {
+    const F2 ngx = pk(sub(0.0f, lo(gx)), sub(0.0f, hi(gx)));
+    const F2 y = trig ? gy : ngx, x = trig ? ngx : gy;
+    const float ys[2] = {lo(y), hi(y)}, xs[2] = {lo(x), hi(x)};
+    float ax[2], ay[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        ax[h] = abs32(xs[h]);
+        ay[h] = abs32(ys[h]);
+    }
+    const F2 at = atan32x2(pk(div(ay[0], ax[0]), div(ay[1], ax[1])));
+    const F2 flip = sub2(splat(kPi), at);
+    const float ats[2] = {lo(at), hi(at)}, flips[2] = {lo(flip), hi(flip)};
+    float a[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        float v = ats[h];
+        if (ay[h] == 0.0f && ax[h] == 0.0f) v = 0.0f;
+        if (ay[h] == ax[h] && ay[h] > 0x1.fffffep+127f) v = kPi4;
+        // sub(kPi, v) for the special values above is their own pair entry
+        float f = flips[h];
+        if (ay[h] == 0.0f && ax[h] == 0.0f) f = kPi;
+        if (ay[h] == ax[h] && ay[h] > 0x1.fffffep+127f) f = sub(kPi, kPi4);
+        if (__float_as_uint(xs[h]) & 0x80000000u) v = f;
+        a[h] = __uint_as_float(__float_as_uint(v) | (__float_as_uint(ys[h]) & 0x80000000u));
+    }
+    F2 d = mul2(pk(a[0], a[1]), splat(kRadToDeg));
+    const float ds[2] = {lo(d), hi(d)};
+    d = add_p(d, pk(ds[0] < 0.0f ? 360.0f : 0.0f, ds[1] < 0.0f ? 360.0f : 0.0f));
+    float r[2] = {lo(d), hi(d)};
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        if (r[h] >= 360.0f) r[h] = 0.0f;
+        if (ys[h] == 0.0f && xs[h] == 0.0f) r[h] = flat;
+    }
+    return pk(r[0], r[1]);
+}
+
+// shade over a pair of gradients.
+__device__ __forceinline__ F2 shade2(F2 gx, F2 gy, float c, float bx, float by) {
+    const F2 num = add2(splat(c), add_p(mul2(splat(bx), gx), mul2(splat(by), gy)));
+    const F2 s = add2(splat(1.0f), add_p(mul2(gx, gx), mul2(gy, gy)));
+    float v[2] = {div(lo(num), sqrt64of32(lo(s))), div(hi(num), sqrt64of32(hi(s)))};
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        if (v[h] < 0.0f) v[h] = 0.0f;
+        if (v[h] > 255.0f) v[h] = 255.0f;
+    }
+    return pk(v[0], v[1]);
+}
+
 __device__ __forceinline__ double sq64(float d) {
     double x = (double)d;
     return __dmul_rn(x, x);

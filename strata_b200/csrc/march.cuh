@@ -50,8 +50,9 @@ __device__ __forceinline__ void row_compute(const LaunchParams& P, const EpiTabl
                                             const float (&ha)[4], const float (&hb)[4], const float (&hc)[4],
                                             bool rowin, const bool (&colin)[4], float (&o0)[4], float (&o1)[4]) {
     const float nan = nanf32();
-    if constexpr (kIsHorn<OP>) {
-        // hornDY's vertical differences: bottom row minus top row.
+    if constexpr (OP == STRATA_OP_GRADIENT) {
+        // hornDY's vertical differences: bottom row minus top row. (Two
+        // outputs and no finisher: the scalar form holds fewer registers.)
         float v[6];
 #pragma unroll
         for (int j = 0; j < 6; j++) v[j] = sub(c.v[j], a.v[j]);
@@ -59,22 +60,41 @@ __device__ __forceinline__ void row_compute(const LaunchParams& P, const EpiTabl
         for (int i = 0; i < 4; i++) {
             const float dx = add(add(ha[i], hc[i]), add(hb[i], hb[i]));
             const float dy = add(add(v[i], v[i + 2]), add(v[i + 1], v[i + 1]));
-            const float gx = mul(dx, P.k[0]);
-            const float gy = mul(dy, P.k[1]);
             const bool in = rowin && colin[i];
-            if constexpr (OP == STRATA_OP_GRADIENT) {
-                o0[i] = in ? gx : nan;
-                o1[i] = in ? gy : nan;
-            } else {
-                float r;
-                if constexpr (OP == STRATA_OP_SLOPE) r = slope(gx, gy, P.k[2], KIND != 0);
-                else if constexpr (OP == STRATA_OP_ASPECT) r = aspect(gx, gy, P.k[2], KIND != 0);
-                else r = shade(gx, gy, P.k[2], P.k[3], P.k[4]);
-                o0[i] = in ? r : nan;
-            }
+            o0[i] = in ? mul(dx, P.k[0]) : nan;
+            o1[i] = in ? mul(dy, P.k[1]) : nan;
+        }
+    } else if constexpr (kIsHorn<OP>) {
+        // The lane's cells in pairs (0, 1) and (2, 3), packed (cellops F2),
+        // each step the scalar hornDX / hornDY / finisher step of its cell.
+        // hornDY's vertical differences V_j, bottom row minus top row: the
+        // centre columns 1..4 come in aligned pairs, the halo columns alone.
+        const F2 V12 = sub2(pk(c.v[1], c.v[2]), pk(a.v[1], a.v[2]));
+        const F2 V34 = sub2(pk(c.v[3], c.v[4]), pk(a.v[3], a.v[4]));
+        const float V0 = sub(c.v[0], a.v[0]), V5 = sub(c.v[5], a.v[5]);
+        // dy_i = (V_i + V_i+2) + (V_i+1 + V_i+1)
+        const F2 dy[2] = {add2(pk(add(V0, hi(V12)), add(lo(V12), lo(V34))), add2(V12, V12)),
+                          add2(pk(add(hi(V12), hi(V34)), add(lo(V34), V5)), add2(V34, V34))};
+        // dx_i = (ha_i + hc_i) + (hb_i + hb_i)
+        F2 gx[2], gy[2];
+#pragma unroll
+        for (int p = 0; p < 2; p++) {
+            const F2 hb2 = pk(hb[2 * p], hb[2 * p + 1]);
+            const F2 dx = add2(add2(pk(ha[2 * p], ha[2 * p + 1]), pk(hc[2 * p], hc[2 * p + 1])), add2(hb2, hb2));
+            gx[p] = mul2(dx, splat(P.k[0]));
+            gy[p] = mul2(dy[p], splat(P.k[1]));
+        }
+#pragma unroll
+        for (int p = 0; p < 2; p++) {
+            F2 r;
+            if constexpr (OP == STRATA_OP_SLOPE) r = slope2(gx[p], gy[p], splat(P.k[2]), KIND != 0);
+            else if constexpr (OP == STRATA_OP_ASPECT) r = aspect2(gx[p], gy[p], P.k[2], KIND != 0);
+            else r = shade2(gx[p], gy[p], P.k[2], P.k[3], P.k[4]);
+            o0[2 * p] = rowin && colin[2 * p] ? lo(r) : nan;
+            o0[2 * p + 1] = rowin && colin[2 * p + 1] ? hi(r) : nan;
         }
         // The epilogue maps NaN to itself, so the edge ring stays NaN.
-        if constexpr (EPI && OP != STRATA_OP_GRADIENT) epilogue4(P, *T, o0);
+        if constexpr (EPI) epilogue4(P, *T, o0);
     } else {
 #pragma unroll
         for (int i = 0; i < 4; i++) {

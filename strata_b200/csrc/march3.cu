@@ -124,7 +124,7 @@ __device__ __forceinline__ Row6 load_row(Lane& L) {
 constexpr int kRing = 4;  // three window rows and one in flight
 
 template <int OP, int KIND, bool EPI>
-__global__ void __launch_bounds__(kWarps * 32, 8) march3_kernel(const __grid_constant__ LaunchParams P, int strip,
+__global__ void __launch_bounds__(kWarps * 32, 6) march3_kernel(const __grid_constant__ LaunchParams P, int strip,
                                                                  int col_blocks) {
     constexpr bool kHorn = kIsHorn<OP>;
     EpiTables* T = EpiSmem<EPI>::get();
