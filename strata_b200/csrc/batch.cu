@@ -147,6 +147,7 @@ Key key_of(const LaunchParams& p) {
     if (p.radius <= 1) {
         k.radius = 1;
         if (p.op == STRATA_OP_SLOPE || p.op == STRATA_OP_ASPECT) k.kind = p.kind ? 1 : 0;
+        if (p.op == STRATA_OP_CURVATURE || p.op == STRATA_OP_RUGGEDNESS) k.kind = p.kind;
         k.epi = p.nepi > 0;
     } else if (p.op == STRATA_OP_CORRELATE || (p.op == STRATA_OP_RUGGEDNESS && p.kind != STRATA_RUG_ROUGHNESS)) {
         k.family = 2;
@@ -255,8 +256,21 @@ bool launch_batch_class(const BatchClass& c, const BatchItem* d, cudaStream_t s)
     case STRATA_OP_ASPECT:
         return c.kind ? launch_march_epi<STRATA_OP_ASPECT, 1>(c, d, s) : launch_march_epi<STRATA_OP_ASPECT, 0>(c, d, s);
     case STRATA_OP_HILLSHADE: return launch_march_epi<STRATA_OP_HILLSHADE, 0>(c, d, s);
-    case STRATA_OP_CURVATURE: return launch_march_epi<STRATA_OP_CURVATURE, 0>(c, d, s);
-    case STRATA_OP_RUGGEDNESS: return launch_march_epi<STRATA_OP_RUGGEDNESS, 0>(c, d, s);
+    case STRATA_OP_CURVATURE:
+        switch (c.kind) {
+        case 0: return launch_march_epi<STRATA_OP_CURVATURE, 0>(c, d, s);
+        case 1: return launch_march_epi<STRATA_OP_CURVATURE, 1>(c, d, s);
+        case 2: return launch_march_epi<STRATA_OP_CURVATURE, 2>(c, d, s);
+        }
+        return false;
+    case STRATA_OP_RUGGEDNESS:
+        switch (c.kind) {
+        case STRATA_RUG_TRI_RILEY: return launch_march_epi<STRATA_OP_RUGGEDNESS, kKindAtRun>(c, d, s);
+        case STRATA_RUG_TRI_WILSON: return launch_march_epi<STRATA_OP_RUGGEDNESS, STRATA_RUG_TRI_WILSON>(c, d, s);
+        case STRATA_RUG_TPI: return launch_march_epi<STRATA_OP_RUGGEDNESS, STRATA_RUG_TPI>(c, d, s);
+        case STRATA_RUG_ROUGHNESS: return launch_march_epi<STRATA_OP_RUGGEDNESS, STRATA_RUG_ROUGHNESS>(c, d, s);
+        }
+        return false;
     case STRATA_OP_CORRELATE: return launch_march_epi<STRATA_OP_CORRELATE, 0>(c, d, s);
     case STRATA_OP_SEPARABLE: return launch_march_epi<STRATA_OP_SEPARABLE, 0>(c, d, s);
     case STRATA_OP_MEAN: return launch_march_epi<STRATA_OP_MEAN, 0>(c, d, s);

@@ -214,9 +214,10 @@ __device__ __forceinline__ F2 mul2(F2 a, F2 b) {
     asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d.r) : "l"(a.r), "l"(b.r));
     return d;
 }
-// prod + b and prod - b for a packed product prod, half by half.
-__device__ __forceinline__ F2 add_p(F2 prod, F2 b) { return pk(add(lo(prod), lo(b)), add(hi(prod), hi(b))); }
-__device__ __forceinline__ F2 sub_p(F2 prod, F2 b) { return pk(sub(lo(prod), lo(b)), sub(hi(prod), hi(b))); }
+// a + b and a - b half by half: the sums with a packed product among
+// their operands.
+__device__ __forceinline__ F2 add_p(F2 a, F2 b) { return pk(add(lo(a), lo(b)), add(hi(a), hi(b))); }
+__device__ __forceinline__ F2 sub_p(F2 a, F2 b) { return pk(sub(lo(a), lo(b)), sub(hi(a), hi(b))); }
 
 // atan32 over a pair: the same steps, the halves apart only for the
 // argument reduction and the division.
@@ -303,6 +304,48 @@ __device__ __forceinline__ F2 shade2(F2 gx, F2 gy, float c, float bx, float by) 
     for (int h = 0; h < 2; h++) {
         if (v[h] < 0.0f) v[h] = 0.0f;
         if (v[h] > 255.0f) v[h] = 255.0f;
+    }
+    return pk(v[0], v[1]);
+}
+
+// zt_curvature over a pair of cells, from the window sums and differences
+// the caller forms: d64 = z6 - z4, d82 = z8 - z2, c = z5 + z5,
+// s46 = z4 + z6, s28 = z2 + z8, s19 = z1 + z9, s37 = z3 + z7.
+__device__ __forceinline__ F2 zt_curvature2(F2 d64, F2 d82, F2 c, F2 s46, F2 s28, F2 s19, F2 s37, const float* k,
+                                            int kind) {
+    const F2 P = mul2(d64, splat(k[0]));
+    const F2 Q = mul2(d82, splat(k[1]));
+    const F2 R = mul2(sub2(s46, c), splat(k[2]));
+    const F2 T = mul2(sub2(s28, c), splat(k[3]));
+    const F2 S = mul2(sub2(s19, s37), splat(k[4]));
+    const F2 p2 = mul2(P, P), q2 = mul2(Q, Q);
+    const F2 pq = mul2(P, Q);
+    const F2 pq2 = add_p(pq, pq);
+    const F2 one = splat(1.0f);
+    float v[2];
+    if (kind == 0) {
+        const F2 g = add_p(p2, q2);
+        const F2 w = add2(one, g);
+        const F2 num = add_p(add_p(mul2(p2, R), mul2(pq2, S)), mul2(q2, T));
+        const F2 den = mul2(w, pk(sqrt64of32(lo(w)), sqrt64of32(hi(w))));
+        const F2 r = sub2(splat(0.0f), pk(div(div(lo(num), lo(g)), lo(den)), div(div(hi(num), hi(g)), hi(den))));
+        v[0] = lo(g) == 0.0f ? add(lo(num), 0.0f) : lo(r);
+        v[1] = hi(g) == 0.0f ? add(hi(num), 0.0f) : hi(r);
+    } else if (kind == 1) {
+        const F2 g = add_p(p2, q2);
+        const F2 num = add_p(sub_p(mul2(q2, R), mul2(pq2, S)), mul2(p2, T));
+        const F2 r = sub2(splat(0.0f), pk(div(div(lo(num), lo(g)), sqrt64of32(lo(g))),
+                                          div(div(hi(num), hi(g)), sqrt64of32(hi(g)))));
+        v[0] = lo(g) == 0.0f ? add(lo(num), 0.0f) : lo(r);
+        v[1] = hi(g) == 0.0f ? add(hi(num), 0.0f) : hi(r);
+    } else {
+        const F2 w = add2(one, add_p(p2, q2));
+        const F2 num = add_p(sub_p(mul2(add_p(one, q2), R), mul2(pq2, S)), mul2(add_p(one, p2), T));
+        const F2 d = mul2(w, pk(sqrt64of32(lo(w)), sqrt64of32(hi(w))));
+        const F2 dd = add_p(d, d);
+        const F2 r = sub2(splat(0.0f), pk(div(lo(num), lo(dd)), div(hi(num), hi(dd))));
+        v[0] = lo(r);
+        v[1] = hi(r);
     }
     return pk(v[0], v[1]);
 }

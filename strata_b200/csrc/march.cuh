@@ -95,13 +95,29 @@ __device__ __forceinline__ void row_compute(const LaunchParams& P, const EpiTabl
         }
         // The epilogue maps NaN to itself, so the edge ring stays NaN.
         if constexpr (EPI) epilogue4(P, *T, o0);
+    } else if constexpr (OP == STRATA_OP_CURVATURE) {
+        // Pairs (0, 1) and (2, 3) again: the centre column's terms come
+        // packed from the rows, the terms of the shifted columns per cell.
+#pragma unroll
+        for (int p = 0; p < 2; p++) {
+            const int i = 2 * p, j = 2 * p + 1;
+            const F2 z2 = pk(a.v[i + 1], a.v[j + 1]), z5 = pk(b.v[i + 1], b.v[j + 1]);
+            const F2 z8 = pk(c.v[i + 1], c.v[j + 1]);
+            const F2 r = zt_curvature2(pk(sub(b.v[i + 2], b.v[i]), sub(b.v[j + 2], b.v[j])), sub2(z8, z2),
+                                       add2(z5, z5), pk(add(b.v[i], b.v[i + 2]), add(b.v[j], b.v[j + 2])),
+                                       add2(z2, z8), pk(add(a.v[i], c.v[i + 2]), add(a.v[j], c.v[j + 2])),
+                                       pk(add(a.v[i + 2], c.v[i]), add(a.v[j + 2], c.v[j])), P.k, KIND);
+            o0[i] = rowin && colin[i] ? lo(r) : nan;
+            o0[j] = rowin && colin[j] ? hi(r) : nan;
+        }
+        if constexpr (EPI) epilogue4(P, *T, o0);
     } else {
 #pragma unroll
         for (int i = 0; i < 4; i++) {
             const float z[9] = {a.v[i], a.v[i + 1], a.v[i + 2], b.v[i], b.v[i + 1],
                                 b.v[i + 2], c.v[i], c.v[i + 1], c.v[i + 2]};
             float r0 = nan, r1 = nan;
-            apply3<OP>(P, z, r0, r1);
+            apply3<OP, KIND>(P, z, r0, r1);
             o0[i] = (rowin && colin[i]) ? r0 : nan;
         }
         if constexpr (EPI) epilogue4(P, *T, o0);

@@ -474,8 +474,21 @@ int64_t launch_march_any(const LaunchParams& p, cudaStream_t s) {
     case STRATA_OP_ASPECT:
         return p.kind ? launch_any_epi<STRATA_OP_ASPECT, 1>(p, s) : launch_any_epi<STRATA_OP_ASPECT, 0>(p, s);
     case STRATA_OP_HILLSHADE: return launch_any_epi<STRATA_OP_HILLSHADE, 0>(p, s);
-    case STRATA_OP_CURVATURE: return launch_any_epi<STRATA_OP_CURVATURE, 0>(p, s);
-    case STRATA_OP_RUGGEDNESS: return launch_any_epi<STRATA_OP_RUGGEDNESS, 0>(p, s);
+    case STRATA_OP_CURVATURE:
+        switch (p.kind) {
+        case 0: return launch_any_epi<STRATA_OP_CURVATURE, 0>(p, s);
+        case 1: return launch_any_epi<STRATA_OP_CURVATURE, 1>(p, s);
+        case 2: return launch_any_epi<STRATA_OP_CURVATURE, 2>(p, s);
+        }
+        return -1;
+    case STRATA_OP_RUGGEDNESS:
+        switch (p.kind) {
+        case STRATA_RUG_TRI_RILEY: return launch_any_epi<STRATA_OP_RUGGEDNESS, kKindAtRun>(p, s);
+        case STRATA_RUG_TRI_WILSON: return launch_any_epi<STRATA_OP_RUGGEDNESS, STRATA_RUG_TRI_WILSON>(p, s);
+        case STRATA_RUG_TPI: return launch_any_epi<STRATA_OP_RUGGEDNESS, STRATA_RUG_TPI>(p, s);
+        case STRATA_RUG_ROUGHNESS: return launch_any_epi<STRATA_OP_RUGGEDNESS, STRATA_RUG_ROUGHNESS>(p, s);
+        }
+        return -1;
     case STRATA_OP_CORRELATE: return launch_any_epi<STRATA_OP_CORRELATE, 0>(p, s);
     case STRATA_OP_SEPARABLE: return launch_any_epi<STRATA_OP_SEPARABLE, 0>(p, s);
     case STRATA_OP_MEAN: return launch_any_epi<STRATA_OP_MEAN, 0>(p, s);
@@ -493,8 +506,21 @@ int64_t launch_march3(const LaunchParams& p, cudaStream_t s) {
     case STRATA_OP_ASPECT:
         return p.kind ? launch_epi<STRATA_OP_ASPECT, 1>(p, s) : launch_epi<STRATA_OP_ASPECT, 0>(p, s);
     case STRATA_OP_HILLSHADE: return launch_epi<STRATA_OP_HILLSHADE, 0>(p, s);
-    case STRATA_OP_CURVATURE: return launch_epi<STRATA_OP_CURVATURE, 0>(p, s);
-    case STRATA_OP_RUGGEDNESS: return launch_epi<STRATA_OP_RUGGEDNESS, 0>(p, s);
+    case STRATA_OP_CURVATURE:
+        switch (p.kind) {
+        case 0: return launch_epi<STRATA_OP_CURVATURE, 0>(p, s);
+        case 1: return launch_epi<STRATA_OP_CURVATURE, 1>(p, s);
+        case 2: return launch_epi<STRATA_OP_CURVATURE, 2>(p, s);
+        }
+        return -1;
+    case STRATA_OP_RUGGEDNESS:
+        switch (p.kind) {
+        case STRATA_RUG_TRI_RILEY: return launch_epi<STRATA_OP_RUGGEDNESS, kKindAtRun>(p, s);
+        case STRATA_RUG_TRI_WILSON: return launch_epi<STRATA_OP_RUGGEDNESS, STRATA_RUG_TRI_WILSON>(p, s);
+        case STRATA_RUG_TPI: return launch_epi<STRATA_OP_RUGGEDNESS, STRATA_RUG_TPI>(p, s);
+        case STRATA_RUG_ROUGHNESS: return launch_epi<STRATA_OP_RUGGEDNESS, STRATA_RUG_ROUGHNESS>(p, s);
+        }
+        return -1;
     case STRATA_OP_CORRELATE: return launch_epi<STRATA_OP_CORRELATE, 0>(p, s);
     case STRATA_OP_SEPARABLE: return launch_epi<STRATA_OP_SEPARABLE, 0>(p, s);
     case STRATA_OP_MEAN: return launch_epi<STRATA_OP_MEAN, 0>(p, s);

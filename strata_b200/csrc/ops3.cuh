@@ -14,13 +14,20 @@
 
 namespace strata {
 
-template <int OP>
+// KIND: the op's kind, fixed per kernel (Curvature's type, Ruggedness's
+// measure), so each kernel carries one kind's arithmetic; kKindAtRun reads
+// it from the launch instead (Riley's TRI: its float64 sums over a lane's
+// four cells, scheduled side by side in a kernel of its own, outgrow the
+// register budget).
+constexpr int kKindAtRun = -1;
+
+template <int OP, int KIND>
 __device__ __forceinline__ void apply3(const LaunchParams& P, const float (&z)[9], float& o0, float& o1) {
     using namespace cell;
     if constexpr (OP == STRATA_OP_CURVATURE) {
-        o0 = zt_curvature(z[0], z[1], z[2], z[3], z[4], z[5], z[6], z[7], z[8], P.k, P.kind);
+        o0 = zt_curvature(z[0], z[1], z[2], z[3], z[4], z[5], z[6], z[7], z[8], P.k, KIND);
     } else if constexpr (OP == STRATA_OP_RUGGEDNESS) {
-        o0 = rugged3(z[0], z[1], z[2], z[3], z[4], z[5], z[6], z[7], z[8], P.kind);
+        o0 = rugged3(z[0], z[1], z[2], z[3], z[4], z[5], z[6], z[7], z[8], KIND == kKindAtRun ? P.kind : KIND);
     } else if constexpr (OP == STRATA_OP_CORRELATE) {
         float acc = mul(P.w[0], z[0]);
 #pragma unroll
