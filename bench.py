@@ -562,7 +562,8 @@ def run_serve(args, rank, world, local_rank):
                         w, h))
         return out
 
-    srv = serve.Server(mosaic, budget_bytes=120 << 30, streams=4, max_batch=64, device=local_rank)
+    srv = serve.Server(mosaic, budget_bytes=120 << 30, streams=4, max_batch=64, device=local_rank,
+                       band=args.band or 0)
 
     def burst(reqs):
         """All at once (closed loop, the requests submitted, waited for and
@@ -636,7 +637,7 @@ def run_serve(args, rank, world, local_rank):
         "config": {"workload": "40000x40000 resident DEM mosaic (fBm tile mirrored and tiled, 2% NoData 8x8 blocks), "
                                "windows with sides log-uniform 256..4096 at uniform origins, "
                                "ops Slope/Aspect/Hillshade/Mean r5/TPI", "requests_per_step": per_step,
-                   "budget_bytes": 120 << 30, "streams": 4, "max_batch": 64,
+                   "budget_bytes": 120 << 30, "streams": 4, "max_batch": 64, "band": args.band or "default",
                    "timing": "host wall clock (the serving path is asynchronous)",
                    "closed_loop": "value: each step's requests submitted, waited for and released as one group"},
         "latency_ms": {"offered_load": "Poisson arrivals at 60% of the closed-loop capacity",
@@ -689,6 +690,7 @@ def main():
     ap.add_argument("--tune-cache", action="store_true", help="keep the batch autotuner's choices in a file")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--side", type=int, default=None, help="raster side override (profiling captures)")
+    ap.add_argument("--band", type=int, default=None, help="serving: rows per unit of the radius-1 batch kernels")
     ap.add_argument("--ops", default=None, help="comma-separated ops of the workload to keep (profiling captures)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -301,6 +301,8 @@ typedef struct {
     int64_t budget_bytes; /* 0 = 120 GiB */
     int32_t streams;      /* 0 = 4 */
     int32_t max_batch;    /* 0 = 64 */
+    int32_t band;         /* rows per work unit of the radius-1 batch kernels, 1..256; 0 = 16 */
+    int32_t reserved;
 } strata_server_opts;
 
 typedef struct {

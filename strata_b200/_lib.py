@@ -67,7 +67,8 @@ class BatchItem(ctypes.Structure):
 
 
 class ServerOpts(ctypes.Structure):
-    _fields_ = [("budget_bytes", c_i64), ("streams", c_i32), ("max_batch", c_i32)]
+    _fields_ = [("budget_bytes", c_i64), ("streams", c_i32), ("max_batch", c_i32), ("band", c_i32),
+                ("reserved", c_i32)]
 
 
 class ServerResult(ctypes.Structure):

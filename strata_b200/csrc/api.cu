@@ -2002,6 +2002,7 @@ struct strata_server {
     DevOperand dm;
     size_t budget = 0, used = 0;
     int max_batch = 64;
+    int band = 16;  // rows per unit of the radius-1 batch kernels
     std::vector<Slot> slots;
     std::mutex mu;
     std::condition_variable cv;       // the scheduler waits here
@@ -2029,6 +2030,7 @@ int launch_batch(strata_server* S, Slot& s) {
         strata::BatchItem& b = s.h_items[i];
         memset(&b, 0, sizeof b);
         b.p = r->p;
+        if (r->p.radius <= 1) b.th = S->band;
         for (int k = 0; k < r->nout; k++) {
             if (!r->out_bits[k]) continue;
             ValidityParams& v = b.v[b.nvalid++];
@@ -2174,6 +2176,11 @@ extern "C" int strata_server_create(strata_ctx* c, const strata_raster* mosaic, 
     S->mosaic = *mosaic;
     S->budget = o && o->budget_bytes ? (size_t)o->budget_bytes : (size_t)120 << 30;
     S->max_batch = o && o->max_batch > 0 ? o->max_batch : 64;
+    if (o && (o->band < 0 || o->band > 256)) {
+        delete S;
+        return fail(STRATA_EINVAL, "engine: server band %d (1 to 256, 0 for the default)", o->band);
+    }
+    S->band = o && o->band > 0 ? o->band : 16;
     const int nstreams = o && o->streams > 0 ? o->streams : 4;
     cudaSetDevice(c->device);
     cudaDeviceGetAttribute(&S->sms, cudaDevAttrMultiProcessorCount, c->device);

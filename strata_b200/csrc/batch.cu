@@ -36,8 +36,10 @@ void batch_focal_shape(int op, int radius, int kind, int band, int* tw, int* th)
 
 namespace {
 
+// Five blocks per SM: 96 registers a thread, which every class fits without
+// spilling (at six, 80, the Horn and curvature classes spill).
 template <int OP, int KIND, bool EPI>
-__global__ void __launch_bounds__(kBatchThreads) batch_march_kernel(const BatchItem* __restrict__ items, int n,
+__global__ void __launch_bounds__(kBatchThreads, 5) batch_march_kernel(const BatchItem* __restrict__ items, int n,
                                                                     int64_t total) {
     __shared__ __align__(16) LaunchParams P;
     EpiTables* T = EpiSmem<EPI>::get();

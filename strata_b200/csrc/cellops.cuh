@@ -256,7 +256,9 @@ __device__ __forceinline__ F2 slope2(F2 gx, F2 gy, F2 scale, bool take_atan) {
     return mul2(take_atan ? atan32x2(m) : m, scale);
 }
 
-// aspect over a pair of gradients (atan2f32's steps inline).
+// aspect over a pair of gradients, atan2f32's steps inline. Its fix-up
+// for two zero arguments is left out: when it applies, y and x are both
+// zero and aspect's last step replaces the angle by the flat value.
 __device__ __forceinline__ F2 aspect2(F2 gx, F2 gy, float flat, bool trig) {
     const F2 ngx = pk(sub(0.0f, lo(gx)), sub(0.0f, hi(gx)));
     const F2 y = trig ? gy : ngx, x = trig ? ngx : gy;
@@ -268,19 +270,12 @@ __device__ __forceinline__ F2 aspect2(F2 gx, F2 gy, float flat, bool trig) {
         ay[h] = abs32(ys[h]);
     }
     const F2 at = atan32x2(pk(div(ay[0], ax[0]), div(ay[1], ax[1])));
-    const F2 flip = sub2(splat(kPi), at);
-    const float ats[2] = {lo(at), hi(at)}, flips[2] = {lo(flip), hi(flip)};
+    const float ats[2] = {lo(at), hi(at)};
     float a[2];
 #pragma unroll
     for (int h = 0; h < 2; h++) {
-        float v = ats[h];
-        if (ay[h] == 0.0f && ax[h] == 0.0f) v = 0.0f;
-        if (ay[h] == ax[h] && ay[h] > 0x1.fffffep+127f) v = kPi4;
-        // sub(kPi, v) for the special values above is their own pair entry
-        float f = flips[h];
-        if (ay[h] == 0.0f && ax[h] == 0.0f) f = kPi;
-        if (ay[h] == ax[h] && ay[h] > 0x1.fffffep+127f) f = sub(kPi, kPi4);
-        if (__float_as_uint(xs[h]) & 0x80000000u) v = f;
+        float v = ay[h] == ax[h] && ay[h] > 0x1.fffffep+127f ? kPi4 : ats[h];
+        if (__float_as_uint(xs[h]) & 0x80000000u) v = sub(kPi, v);
         a[h] = __uint_as_float(__float_as_uint(v) | (__float_as_uint(ys[h]) & 0x80000000u));
     }
     F2 d = mul2(pk(a[0], a[1]), splat(kRadToDeg));

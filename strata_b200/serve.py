@@ -58,10 +58,10 @@ def _device_view(ptr: int, n: int, typestr: str):
 
 class Server:
     def __init__(self, mosaic: Float32Raster, budget_bytes: int = 0, streams: int = 0, max_batch: int = 0,
-                 device: int = 0):
+                 device: int = 0, band: int = 0):
         self.mosaic = mosaic  # keeps the device buffers alive
         c = engine.device_context(device)
-        o = _lib.ServerOpts(budget_bytes, streams, max_batch)
+        o = _lib.ServerOpts(budget_bytes, streams, max_batch, band, 0)
         p = ctypes.c_void_p()
         _lib.check(_lib.lib().strata_server_create(c, ctypes.byref(engine.c_raster(mosaic)), ctypes.byref(o),
                                                    ctypes.byref(p)))

@@ -223,6 +223,34 @@ def test_folded_pointwise_tail_edges(seed):
         f"slope+tail seed={seed}")
 
 
+@pytest.mark.parametrize("trig", [False, True])
+def test_aspect_special_gradients(trig):
+    """Aspect where the gradient is zero (flat patches: the flat value),
+    where both components overflow to infinity (huge steps: atan2's pi/4
+    case, in every quadrant) or one does, and on ±0 and NaN cells, equal to
+    the oracle bit for bit."""
+    w, h = 96, 64
+    rng = np.random.default_rng(7 + trig)
+    dem = (rng.standard_normal((h, w)) * 50 + 500).astype(np.float32)
+    dem[5:15, 5:30] = np.float32(250.0)  # flat
+    dem[20:24, 40:44] = np.float32(-0.0)
+    dem[20:24, 44:48] = np.float32(0.0)
+    big = np.float32(3e38)
+    for k, (sy, sx) in enumerate([(1, 1), (1, -1), (-1, 1), (-1, -1)]):
+        y0, x0 = 30 + 8 * (k // 2), 8 + 20 * (k % 2)
+        block = np.zeros((5, 5), np.float32)
+        block += np.arange(5, dtype=np.float32)[None, :] * (sx * big)
+        block += np.arange(5, dtype=np.float32)[:, None] * (sy * big)
+        dem[y0:y0 + 5, x0:x0 + 5] = np.nan_to_num(block, posinf=np.inf, neginf=-np.inf)
+    dem[50:55, 60:65] = np.arange(5, dtype=np.float32)[None, :] * big  # x only
+    dem[3, 70] = np.nan
+    make = lambda: terrain.aspect_stage(terrain.AspectOptions(CellSize=10, ZeroForFlat=not trig,
+                                                              Trigonometric=trig))
+    for masked, device in itertools.product((False, True), (False, True)):
+        for li, lay in enumerate(layouts(w, h, 3, masked)):
+            check_case(make(), dem, 1, device, lay, f"trig={trig} masked={masked} device={device} layout={li}")
+
+
 @pytest.mark.parametrize("nb", [0, 1, 2, 4, 7, 8, 9, 20])
 def test_stencil_reclass_on_output_values(nb):
     """A lone Reclass after a stencil, with breaks drawn from the stencil's
