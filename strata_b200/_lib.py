@@ -10,6 +10,8 @@ import ctypes
 import os
 import threading
 
+import numpy as np
+
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libstrata_cuda.so")
 
@@ -76,9 +78,24 @@ class ServerResult(ctypes.Structure):
                 ("t_start_ns", c_i64), ("t_done_ns", c_i64)]
 
 
+# The same layouts as numpy dtypes, for filling and reading many at once
+# (pointers as unsigned 64-bit integers).
+RASTER_DTYPE = np.dtype([("data", "<u8"), ("width", "<i8"), ("height", "<i8"), ("stride", "<i8"), ("valid", "<u8"),
+                         ("valid_offset", "<i8"), ("on_device", "<i4"), ("reserved", "<i4")])
+SERVER_RESULT_DTYPE = np.dtype([("status", "<i4"), ("nout", "<i4"), ("out", RASTER_DTYPE, (2,)),
+                                ("t_submit_ns", "<i8"), ("t_start_ns", "<i8"), ("t_done_ns", "<i8")])
+SERVER_REQUEST_DTYPE = np.dtype([("stages", "<u8"), ("nstages", "<i4"), ("reserved", "<i4"), ("x", "<i8"),
+                                 ("y", "<i8"), ("w", "<i8"), ("h", "<i8")])
+
+
 class ServerRequest(ctypes.Structure):
     _fields_ = [("stages", ctypes.POINTER(Stage)), ("nstages", c_i32), ("reserved", c_i32), ("x", c_i64),
                 ("y", c_i64), ("w", c_i64), ("h", c_i64)]
+
+
+assert RASTER_DTYPE.itemsize == ctypes.sizeof(Raster)
+assert SERVER_RESULT_DTYPE.itemsize == ctypes.sizeof(ServerResult)
+assert SERVER_REQUEST_DTYPE.itemsize == ctypes.sizeof(ServerRequest)
 
 
 class GradientOptions(ctypes.Structure):

@@ -1975,6 +1975,7 @@ struct Request {
     LaunchParams p;
     int nout = 0;
     int status = 1;  // 1 queued, 2 running, 0 done, < 0 failed
+    void* block = nullptr;  // one pool allocation holding the outputs below
     float* out[2] = {nullptr, nullptr};
     uint32_t* out_bits[2] = {nullptr, nullptr};
     size_t bytes = 0;  // budget charge
@@ -2008,6 +2009,7 @@ struct strata_server {
     std::condition_variable cv;       // the scheduler waits here
     std::condition_variable done_cv;  // callers waiting for results
     std::deque<Request*> queue;
+    std::vector<void*> to_free;  // released requests' allocations, freed by the scheduler
     std::unordered_map<uint64_t, Request*> all;
     uint64_t next_ticket = 1;
     bool stop = false;
@@ -2082,8 +2084,18 @@ constexpr int64_t kCoalesceNs = 100000;  // how long a short queue waits for com
 void scheduler(strata_server* S) {
     cudaSetDevice(S->ctx->device);
     std::unique_lock<std::mutex> lk(S->mu);
+    std::vector<void*> frees;
     while (!S->stop) {
         bool progressed = false;
+        // Return released allocations to the pool, without the lock.
+        if (!S->to_free.empty()) {
+            frees.swap(S->to_free);
+            lk.unlock();
+            for (void* p : frees) cudaFreeAsync(p, S->ctx->stream);
+            frees.clear();
+            lk.lock();
+            progressed = true;
+        }
         // Retire finished batches.
         for (Slot& s : S->slots) {
             if (!s.busy) continue;
@@ -2114,18 +2126,21 @@ void scheduler(strata_server* S) {
             while (!S->queue.empty() && (int)s.reqs.size() < S->max_batch) {
                 Request* r = S->queue.front();
                 if (S->used + r->bytes > S->budget && !(S->used == 0 && s.reqs.empty())) break;
-                // Outputs from the stream-ordered pool.
-                bool ok = true;
-                for (int k = 0; k < r->nout && ok; k++) {
-                    ok = cudaMallocFromPoolAsync((void**)&r->out[k], (size_t)(r->w * r->h) * 4, S->pool, s.stream) ==
-                         cudaSuccess;
-                    if (ok && S->mosaic.valid)
-                        ok = cudaMallocFromPoolAsync((void**)&r->out_bits[k], (size_t)((r->w * r->h + 63) / 64) * 8,
-                                                     S->pool, s.stream) == cudaSuccess;
-                }
-                if (!ok) {
+                // Outputs and their validity words from the stream-ordered
+                // pool, in one allocation (one call to allocate and one to
+                // free per request), each part on a 256-byte boundary.
+                const size_t data_bytes = ((size_t)(r->w * r->h) * 4 + 255) & ~(size_t)255;
+                const size_t bit_bytes = S->mosaic.valid ? ((size_t)((r->w * r->h + 63) / 64) * 8 + 255) & ~(size_t)255 : 0;
+                if (cudaMallocFromPoolAsync(&r->block, (data_bytes + bit_bytes) * (size_t)r->nout, S->pool, s.stream) !=
+                    cudaSuccess) {
+                    r->block = nullptr;
                     cudaGetLastError();
                     break;
+                }
+                for (int k = 0; k < r->nout; k++) {
+                    char* base = static_cast<char*>(r->block) + (data_bytes + bit_bytes) * (size_t)k;
+                    r->out[k] = reinterpret_cast<float*>(base);
+                    if (S->mosaic.valid) r->out_bits[k] = reinterpret_cast<uint32_t*>(base + data_bytes);
                 }
                 S->queue.pop_front();
                 S->used += r->bytes;
@@ -2256,7 +2271,11 @@ Request* prepare_request(strata_server* S, const strata_stage* stages, int nstag
     p.out_x1 = w;
     p.out_y1 = h;
     p.status = S->ctx->d_status;
-    r->bytes = (size_t)(w * h) * 4 * (size_t)r->nout + (M.valid ? (size_t)((w * h + 63) / 64) * 8 * r->nout : 0);
+    // The charge is the request's allocation: each output's cells and its
+    // validity words, each rounded up to 256 bytes.
+    const size_t data_bytes = ((size_t)(w * h) * 4 + 255) & ~(size_t)255;
+    const size_t bit_bytes = M.valid ? ((size_t)((w * h + 63) / 64) * 8 + 255) & ~(size_t)255 : 0;
+    r->bytes = (data_bytes + bit_bytes) * (size_t)r->nout;
     *rc_out = STRATA_OK;
     return r;
 }
@@ -2276,9 +2295,10 @@ int release_locked(strata_server* S, uint64_t ticket) {
     if (it == S->all.end()) return fail(STRATA_EINVAL, "engine: unknown ticket %llu", (unsigned long long)ticket);
     Request* r = it->second;
     if (r->status > 0) return fail(STRATA_EINVAL, "engine: request %llu is still running", (unsigned long long)ticket);
-    for (int k = 0; k < 2; k++) {
-        if (r->out[k]) cudaFreeAsync(r->out[k], S->ctx->stream);
-        if (r->out_bits[k]) cudaFreeAsync(r->out_bits[k], S->ctx->stream);
+    // The scheduler returns the allocation to the pool, off the caller's path.
+    if (r->block) {
+        S->to_free.push_back(r->block);
+        S->cv.notify_one();
     }
     if (r->t_start) S->used -= r->bytes;
     S->all.erase(it);
@@ -2413,12 +2433,10 @@ extern "C" void strata_server_destroy(strata_server* S) {
         if (s.stream) cudaStreamDestroy(s.stream);
     }
     cudaStreamSynchronize(S->ctx->stream);
+    for (void* p : S->to_free) cudaFree(p);
     for (auto& kv : S->all) {
         Request* r = kv.second;
-        for (int k = 0; k < 2; k++) {
-            if (r->out[k]) cudaFree(r->out[k]);
-            if (r->out_bits[k]) cudaFree(r->out_bits[k]);
-        }
+        if (r->block) cudaFree(r->block);
         delete r;
     }
     delete S;

@@ -152,19 +152,30 @@ class StageList:
     def __init__(self):
         self.stages: List[_lib.Stage] = []
         self.keep: list = []
+        self._c = None
 
     def add(self, st: _lib.Stage, *arrays) -> "StageList":
         self.stages.append(st)
         self.keep.extend(arrays)
+        self._c = None
         return self
 
     def extend(self, other: "StageList") -> "StageList":
         self.stages.extend(other.stages)
         self.keep.extend(other.keep)
+        self._c = None
         return self
 
     def c_array(self):
         return (_lib.Stage * len(self.stages))(*self.stages)
+
+    def c_address(self) -> int:
+        """The address of the stages as a C array, built once and kept with
+        the list until stages are added (for calls that pass many lists)."""
+        if self._c is None:
+            arr = self.c_array()
+            self._c = (arr, ctypes.addressof(arr))
+        return self._c[1]
 
 
 def _stats_out(opts: Optional[Options], cst: _lib.Stats) -> None:

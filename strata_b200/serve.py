@@ -17,21 +17,36 @@ is the one strata_process gives for the window view.
 from __future__ import annotations
 
 import ctypes
-from dataclasses import dataclass
 from typing import List, Optional, Sequence
 
-
+import numpy as np
 
 from . import _lib, engine
 from .raster import Float32Raster
 
 
-@dataclass
 class Result:
-    outputs: List[Float32Raster]  # device rasters owned by the server until release
-    t_submit_ns: int
-    t_start_ns: int
-    t_done_ns: int
+    """A request's outputs (device rasters the server owns until release)
+    and its submit / start / done times (steady clock, ns). The outputs of
+    a result from wait_many are built on first use from the columns of the
+    whole call's result table (cols, row)."""
+
+    __slots__ = ("_outputs", "_cols", "t_submit_ns", "t_start_ns", "t_done_ns")
+
+    def __init__(self, outputs: Optional[List[Float32Raster]], t_submit_ns: int, t_start_ns: int, t_done_ns: int,
+                 cols=None):
+        self._outputs = outputs
+        self._cols = cols
+        self.t_submit_ns, self.t_start_ns, self.t_done_ns = t_submit_ns, t_start_ns, t_done_ns
+
+    @property
+    def outputs(self) -> List[Float32Raster]:
+        if self._outputs is None:
+            (nout, data, width, height, stride, valid), i = self._cols
+            self._outputs = [Float32Raster(data[i][k], width[i][k], height[i][k], stride[i][k], valid[i][k] or None, 0)
+                             for k in range(nout[i])]
+            self._cols = None
+        return self._outputs
 
     @property
     def latency_ms(self) -> float:
@@ -79,29 +94,35 @@ class Server:
         invalid."""
         requests = list(requests)
         n = len(requests)
-        arr = (_lib.ServerRequest * n)()
-        keep = []
-        for i, (stages, x, y, w, h) in enumerate(requests):
-            st = stages.c_array()
-            keep.append(st)
-            arr[i].stages = ctypes.cast(st, ctypes.POINTER(_lib.Stage))
-            arr[i].nstages = len(stages.stages)
-            arr[i].x, arr[i].y, arr[i].w, arr[i].h = x, y, w, h
-        t = (ctypes.c_uint64 * n)()
-        _lib.check(_lib.lib().strata_server_submit_many(self._h, arr, n, t))
-        return list(t)
+        req = np.zeros(n, _lib.SERVER_REQUEST_DTYPE)
+        if n:
+            req["stages"] = [r[0].c_address() for r in requests]
+            req["nstages"] = [len(r[0].stages) for r in requests]
+            xywh = np.array([r[1:5] for r in requests], dtype=np.int64)
+            req["x"], req["y"], req["w"], req["h"] = xywh[:, 0], xywh[:, 1], xywh[:, 2], xywh[:, 3]
+        t = np.zeros(n, np.uint64)
+        _lib.check(_lib.lib().strata_server_submit_many(self._h, req.ctypes.data_as(ctypes.POINTER(_lib.ServerRequest)),
+                                                        n, t.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))))
+        return t.tolist()
 
     def wait_many(self, tickets: Sequence[int], timeout_ms: int = -1) -> List[Result]:
         """Waits for every ticket, in order; their results."""
         n = len(tickets)
-        t = (ctypes.c_uint64 * n)(*tickets)
-        res = (_lib.ServerResult * n)()
-        _lib.check(_lib.lib().strata_server_wait_many(self._h, t, n, timeout_ms, res))
-        return [self._result(res[i]) for i in range(n)]
+        t = np.ascontiguousarray(tickets, dtype=np.uint64)
+        res = np.zeros(n, _lib.SERVER_RESULT_DTYPE)
+        _lib.check(_lib.lib().strata_server_wait_many(self._h, t.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), n,
+                                                      timeout_ms, res.ctypes.data_as(
+                                                          ctypes.POINTER(_lib.ServerResult))))
+        out = res["out"]
+        cols = (res["nout"].tolist(), out["data"].tolist(), out["width"].tolist(), out["height"].tolist(),
+                out["stride"].tolist(), out["valid"].tolist())
+        ts, tb, td = res["t_submit_ns"].tolist(), res["t_start_ns"].tolist(), res["t_done_ns"].tolist()
+        return [Result(None, ts[i], tb[i], td[i], (cols, i)) for i in range(n)]
 
     def release_many(self, tickets: Sequence[int]) -> None:
         n = len(tickets)
-        _lib.check(_lib.lib().strata_server_release_many(self._h, (ctypes.c_uint64 * n)(*tickets), n))
+        t = np.ascontiguousarray(tickets, dtype=np.uint64)
+        _lib.check(_lib.lib().strata_server_release_many(self._h, t.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), n))
 
     @staticmethod
     def _result(r) -> Result:
