@@ -194,6 +194,45 @@ constexpr int kSepUnroll = R >= 5 ? 4 : 2 * R + 1;
 template <int R>
 constexpr int kSepRing = kSepUnroll<R> == 2 * R + 1 ? 2 * R + 1 : 2 * R + kSepUnroll<R>;
 
+// Min and Max folds (Go's min/max: NaN wins, -0 below +0, as PTX min.NaN /
+// max.NaN) are exactly associative and commutative, so any grouping of a
+// window's terms gives the reference's bits. Their folds share work between
+// neighbouring windows: the four output rows of a 4-row step share window
+// rows 3 .. 2R, and a thread's four outputs share column results 3 .. 2R
+// of their windows, so each such core is folded once and every window adds
+// its own three edge terms (25 operations for four windows at R = 8, where
+// four separate folds take 64).
+template <int FOLD>
+constexpr bool kMinMax = FOLD == STRATA_OP_MIN || FOLD == STRATA_OP_MAX;
+
+template <int FOLD>
+__device__ __forceinline__ float minmax(float a, float b) {
+    if constexpr (FOLD == STRATA_OP_MIN) return go_min(a, b);
+    else return go_max(a, b);
+}
+
+// The core of a 4-row step's column folds (ring slots 3 .. 2R, the step's
+// first output row at slot 0).
+template <int FOLD, int R, int RS>
+__device__ __forceinline__ float col_core(const float (&ring)[RS][4], int i) {
+    float a = ring[3][i];
+#pragma unroll
+    for (int k = 4; k <= 2 * R; k++) a = minmax<FOLD>(a, ring[k][i]);
+    return a;
+}
+
+// Output row u's column fold from the core: its rows u .. 2 before the
+// core and 2R+1 .. 2R+u after it.
+template <int FOLD, int R, int RS>
+__device__ __forceinline__ float col_from_core(const float (&ring)[RS][4], int i, int u, float core) {
+    float a = core;
+#pragma unroll
+    for (int k = u; k <= 2; k++) a = minmax<FOLD>(a, ring[k][i]);
+#pragma unroll
+    for (int k = 2 * R + 1; k <= 2 * R + u; k++) a = minmax<FOLD>(a, ring[k][i]);
+    return a;
+}
+
 // Term c (0 .. 2R) of a fold across column results, left to right: the
 // first term starts the fold.
 template <int FOLD>
@@ -259,6 +298,12 @@ __device__ __forceinline__ void sep_body(const LaunchParams& P, int64_t X0, int6
     const bool writer = tid < OW / 4 && X0 + 4 * tid < P.out_x1;
     OutWalk dst(P, X0 + 4 * tid, y0, R, vec);
     int buf = 0;
+    // Min/Max column folds through a core shared by the 4-row step (the
+    // ring holds the step's 2R + 4 rows).
+    constexpr bool kCoreRows = kMinMax<F0> && U == 4 && RS == 2 * R + 4;
+    float core0[4], core1[4];
+    (void)core0;
+    (void)core1;
     for (int yb = 0; yb < rows; yb += U) {
 #pragma unroll
         for (int u = 0; u < U; u++) {
@@ -273,16 +318,77 @@ __device__ __forceinline__ void sep_body(const LaunchParams& P, int64_t X0, int6
                 slot[3] = v.w;
             }
             float c0[4], c1[4];
+            if constexpr (kCoreRows) {
+                // the core is complete once row 2R (slot 2R) has landed
+                if (u == 0) {
 #pragma unroll
-            for (int i = 0; i < 4; i++) {
-                c0[i] = col_fold<F0, R, RS>(P, ring, i, u);
-                if constexpr (NF == 2) c1[i] = col_fold<F1, R, RS>(P, ring, i, u);
+                    for (int i = 0; i < 4; i++) {
+                        core0[i] = col_core<F0, R, RS>(ring, i);
+                        if constexpr (NF == 2) core1[i] = col_core<F1, R, RS>(ring, i);
+                    }
+                }
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    c0[i] = col_from_core<F0, R, RS>(ring, i, u, core0[i]);
+                    if constexpr (NF == 2) c1[i] = col_from_core<F1, R, RS>(ring, i, u, core1[i]);
+                }
+            } else {
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    c0[i] = col_fold<F0, R, RS>(P, ring, i, u);
+                    if constexpr (NF == 2) c1[i] = col_fold<F1, R, RS>(P, ring, i, u);
+                }
             }
             *reinterpret_cast<float4*>(&tb[buf][0][4 * tid]) = make_float4(c0[0], c0[1], c0[2], c0[3]);
             if constexpr (NF == 2)
                 *reinterpret_cast<float4*>(&tb[buf][NF - 1][4 * tid]) = make_float4(c1[0], c1[1], c1[2], c1[3]);
             __syncthreads();
-            if (writer) {
+            if (writer && kMinMax<F0>) {
+                // Min/Max: output i's window is column results B+i ..
+                // B+i+2R; results B+3 .. B+2R are common to the four, the
+                // rest (B .. B+2 before, B+2R+1 .. B+2R+3 after) are kept
+                // apart and added per output.
+                constexpr int B = HL - R;
+                float core[2], lo[2][3], hi[2][3];
+#pragma unroll
+                for (int q = 0; q < NT / 4; q++) {
+                    const float4 f0 = *reinterpret_cast<const float4*>(&tb[buf][0][4 * tid + 4 * q]);
+                    float4 f1 = f0;
+                    if constexpr (NF == 2) f1 = *reinterpret_cast<const float4*>(&tb[buf][NF - 1][4 * tid + 4 * q]);
+                    const float v[2][4] = {{f0.x, f0.y, f0.z, f0.w}, {f1.x, f1.y, f1.z, f1.w}};
+#pragma unroll
+                    for (int e = 0; e < 4; e++) {
+                        const int t = 4 * q + e;
+#pragma unroll
+                        for (int f = 0; f < NF; f++) {
+                            if (t < B || t > B + 2 * R + 3) continue;
+                            if (t <= B + 2) lo[f][t - B] = v[f][e];
+                            else if (t > B + 2 * R) hi[f][t - B - 2 * R - 1] = v[f][e];
+                            else if (t == B + 3) core[f] = v[f][e];
+                            else core[f] = f == 0 ? minmax<F0>(core[f], v[f][e]) : minmax<F1>(core[f], v[f][e]);
+                        }
+                    }
+                }
+                float o[4];
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    float a = core[0];
+#pragma unroll
+                    for (int k = i; k <= 2; k++) a = minmax<F0>(a, lo[0][k]);
+#pragma unroll
+                    for (int k = 0; k < i; k++) a = minmax<F0>(a, hi[0][k]);
+                    if constexpr (NF == 2) {
+                        float b = core[1];
+#pragma unroll
+                        for (int k = i; k <= 2; k++) b = minmax<F1>(b, lo[1][k]);
+#pragma unroll
+                        for (int k = 0; k < i; k++) b = minmax<F1>(b, hi[1][k]);
+                        a = sub(a, b);
+                    }
+                    o[i] = a;
+                }
+                dst.put(P, o);
+            } else if (writer) {
                 // Stream the column results left to right; each feeds the
                 // outputs whose windows hold it, so every output folds its
                 // 2R+1 terms in order with only its accumulator live.
