@@ -75,6 +75,29 @@ def test_served_equals_alone(budget):
     srv.close()
 
 
+@pytest.mark.parametrize("band", [1, 7, 64])
+def test_band_option(band):
+    """The server's unit band only changes how radius-1 requests are cut
+    into work units: every result equals the window alone at any band, and
+    bands outside 0..256 are refused."""
+    from strata_b200.raster import StrataPanic
+
+    W, H = 700, 600
+    m = to_device(_mosaic(W, H))
+    for bad in (-1, 257):
+        with pytest.raises(StrataPanic):
+            serve.Server(m, band=bad)
+    srv = serve.Server(m, band=band, streams=2, max_batch=8)
+    reqs = _requests(np.random.default_rng(40 + band), W, H, 20)
+    tickets = srv.submit_many([(OPS[o](), x, y, w, h) for o, x, y, w, h in reqs])
+    for res, (op, x, y, w, h) in zip(srv.wait_many(tickets, timeout_ms=60000), reqs):
+        assert_same_raster(to_host(res.copy()), _alone(m, op, x, y, w, h),
+                           f"band={band} op={op} at ({x}, {y}) {w}x{h}")
+    srv.release_many(tickets)
+    assert srv.stats()["used_bytes"] == 0
+    srv.close()
+
+
 def test_unmasked_mosaic_and_bad_window():
     W, H = 300, 200
     m = to_device(_mosaic(W, H, masked=False))
