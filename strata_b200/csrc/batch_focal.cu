@@ -13,7 +13,7 @@ template <int OP, int R>
 __global__ void __launch_bounds__(kSepThreads, (OP == STRATA_OP_SEPARABLE || OP == STRATA_OP_RUGGEDNESS) && R >= 6 ? 3 : 4)
     batch_sep_kernel(const BatchItem* __restrict__ items, int n, int64_t total) {
     __shared__ __align__(16) LaunchParams P;
-    __shared__ __align__(16) SepSmem<OP> sm;
+    __shared__ __align__(16) SepSmem<OP, R> sm;
     int cur = -1;
     for (int64_t u = blockIdx.x; u < total; u += gridDim.x) {
         const int it = batch_item_of(items, n, u);

@@ -36,7 +36,7 @@ namespace {
 template <int OP, int R>
 __global__ void __launch_bounds__(kSepThreads, (OP == STRATA_OP_SEPARABLE || OP == STRATA_OP_RUGGEDNESS) && R >= 6 ? 3 : 4)
     sep_march_kernel(const __grid_constant__ LaunchParams P, int colblocks, int strip, int vec) {
-    __shared__ __align__(16) SepSmem<OP> sm;
+    __shared__ __align__(16) SepSmem<OP, R> sm;
     const int cb = (int)(blockIdx.x % (unsigned)colblocks);
     const int sb = (int)(blockIdx.x / (unsigned)colblocks);
     const int64_t X0 = P.out_x0 + (int64_t)cb * kSepOut<R>;

@@ -251,11 +251,18 @@ __device__ __forceinline__ float fold_term(const LaunchParams& P, float a, float
 template <int OP>
 constexpr int kSepFolds = OP == STRATA_OP_RUGGEDNESS ? 2 : 1;
 
+// Rows of column results a block stores between two barriers: the whole
+// 4-row step where the loop body covers 4 rows and the op has one fold
+// (its four row folds then follow one barrier; roughness's two folds would
+// outgrow the 48 KB of static shared memory), else one.
+template <int OP, int R>
+constexpr int kSepTbRows = kSepUnroll<R> == 4 && kSepFolds<OP> == 1 ? 4 : 1;
+
 // The block's shared memory for sep_body.
-template <int OP>
+template <int OP, int R>
 struct SepSmem {
-    float tb[2][kSepFolds<OP>][kSepCols];  // column results, double-buffered
-    float stg[kStageRows][kSepCols];      // source rows in flight
+    float tb[2][kSepFolds<OP>][kSepTbRows<OP, R>][kSepCols];  // column results, double-buffered
+    float stg[kStageRows][kSepCols];                          // source rows in flight
 };
 
 // One unit of the separable march, by a block of kSepThreads threads:
@@ -265,7 +272,7 @@ struct SepSmem {
 // synchronises the block before the shared memory is used again.
 template <int OP, int R>
 __device__ __forceinline__ void sep_body(const LaunchParams& P, int64_t X0, int64_t y0, int rows, bool vec,
-                                         SepSmem<OP>& sm) {
+                                         SepSmem<OP, R>& sm) {
     constexpr int D = 2 * R + 1;
     constexpr int HL = kHalo<R>;
     constexpr int OW = kSepOut<R>;
@@ -304,6 +311,85 @@ __device__ __forceinline__ void sep_body(const LaunchParams& P, int64_t X0, int6
     float core0[4], core1[4];
     (void)core0;
     (void)core1;
+    // Row w of the stored column results folded across into this thread's
+    // four outputs of the row, which it stores.
+    auto fold_row = [&](int w) {
+        if constexpr (kMinMax<F0>) {
+            // Min/Max: output i's window is column results B+i ..
+            // B+i+2R; results B+3 .. B+2R are common to the four, the
+            // rest (B .. B+2 before, B+2R+1 .. B+2R+3 after) are kept
+            // apart and added per output.
+            constexpr int B = HL - R;
+            float core[2], lo[2][3], hi[2][3];
+#pragma unroll
+            for (int q = 0; q < NT / 4; q++) {
+                const float4 f0 = *reinterpret_cast<const float4*>(&tb[buf][0][w][4 * tid + 4 * q]);
+                float4 f1 = f0;
+                if constexpr (NF == 2) f1 = *reinterpret_cast<const float4*>(&tb[buf][NF - 1][w][4 * tid + 4 * q]);
+                const float v[2][4] = {{f0.x, f0.y, f0.z, f0.w}, {f1.x, f1.y, f1.z, f1.w}};
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    const int t = 4 * q + e;
+#pragma unroll
+                    for (int f = 0; f < NF; f++) {
+                        if (t < B || t > B + 2 * R + 3) continue;
+                        if (t <= B + 2) lo[f][t - B] = v[f][e];
+                        else if (t > B + 2 * R) hi[f][t - B - 2 * R - 1] = v[f][e];
+                        else if (t == B + 3) core[f] = v[f][e];
+                        else core[f] = f == 0 ? minmax<F0>(core[f], v[f][e]) : minmax<F1>(core[f], v[f][e]);
+                    }
+                }
+            }
+            float o[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                float a = core[0];
+#pragma unroll
+                for (int k = i; k <= 2; k++) a = minmax<F0>(a, lo[0][k]);
+#pragma unroll
+                for (int k = 0; k < i; k++) a = minmax<F0>(a, hi[0][k]);
+                if constexpr (NF == 2) {
+                    float b = core[1];
+#pragma unroll
+                    for (int k = i; k <= 2; k++) b = minmax<F1>(b, lo[1][k]);
+#pragma unroll
+                    for (int k = 0; k < i; k++) b = minmax<F1>(b, hi[1][k]);
+                    a = sub(a, b);
+                }
+                o[i] = a;
+            }
+            dst.put(P, o);
+        } else {
+            // Stream the column results left to right; each feeds the
+            // outputs whose windows hold it, so every output folds its
+            // 2R+1 terms in order with only its accumulator live.
+            float o[4], o1[4];
+#pragma unroll
+            for (int q = 0; q < NT / 4; q++) {
+                const float4 f0 = *reinterpret_cast<const float4*>(&tb[buf][0][w][4 * tid + 4 * q]);
+                float4 f1 = f0;
+                if constexpr (NF == 2) f1 = *reinterpret_cast<const float4*>(&tb[buf][NF - 1][w][4 * tid + 4 * q]);
+                const float v0[4] = {f0.x, f0.y, f0.z, f0.w};
+                const float v1[4] = {f1.x, f1.y, f1.z, f1.w};
+#pragma unroll
+                for (int e = 0; e < 4; e++)
+#pragma unroll
+                    for (int i = 0; i < 4; i++) {
+                        // output X0 + 4t + i folds column results from t index HL - R + i
+                        const int c = 4 * q + e - (HL - R + i);
+                        if (c < 0 || c > 2 * R) continue;
+                        o[i] = fold_term<F0>(P, o[i], v0[e], c);
+                        if constexpr (NF == 2) o1[i] = fold_term<F1>(P, o1[i], v1[e], c);
+                    }
+            }
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                if constexpr (F0 == STRATA_OP_MEAN) o[i] = div(o[i], (float)(D * D));
+                if constexpr (NF == 2) o[i] = sub(o[i], o1[i]);
+            }
+            dst.put(P, o);
+        }
+    };
     for (int yb = 0; yb < rows; yb += U) {
 #pragma unroll
         for (int u = 0; u < U; u++) {
@@ -339,86 +425,28 @@ __device__ __forceinline__ void sep_body(const LaunchParams& P, int64_t X0, int6
                     if constexpr (NF == 2) c1[i] = col_fold<F1, R, RS>(P, ring, i, u);
                 }
             }
-            *reinterpret_cast<float4*>(&tb[buf][0][4 * tid]) = make_float4(c0[0], c0[1], c0[2], c0[3]);
+            constexpr int TB = kSepTbRows<OP, R>;
+            const int w = TB == 1 ? 0 : u;
+            *reinterpret_cast<float4*>(&tb[buf][0][w][4 * tid]) = make_float4(c0[0], c0[1], c0[2], c0[3]);
             if constexpr (NF == 2)
-                *reinterpret_cast<float4*>(&tb[buf][NF - 1][4 * tid]) = make_float4(c1[0], c1[1], c1[2], c1[3]);
-            __syncthreads();
-            if (writer && kMinMax<F0>) {
-                // Min/Max: output i's window is column results B+i ..
-                // B+i+2R; results B+3 .. B+2R are common to the four, the
-                // rest (B .. B+2 before, B+2R+1 .. B+2R+3 after) are kept
-                // apart and added per output.
-                constexpr int B = HL - R;
-                float core[2], lo[2][3], hi[2][3];
-#pragma unroll
-                for (int q = 0; q < NT / 4; q++) {
-                    const float4 f0 = *reinterpret_cast<const float4*>(&tb[buf][0][4 * tid + 4 * q]);
-                    float4 f1 = f0;
-                    if constexpr (NF == 2) f1 = *reinterpret_cast<const float4*>(&tb[buf][NF - 1][4 * tid + 4 * q]);
-                    const float v[2][4] = {{f0.x, f0.y, f0.z, f0.w}, {f1.x, f1.y, f1.z, f1.w}};
-#pragma unroll
-                    for (int e = 0; e < 4; e++) {
-                        const int t = 4 * q + e;
-#pragma unroll
-                        for (int f = 0; f < NF; f++) {
-                            if (t < B || t > B + 2 * R + 3) continue;
-                            if (t <= B + 2) lo[f][t - B] = v[f][e];
-                            else if (t > B + 2 * R) hi[f][t - B - 2 * R - 1] = v[f][e];
-                            else if (t == B + 3) core[f] = v[f][e];
-                            else core[f] = f == 0 ? minmax<F0>(core[f], v[f][e]) : minmax<F1>(core[f], v[f][e]);
-                        }
-                    }
-                }
-                float o[4];
-#pragma unroll
-                for (int i = 0; i < 4; i++) {
-                    float a = core[0];
-#pragma unroll
-                    for (int k = i; k <= 2; k++) a = minmax<F0>(a, lo[0][k]);
-#pragma unroll
-                    for (int k = 0; k < i; k++) a = minmax<F0>(a, hi[0][k]);
-                    if constexpr (NF == 2) {
-                        float b = core[1];
-#pragma unroll
-                        for (int k = i; k <= 2; k++) b = minmax<F1>(b, lo[1][k]);
-#pragma unroll
-                        for (int k = 0; k < i; k++) b = minmax<F1>(b, hi[1][k]);
-                        a = sub(a, b);
-                    }
-                    o[i] = a;
-                }
-                dst.put(P, o);
-            } else if (writer) {
-                // Stream the column results left to right; each feeds the
-                // outputs whose windows hold it, so every output folds its
-                // 2R+1 terms in order with only its accumulator live.
-                float o[4], o1[4];
-#pragma unroll
-                for (int q = 0; q < NT / 4; q++) {
-                    const float4 f0 = *reinterpret_cast<const float4*>(&tb[buf][0][4 * tid + 4 * q]);
-                    float4 f1 = f0;
-                    if constexpr (NF == 2) f1 = *reinterpret_cast<const float4*>(&tb[buf][NF - 1][4 * tid + 4 * q]);
-                    const float v0[4] = {f0.x, f0.y, f0.z, f0.w};
-                    const float v1[4] = {f1.x, f1.y, f1.z, f1.w};
-#pragma unroll
-                    for (int e = 0; e < 4; e++)
-#pragma unroll
-                        for (int i = 0; i < 4; i++) {
-                            // output X0 + 4t + i folds column results from t index HL - R + i
-                            const int c = 4 * q + e - (HL - R + i);
-                            if (c < 0 || c > 2 * R) continue;
-                            o[i] = fold_term<F0>(P, o[i], v0[e], c);
-                            if constexpr (NF == 2) o1[i] = fold_term<F1>(P, o1[i], v1[e], c);
-                        }
-                }
-#pragma unroll
-                for (int i = 0; i < 4; i++) {
-                    if constexpr (F0 == STRATA_OP_MEAN) o[i] = div(o[i], (float)(D * D));
-                    if constexpr (NF == 2) o[i] = sub(o[i], o1[i]);
-                }
-                dst.put(P, o);
+                *reinterpret_cast<float4*>(&tb[buf][NF - 1][w][4 * tid]) = make_float4(c1[0], c1[1], c1[2], c1[3]);
+            if constexpr (TB == 1) {
+                __syncthreads();
+                if (writer) fold_row(0);
+                dst.step();
+                buf ^= 1;
             }
-            dst.step();
+        }
+        if constexpr (kSepTbRows<OP, R> == 4) {
+            // The step's column results are all stored: one barrier, then
+            // its row folds.
+            const int nu = rows - yb < U ? rows - yb : U;
+            __syncthreads();
+#pragma unroll 1
+            for (int w = 0; w < nu; w++) {
+                if (writer) fold_row(w);
+                dst.step();
+            }
             buf ^= 1;
         }
         if constexpr (RS != D) {
