@@ -597,6 +597,7 @@ def run_serve(args, rank, world, local_rank):
 
     lat = []
     issued = queue.Queue()
+    failed = []
 
     def drain():
         done = False
@@ -611,9 +612,12 @@ def run_serve(args, rank, world, local_rank):
                 if len(batch) >= 256 or issued.empty():
                     break
                 t = issued.get()
-            if batch:
-                lat.extend(r.latency_ms for r in srv.wait_many(batch))
-                srv.release_many(batch)
+            if batch and not failed:
+                try:
+                    lat.extend(r.latency_ms for r in srv.wait_many(batch))
+                    srv.release_many(batch)
+                except Exception as e:  # kept, and raised after the join
+                    failed.append(e)
 
     drainer = threading.Thread(target=drain)
     drainer.start()
@@ -633,6 +637,9 @@ def run_serve(args, rank, world, local_rank):
     issued.put(None)
     drainer.join()
     open_s = time.perf_counter() - t0
+    if failed:
+        raise failed[0]
+    assert len(lat) == len(reqs), f"{len(lat)} latencies for {len(reqs)} requests"
     st = srv.stats()
     srv.close()
 

@@ -270,13 +270,20 @@ void strata_batch_destroy(strata_batch *batch);
  * device memory (one per device, room for STRATA_NOALLOC_BATCH_MAX items;
  * more is EINVAL) and launches the class kernels directly on the stream
  * (0 = the context's), so it makes no cudaMalloc or cudaFree call and
- * builds no graph. The first call on a device looks the scratch area up;
- * make that call before any stream capture. The scratch is shared by
- * every call on the device: calls on one stream follow each other in
- * stream order, but calls on different streams (or different contexts of
- * one device) that overlap on the device race on it, so a caller
- * serialises them, e.g. by keeping every call on one stream.
- * synchronize != 0 waits for the kernels and reports their status.
+ * builds no graph. The first call on a device looks the scratch area up
+ * (and clears its status word); make that call before any stream capture.
+ * The descriptors go up by copies from the library's pageable host
+ * staging, which the next call rewrites, so a call on a stream that is
+ * being captured returns STRATA_EINVAL. The scratch is shared by every
+ * call on the device: calls on one stream follow each other in stream
+ * order, but calls on different streams (or different contexts of one
+ * device) that overlap on the device race on it, so a caller serialises
+ * them, e.g. by keeping every call on one stream. synchronize != 0 waits
+ * for the kernels and reports their status; with synchronize == 0 the
+ * call returns after the launches, and a status its kernels set (a
+ * bounded device wait that ran out) stays in the scratch until the next
+ * call with synchronize != 0 on the device reports it and clears it. The
+ * caller's current device is the same after the call as before it.
  */
 #define STRATA_NOALLOC_BATCH_MAX 64
 int strata_batch_run_noalloc(strata_ctx *ctx, const strata_batch_item *items, int nitems, void *stream,

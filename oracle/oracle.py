@@ -75,6 +75,8 @@ def lib():
         L.orc_go_max.restype = f
         L.orc_go_max.argtypes = [f, f]
         L.orc_atan32_array.argtypes = [p, p, i64]
+        L.orc_atan32_drops.restype = i64
+        L.orc_atan32_drops.argtypes = [ctypes.c_int]
         L.orc_atan2f32_array.argtypes = [p, p, p, i64]
         L.orc_horn_scales.argtypes = [d, d, d, ctypes.POINTER(f), ctypes.POINTER(f)]
         L.orc_zt_scales.argtypes = [d, d, d, ctypes.POINTER(f)]
@@ -103,6 +105,11 @@ def atan32_array(x: np.ndarray) -> np.ndarray:
     out = np.empty_like(x)
     lib().orc_atan32_array(x.ctypes.data, out.ctypes.data, x.size)
     return out
+
+
+def atan32_drops(nthreads: int) -> int:
+    """Arguments among all 2^31 non-negative floats where Atan32 falls."""
+    return int(lib().orc_atan32_drops(nthreads))
 
 
 def atan2f32_array(y: np.ndarray, x: np.ndarray) -> np.ndarray:

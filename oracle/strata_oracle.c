@@ -100,6 +100,49 @@ float orc_atan2f32(float y, float x)
     return u2f(f2u(a) | (f2u(y) & 0x80000000u));
 }
 
+/* The number of non-negative floats x (0 < bits(x) <= bits(+Inf)) with
+ * Atan32(x) < Atan32(the float just below x): 0 when Atan32 never falls
+ * as its argument grows, which the device backend relies on to classify a
+ * slope by its squared gradient magnitude. nthreads threads share the
+ * 2^31 arguments. */
+typedef struct { uint32_t lo, hi; int64_t drops; } mono_job;
+
+static void *mono_worker(void *arg)
+{
+    mono_job *j = (mono_job *)arg;
+    float prev = orc_atan32(u2f(j->lo - 1));
+    for (uint32_t u = j->lo;; u++) {
+        const float y = orc_atan32(u2f(u));
+        if (y < prev) j->drops++;
+        prev = y;
+        if (u == j->hi) break;
+    }
+    return NULL;
+}
+
+int64_t orc_atan32_drops(int nthreads)
+{
+    if (nthreads < 1) nthreads = 1;
+    if (nthreads > 256) nthreads = 256;
+    mono_job jobs[256];
+    pthread_t tid[256];
+    const uint32_t first = 1, last = 0x7f800000u;
+    const uint32_t per = (last - first) / (uint32_t)nthreads + 1;
+    int n = 0;
+    for (uint32_t lo = first; n < nthreads && lo <= last; n++, lo += per) {
+        jobs[n].lo = lo;
+        jobs[n].hi = (last - lo < per - 1) ? last : lo + per - 1;
+        jobs[n].drops = 0;
+        pthread_create(&tid[n], NULL, mono_worker, &jobs[n]);
+    }
+    int64_t drops = 0;
+    for (int i = 0; i < n; i++) {
+        pthread_join(tid[i], NULL);
+        drops += jobs[i].drops;
+    }
+    return drops;
+}
+
 void orc_atan32_array(const float *x, float *out, int64_t n)
 {
     for (int64_t i = 0; i < n; i++) out[i] = orc_atan32(x[i]);

@@ -60,6 +60,7 @@ float orc_atan2f32(float y, float x);
 float orc_go_min(float a, float b);
 float orc_go_max(float a, float b);
 void orc_atan32_array(const float *x, float *out, int64_t n);
+int64_t orc_atan32_drops(int nthreads);
 void orc_atan2f32_array(const float *y, const float *x, float *out, int64_t n);
 
 /* Host constants, as the reference's option code derives them. */

@@ -90,6 +90,44 @@ std::string fmt_v(double x, bool f32 = false) {
 }  // namespace
 
 // ---------------------------------------------------------------------------
+// The caller's current device, put back when an entry point returns. Each
+// entry point makes its context's device current for its CUDA calls; the
+// guard restores the caller's device afterwards, unless the caller's
+// thread had no context on it (then restoring would create one, with its
+// memory, on a device the caller never used).
+
+namespace {
+
+using PrimaryCtxStateFn = int (*)(int, unsigned int*, int*);  // cuDevicePrimaryCtxGetState
+
+bool primary_active(int dev) {
+    static PrimaryCtxStateFn fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuDevicePrimaryCtxGetState", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return reinterpret_cast<PrimaryCtxStateFn>(p);
+    }();
+    unsigned int flags = 0;
+    int active = 0;
+    return fn && fn(dev, &flags, &active) == 0 && active;
+}
+
+struct DeviceGuard {
+    int prev = -1, dev;
+    explicit DeviceGuard(int d) : dev(d) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != d) cudaSetDevice(d);
+    }
+    ~DeviceGuard() {
+        if (prev >= 0 && prev != dev && primary_active(prev)) cudaSetDevice(prev);
+    }
+};
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
 // Context.
 
 struct strata_ctx {
@@ -147,6 +185,7 @@ extern "C" int strata_ctx_create(int device, strata_ctx** out) {
     cudaError_t e = cudaGetDeviceCount(&n);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetDeviceCount");
     if (device < 0 || device >= n) return fail(STRATA_EINVAL, "strata_cuda: device %d out of range [0, %d)", device, n);
+    DeviceGuard device_guard(device);
     e = cudaSetDevice(device);
     if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
     auto* c = new strata_ctx;
@@ -167,7 +206,7 @@ extern "C" int strata_ctx_create(int device, strata_ctx** out) {
 
 extern "C" void strata_ctx_destroy(strata_ctx* c) {
     if (!c) return;
-    cudaSetDevice(c->device);
+    DeviceGuard device_guard(c->device);
     cudaStreamSynchronize(c->stream);
     for (auto& b : c->bufs)
         if (b.p) cudaFree(b.p);
@@ -202,7 +241,7 @@ int take_status(strata_ctx* c, cudaStream_t st) {
 
 extern "C" int strata_ctx_synchronize(strata_ctx* c) {
     if (!c) return fail(STRATA_EINVAL, "strata_cuda: nil context");
-    cudaSetDevice(c->device);
+    DeviceGuard device_guard(c->device);
     cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceSynchronize");
     return take_status(c, c->stream);
@@ -210,7 +249,7 @@ extern "C" int strata_ctx_synchronize(strata_ctx* c) {
 
 extern "C" int strata_alloc(strata_ctx* c, size_t bytes, void** dev) {
     if (!c || !dev) return fail(STRATA_EINVAL, "strata_cuda: nil argument");
-    cudaSetDevice(c->device);
+    DeviceGuard device_guard(c->device);
     cudaError_t e = cudaMalloc(dev, bytes ? bytes : 1);
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -221,7 +260,7 @@ extern "C" int strata_alloc(strata_ctx* c, size_t bytes, void** dev) {
 
 extern "C" int strata_free(strata_ctx* c, void* dev) {
     if (!c) return fail(STRATA_EINVAL, "strata_cuda: nil context");
-    cudaSetDevice(c->device);
+    DeviceGuard device_guard(c->device);
     cudaError_t e = cudaFree(dev);
     if (e != cudaSuccess) return cuda_fail(e, "cudaFree");
     return STRATA_OK;
@@ -229,7 +268,7 @@ extern "C" int strata_free(strata_ctx* c, void* dev) {
 
 extern "C" int strata_upload(strata_ctx* c, void* dev, const void* host, size_t bytes) {
     if (!c) return fail(STRATA_EINVAL, "strata_cuda: nil context");
-    cudaSetDevice(c->device);
+    DeviceGuard device_guard(c->device);
     cudaError_t e = cudaMemcpyAsync(dev, host, bytes, cudaMemcpyHostToDevice, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) return cuda_fail(e, "upload");
@@ -238,7 +277,7 @@ extern "C" int strata_upload(strata_ctx* c, void* dev, const void* host, size_t 
 
 extern "C" int strata_download(strata_ctx* c, void* host, const void* dev, size_t bytes) {
     if (!c) return fail(STRATA_EINVAL, "strata_cuda: nil context");
-    cudaSetDevice(c->device);
+    DeviceGuard device_guard(c->device);
     cudaError_t e = cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) return cuda_fail(e, "download");
@@ -364,6 +403,9 @@ int fill_stage(const strata_stage& s, LaunchParams& p, int epi_index) {
     p.op = (int)s.op;
     p.radius = op_radius(s);
     p.kind = s.kind;
+    // Slope and Aspect read their kind as a flag (take the arctangent;
+    // trigonometric angles).
+    if (s.op == STRATA_OP_SLOPE || s.op == STRATA_OP_ASPECT) p.kind = s.kind != 0;
     memcpy(p.k, s.k, sizeof p.k);
     int r = p.radius;
     if (s.op >= STRATA_OP_RUGGEDNESS && s.op <= STRATA_OP_MAX && (r < 1 || r > STRATA_MAX_RADIUS))
@@ -561,6 +603,80 @@ void fold_tail(LaunchParams& p) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// A Slope followed by a lone Reclass (a classification, or the fold above
+// of a Lookup -> Reclass tail) as a Reclass of the squared gradient
+// magnitude s = gx*gx + gy*gy, the float32 the reference takes the square
+// root of (internal/stencil/horn.go:193-222). The slope of s is
+// float32(Atan32(sqrt(s)) * scale) (or sqrt(s) * scale without the
+// arctangent): the correctly rounded square root is monotone, Atan32 is
+// monotone non-decreasing on the non-negative floats (checked on all 2^31
+// of them), and a product by a positive scale rounded to nearest is
+// monotone, so the slope never falls as s grows. A class break b is then
+// reached exactly from the first s whose slope is at or above b, which a
+// bisection over the floats finds with the device's arithmetic; the kernel
+// compares s with those thresholds and needs no square root, division or
+// arctangent. s is a sum of squares, so never negative; a NaN s (a NaN in
+// the window) stays NaN as the Reclass leaves it, and a break the slope of
+// +Inf does not reach gets a NaN threshold, which no s passes.
+
+// Atan32 (internal/stencil/horn.go:249-262), rounded step by step as the
+// device rounds it.
+float host_atan32(float x) {
+    const float kTan3Pi8 = 0x1.3504f4p+1f, kTanPi8 = 0x1.a8279ap-2f;
+    float num = x, den = 1.0f, y0 = 0.0f;
+    if (x > kTanPi8) {
+        num = x - 1.0f;
+        den = x + 1.0f;
+        y0 = 0x1.921fb6p-1f;
+    }
+    if (x > kTan3Pi8) {
+        num = -1.0f;
+        den = x;
+        y0 = 0x1.921fb6p+0f;
+    }
+    const float t = num / den;
+    const float z = t * t;
+    float p = 0x1.49e1a2p-4f * z - 0x1.1c370ap-3f;
+    p = p * z + 0x1.9924bep-3f;
+    p = p * z - 0x1.555454p-2f;
+    const float pzt = (p * z) * t;
+    return y0 + (pzt + t);
+}
+
+float host_slope_of_square(float s, float scale, bool take_atan) {
+    const float m = std::sqrt(s);
+    return (take_atan ? host_atan32(m) : m) * scale;
+}
+
+void fold_slope_square(LaunchParams& p) {
+    if (p.op != STRATA_OP_SLOPE || p.nepi != 1 || p.epi[0].op != STRATA_OP_RECLASS) return;
+    EpiStage& e = p.epi[0];
+    const float scale = p.k[2];
+    if (e.n > strata::kChainBreaks || !(scale > 0) || std::isinf(scale)) return;
+    const bool take_atan = p.kind != 0;
+    const float inf = std::numeric_limits<float>::infinity();
+    const uint32_t k0 = float_key(0.0f), kinf = float_key(inf);
+    for (int j = 0; j < e.n; j++) {
+        const float b = e.a[j];
+        float t;
+        if (host_slope_of_square(inf, scale, take_atan) < b) {
+            t = std::numeric_limits<float>::quiet_NaN();
+        } else if (host_slope_of_square(0.0f, scale, take_atan) >= b) {
+            t = 0.0f;
+        } else {
+            uint32_t lo = k0, hi = kinf;  // slope(lo) < b <= slope(hi)
+            while (hi - lo > 1) {
+                const uint32_t m = lo + (hi - lo) / 2;
+                (host_slope_of_square(key_float(m), scale, take_atan) >= b ? hi : lo) = m;
+            }
+            t = key_float(hi);
+        }
+        e.a[j] = t;
+    }
+    p.kind = strata::kSlopeSquareClass;
+}
+
 // Resolves stages into launch parameters (op, radius, epilogue).
 int plan_stages(const strata_stage* stages, int nstages, LaunchParams& p, int* nout) {
     if (!stages || nstages < 1) return fail(STRATA_EINVAL, "engine: nil kernel");
@@ -590,6 +706,7 @@ int plan_stages(const strata_stage* stages, int nstages, LaunchParams& p, int* n
     }
     p.nepi = epi;
     fold_tail(p);
+    fold_slope_square(p);
     *nout = s0.op == STRATA_OP_GRADIENT ? 2 : 1;
     return STRATA_OK;
 }
@@ -795,6 +912,15 @@ void fill_validity(ValidityParams& v, const DevOperand& s, bool src_masked, cons
     v.dst_words = ((b1 + 31) >> 5) - v.dst_lo_word;
 }
 
+
+
+// The failure-path test's switch (STRATA_TEST_STALL_FIRST_WAIT=1): the TMA
+// march then reports a bounded wait that ran out, with nothing faulted.
+bool test_stall_requested() {
+    const char* v = getenv("STRATA_TEST_STALL_FIRST_WAIT");
+    return v && v[0] == '1';
+}
+
 }  // namespace
 
 extern "C" int strata_process(strata_ctx* c, const strata_stage* stages, int nstages, const strata_raster* src,
@@ -809,7 +935,7 @@ extern "C" int strata_process(strata_ctx* c, const strata_stage* stages, int nst
     if ((rc = check_operands(src, nsrc, dst, ndst, nout, p.radius))) return rc;
 
     std::lock_guard<std::mutex> lock(c->mu);
-    cudaSetDevice(c->device);
+    DeviceGuard device_guard(c->device);
     cudaStream_t st = (opts && opts->stream) ? (cudaStream_t)opts->stream : c->stream;
     const int64_t W = src[0].width, H = src[0].height;
 
@@ -835,6 +961,7 @@ extern "C" int strata_process(strata_ctx* c, const strata_stage* stages, int nst
     p.out_x0 = 0;
     p.out_x1 = W;
     p.status = c->d_status;
+    p.test_stall = test_stall_requested();
 
     // Row strips: the whole raster at once, or strips of about 2^22 cells
     // with the cancel flag polled between them.
@@ -1296,7 +1423,7 @@ extern "C" int strata_process_chunked(strata_ctx* c, const strata_stage* stages,
     const int64_t in_cells = (inH - 1) * in_stride + inW;
 
     std::lock_guard<std::mutex> lock(c->mu);
-    cudaSetDevice(c->device);
+    DeviceGuard device_guard(c->device);
     cudaStream_t st = (opts && opts->stream) ? (cudaStream_t)opts->stream : c->stream;
 
     TileSet sets[2];
@@ -1544,7 +1671,7 @@ extern "C" int strata_process_features(strata_ctx* c, const strata_stage* stages
     if ((rc = check_operands(src, 1, dst, ndst, ndst, rmax))) return rc;
 
     std::lock_guard<std::mutex> lock(c->mu);
-    cudaSetDevice(c->device);
+    DeviceGuard device_guard(c->device);
     cudaStream_t st = (opts && opts->stream) ? (cudaStream_t)opts->stream : c->stream;
     cudaStream_t cs = c->copy_stream;
     const int64_t W = src[0].width, H = src[0].height;
@@ -1743,7 +1870,7 @@ extern "C" int strata_batch_create(strata_ctx* c, const strata_batch_item* items
     *out = nullptr;
     if (nitems < 1 || !items) return fail(STRATA_EINVAL, "engine: a batch needs at least one raster");
     std::lock_guard<std::mutex> lock(c->mu);
-    cudaSetDevice(c->device);
+    DeviceGuard device_guard(c->device);
     std::vector<strata::BatchItem> host((size_t)nitems);
     int64_t cells = 0, in_bytes = 0, out_bytes = 0;
     for (int i = 0; i < nitems; i++) {
@@ -1816,7 +1943,7 @@ extern "C" int strata_batch_create(strata_ctx* c, const strata_batch_item* items
 
 extern "C" int strata_batch_run(strata_batch* B, void* stream, int synchronize) {
     if (!B) return fail(STRATA_EINVAL, "engine: nil batch");
-    cudaSetDevice(B->ctx->device);
+    DeviceGuard device_guard(B->ctx->device);
     cudaStream_t st = stream ? (cudaStream_t)stream : B->ctx->stream;
     cudaError_t e = cudaGraphLaunch(B->exec, st);
     if (e != cudaSuccess) return cuda_fail(e, "batch launch");
@@ -1839,7 +1966,7 @@ extern "C" int strata_batch_info(const strata_batch* B, strata_stats* stats, int
 
 extern "C" void strata_batch_destroy(strata_batch* B) {
     if (!B) return;
-    cudaSetDevice(B->ctx->device);
+    DeviceGuard device_guard(B->ctx->device);
     if (B->exec) cudaGraphExecDestroy(B->exec);
     if (B->graph) cudaGraphDestroy(B->graph);
     if (B->d_items) cudaFree(B->d_items);
@@ -1879,13 +2006,14 @@ int g_noalloc_order[STRATA_NOALLOC_BATCH_MAX];
 strata::BatchClass g_noalloc_classes[STRATA_NOALLOC_BATCH_MAX];
 
 // The device address of the scratch area, looked up once per device with
-// that device current.
+// that device current (the caller's guard makes it current), and its
+// status word cleared.
 int scratch_address(int device, unsigned char** ptr) {
     if (device < 0 || device >= kMaxDevices) return fail(STRATA_EINVAL, "engine: device %d out of range", device);
     ScratchSlot& s = g_scratch[device];
     std::call_once(s.once, [&] {
-        s.err = cudaSetDevice(device);
-        if (s.err == cudaSuccess) s.err = cudaGetSymbolAddress((void**)&s.ptr, g_batch_scratch);
+        s.err = cudaGetSymbolAddress((void**)&s.ptr, g_batch_scratch);
+        if (s.err == cudaSuccess) s.err = cudaMemset(s.ptr, 0, sizeof(int));
     });
     if (s.err != cudaSuccess) return cuda_fail(s.err, "batch scratch address");
     *ptr = s.ptr;
@@ -1903,10 +2031,19 @@ extern "C" int strata_batch_run_noalloc(strata_ctx* c, const strata_batch_item* 
                     STRATA_NOALLOC_BATCH_MAX);
     std::lock_guard<std::mutex> lock(c->mu);
     std::lock_guard<std::mutex> staging(g_noalloc_mu);
+    DeviceGuard device_guard(c->device);
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+    // The descriptors go up from the library's pageable host staging,
+    // which the next call rewrites: a capture would record those copies by
+    // host address and replay whatever the latest call left there.
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaError_t e = cudaStreamIsCapturing(st, &cap);
+    if (e != cudaSuccess) return cuda_fail(e, "batch stream");
+    if (cap != cudaStreamCaptureStatusNone)
+        return fail(STRATA_EINVAL, "engine: a batch without allocation does not run on a capturing stream");
     unsigned char* scratch;
     int rc;
     if ((rc = scratch_address(c->device, &scratch))) return rc;
-    cudaSetDevice(c->device);
     int* d_status = reinterpret_cast<int*>(scratch);
     auto* d_items = reinterpret_cast<strata::BatchItem*>(scratch + kScratchHead);
     auto* d_vitems = reinterpret_cast<strata::ValidityItem*>(scratch + kScratchHead + kItemBytes);
@@ -1921,10 +2058,9 @@ extern "C" int strata_batch_run_noalloc(strata_ctx* c, const strata_batch_item* 
     strata::ValidityClass vcls[STRATA_MAX_RADIUS + 1];
     int nvc = 0;
     const int nv = strata::batch_plan_validity(host, nitems, g_noalloc_vitems, vcls, &nvc);
-    cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
-    cudaError_t e = cudaMemsetAsync(d_status, 0, sizeof(int), st);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(d_items, host, sizeof(strata::BatchItem) * (size_t)nitems, cudaMemcpyHostToDevice, st);
+    // The status word is not cleared here: a status that an unsynchronised
+    // call's kernels set stays until a synchronised call reads and clears it.
+    e = cudaMemcpyAsync(d_items, host, sizeof(strata::BatchItem) * (size_t)nitems, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess && nv > 0)
         e = cudaMemcpyAsync(d_vitems, g_noalloc_vitems, sizeof(strata::ValidityItem) * (size_t)nv,
                             cudaMemcpyHostToDevice, st);
@@ -1939,7 +2075,10 @@ extern "C" int strata_batch_run_noalloc(strata_ctx* c, const strata_batch_item* 
     int status = 0;
     if ((e = cudaMemcpy(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost)) != cudaSuccess)
         return cuda_fail(e, "batch status");
-    if (status) return fail(status, "engine: a batch kernel reported status %d", status);
+    if (status) {
+        if ((e = cudaMemset(d_status, 0, sizeof(int))) != cudaSuccess) return cuda_fail(e, "batch status");
+        return fail(status, "engine: a batch kernel reported status %d", status);
+    }
     return STRATA_OK;
 }
 
@@ -2015,7 +2154,6 @@ struct strata_server {
     bool stop = false;
     std::thread thread;
     cudaMemPool_t pool = nullptr;
-    int sms = 148;
     int64_t batches = 0, served = 0;
 };
 
@@ -2197,8 +2335,7 @@ extern "C" int strata_server_create(strata_ctx* c, const strata_raster* mosaic, 
     }
     S->band = o && o->band > 0 ? o->band : 16;
     const int nstreams = o && o->streams > 0 ? o->streams : 4;
-    cudaSetDevice(c->device);
-    cudaDeviceGetAttribute(&S->sms, cudaDevAttrMultiProcessorCount, c->device);
+    DeviceGuard device_guard(c->device);
     if ((rc = stage_in(c, nullptr, *mosaic, 0, false, &S->dm))) {
         delete S;
         return rc;
@@ -2389,7 +2526,7 @@ extern "C" int strata_server_wait_many(strata_server* S, const uint64_t* tickets
 extern "C" int strata_server_release(strata_server* S, uint64_t ticket) {
     if (!S) return fail(STRATA_EINVAL, "engine: nil server");
     std::lock_guard<std::mutex> lk(S->mu);
-    cudaSetDevice(S->ctx->device);
+    DeviceGuard device_guard(S->ctx->device);
     const int rc = release_locked(S, ticket);
     S->cv.notify_one();
     return rc;
@@ -2398,7 +2535,7 @@ extern "C" int strata_server_release(strata_server* S, uint64_t ticket) {
 extern "C" int strata_server_release_many(strata_server* S, const uint64_t* tickets, int n) {
     if (!S || (n > 0 && !tickets)) return fail(STRATA_EINVAL, "engine: nil server");
     std::lock_guard<std::mutex> lk(S->mu);
-    cudaSetDevice(S->ctx->device);
+    DeviceGuard device_guard(S->ctx->device);
     int rc = STRATA_OK;
     for (int i = 0; i < n && rc == STRATA_OK; i++) rc = release_locked(S, tickets[i]);
     S->cv.notify_one();
@@ -2422,7 +2559,7 @@ extern "C" void strata_server_destroy(strata_server* S) {
         S->cv.notify_all();
     }
     if (S->thread.joinable()) S->thread.join();
-    cudaSetDevice(S->ctx->device);
+    DeviceGuard device_guard(S->ctx->device);
     for (Slot& s : S->slots) {
         if (s.stream) cudaStreamSynchronize(s.stream);
         if (s.done) cudaEventDestroy(s.done);

@@ -88,16 +88,7 @@ __global__ void __launch_bounds__(32 * kValidityWarps) batch_validity_kernel(con
 // Blocks that fill the GPU once at the kernel's occupancy (per_sm, looked
 // up once per kernel by its launcher), never more than the units.
 int persistent_grid(int per_sm, int64_t total) {
-    static int sms[64] = {};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev < 0 || dev >= 64) dev = 0;
-    if (!sms[dev]) {
-        int n = 148;
-        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-        sms[dev] = n;
-    }
-    const int64_t g = (int64_t)sms[dev] * per_sm;
+    const int64_t g = (int64_t)sm_count() * per_sm;
     return (int)(total < g ? total : g);
 }
 
@@ -148,7 +139,7 @@ Key key_of(const LaunchParams& p) {
     Key k{0, p.op, p.radius, 0, 0};
     if (p.radius <= 1) {
         k.radius = 1;
-        if (p.op == STRATA_OP_SLOPE || p.op == STRATA_OP_ASPECT) k.kind = p.kind ? 1 : 0;
+        if (p.op == STRATA_OP_SLOPE || p.op == STRATA_OP_ASPECT) k.kind = p.kind;
         if (p.op == STRATA_OP_CURVATURE || p.op == STRATA_OP_RUGGEDNESS) k.kind = p.kind;
         k.epi = p.nepi > 0;
     } else if (p.op == STRATA_OP_CORRELATE || (p.op == STRATA_OP_RUGGEDNESS && p.kind != STRATA_RUG_ROUGHNESS)) {
@@ -254,6 +245,7 @@ bool launch_batch_class(const BatchClass& c, const BatchItem* d, cudaStream_t s)
     switch (c.op) {
     case STRATA_OP_GRADIENT: return launch_march_class<STRATA_OP_GRADIENT, 0, false>(c, d, s);
     case STRATA_OP_SLOPE:
+        if (c.kind == kSlopeSquareClass) return launch_march_class<STRATA_OP_SLOPE, kSlopeSquareClass, false>(c, d, s);
         return c.kind ? launch_march_epi<STRATA_OP_SLOPE, 1>(c, d, s) : launch_march_epi<STRATA_OP_SLOPE, 0>(c, d, s);
     case STRATA_OP_ASPECT:
         return c.kind ? launch_march_epi<STRATA_OP_ASPECT, 1>(c, d, s) : launch_march_epi<STRATA_OP_ASPECT, 0>(c, d, s);

@@ -50,16 +50,7 @@ __global__ void __launch_bounds__(kWinThreads) batch_window_kernel(const BatchIt
 // Blocks that fill the GPU once at the kernel's occupancy (per_sm), never
 // more than the units.
 int grid_for(int per_sm, int64_t total) {
-    static int sms[64] = {};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev < 0 || dev >= 64) dev = 0;
-    if (!sms[dev]) {
-        int n = 148;
-        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-        sms[dev] = n;
-    }
-    const int64_t g = (int64_t)sms[dev] * per_sm;
+    const int64_t g = (int64_t)sm_count() * per_sm;
     return (int)(total < g ? total : g);
 }
 

@@ -66,13 +66,6 @@ int focal_vec(const LaunchParams& p) {
            !((p.out_x0 - p.dst_x0) & 3) && aligned16(p.src) && aligned16(p.dst0);
 }
 
-int sm_count() {
-    int dev = 0, n = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-    return n;
-}
-
 template <int OP, int R>
 int64_t launch_sep(const LaunchParams& p, cudaStream_t s, int64_t* window_cells) {
     constexpr int OW = kSepOut<R>;

@@ -28,10 +28,6 @@ __global__ void __launch_bounds__(256) pointwise_kernel(const __grid_constant__ 
     }
 }
 
-// ---------------------------------------------------------------------------
-// Validity.
-
-
 }  // namespace
 
 
@@ -39,7 +35,7 @@ int64_t launch_data(const LaunchParams& p, cudaStream_t s, int64_t* window_cells
     if (p.op == STRATA_OP_LOOKUP || p.op == STRATA_OP_RECLASS) {
         const int64_t n = (p.out_x1 - p.out_x0) * (p.out_y1 - p.out_y0);
         int64_t blocks = (n + 255) / 256;
-        if (blocks > 148 * 64) blocks = 148 * 64;
+        if (blocks > (int64_t)sm_count() * 64) blocks = (int64_t)sm_count() * 64;
         if (blocks < 1) blocks = 1;
         pointwise_kernel<<<(unsigned)blocks, 256, 0, s>>>(p);
         if (window_cells) *window_cells = n;

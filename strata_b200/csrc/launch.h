@@ -10,6 +10,29 @@
 namespace strata {
 
 constexpr int kMaxEpilogue = 4;  // pointwise stages fused after a stencil
+// Breaks of a lone Reclass epilogue that the kernels take as a chain of
+// compares (ops3.cuh reclass_chain4) rather than a table search.
+constexpr int kChainBreaks = 8;
+// LaunchParams.kind of a Slope whose Reclass epilogue the host has moved
+// onto the squared gradient magnitude (api.cu fold_slope_square): the
+// kernel classifies gx*gx + gy*gy against epi[0]'s thresholds and takes no
+// square root, arctangent or scale.
+constexpr int kSlopeSquareClass = 2;
+
+// The multiprocessor count of the current device, looked up once per
+// device (launch shapes are sized in multiples of it).
+inline int sm_count() {
+    static int cache[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) dev = 0;
+    if (!cache[dev]) {
+        int n = 0;
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n < 1) n = 1;
+        cache[dev] = n;
+    }
+    return cache[dev];
+}
 constexpr int kMaxWeights = (2 * STRATA_MAX_RADIUS + 1) * (2 * STRATA_MAX_RADIUS + 1);
 
 // One pointwise stage fused as an epilogue: LOOKUP (a = xs, b = ys, n
@@ -49,6 +72,11 @@ struct alignas(16) LaunchParams {
     int radius;
     int kind;
     int nepi;
+    // Non-zero only in the failure-path test (the environment variable
+    // STRATA_TEST_STALL_FIRST_WAIT=1): the TMA march's first wait is on a
+    // barrier nothing arrives at, with a short bound, so it runs out.
+    int test_stall;
+    int pad_;
     float k[16];
     float w[kMaxWeights];  // CORRELATE weights (rotation applied); SEPARABLE row taps w[0..], column taps w[17..]
     EpiStage epi[kMaxEpilogue];

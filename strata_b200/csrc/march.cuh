@@ -87,14 +87,19 @@ __device__ __forceinline__ void row_compute(const LaunchParams& P, const EpiTabl
 #pragma unroll
         for (int p = 0; p < 2; p++) {
             F2 r;
-            if constexpr (OP == STRATA_OP_SLOPE) r = slope2(gx[p], gy[p], splat(P.k[2]), KIND != 0);
+            if constexpr (OP == STRATA_OP_SLOPE && KIND == kSlopeSquareClass)
+                r = add_p(mul2(gx[p], gx[p]), mul2(gy[p], gy[p]));  // magnitude's radicand (horn.go:220-222)
+            else if constexpr (OP == STRATA_OP_SLOPE) r = slope2(gx[p], gy[p], splat(P.k[2]), KIND != 0);
             else if constexpr (OP == STRATA_OP_ASPECT) r = aspect2(gx[p], gy[p], P.k[2], KIND != 0);
             else r = shade2(gx[p], gy[p], P.k[2], P.k[3], P.k[4]);
             o0[2 * p] = rowin && colin[2 * p] ? lo(r) : nan;
             o0[2 * p + 1] = rowin && colin[2 * p + 1] ? hi(r) : nan;
         }
-        // The epilogue maps NaN to itself, so the edge ring stays NaN.
-        if constexpr (EPI) epilogue4(P, *T, o0);
+        // The epilogue maps NaN to itself, so the edge ring stays NaN. A
+        // Slope classified on its squared magnitude compares the radicand
+        // with the thresholds the host moved its classes to.
+        if constexpr (OP == STRATA_OP_SLOPE && KIND == kSlopeSquareClass) reclass_chain4(P.epi[0], o0);
+        else if constexpr (EPI) epilogue4(P, *T, o0);
     } else if constexpr (OP == STRATA_OP_CURVATURE) {
         // Pairs (0, 1) and (2, 3) again: the centre column's terms come
         // packed from the rows, the terms of the shifted columns per cell.

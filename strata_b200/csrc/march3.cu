@@ -216,9 +216,9 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 }
 
 // The bounded wait for the phase of `parity` on bar; false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t limit = kSpinLimit) {
     for (uint32_t i = 0; !mbar_try_wait(bar, parity); i++)
-        if (i >= kSpinLimit) return false;
+        if (i >= limit) return false;
     return true;
 }
 
@@ -240,7 +240,7 @@ __global__ void __launch_bounds__(kWarps * 32, 6)
                       int col_blocks) {
     constexpr bool kHorn = kIsHorn<OP>;
     __shared__ __align__(128) float sbuf[kWarps][kBoxes][kBoxRows * kBoxCols];
-    __shared__ __align__(8) uint64_t sbar[kWarps][kBoxes];
+    __shared__ __align__(8) uint64_t sbar[kWarps][kBoxes + 1];  // the last: the failure-path test's
     EpiTables* T = EpiSmem<EPI>::get();
     if constexpr (EPI) {
         stage_epilogue(P, *T);
@@ -263,7 +263,7 @@ __global__ void __launch_bounds__(kWarps * 32, 6)
 
     if (lane == 0) {
 #pragma unroll
-        for (int s = 0; s < kBoxes; s++) mbar_init(&bars[s], 1);
+        for (int s = 0; s <= kBoxes; s++) mbar_init(&bars[s], 1);
         mbar_fence_init();
     }
     __syncwarp();
@@ -279,6 +279,9 @@ __global__ void __launch_bounds__(kWarps * 32, 6)
         for (int b = 0; b < issued; b++) issue(b);
 
     bool ok = true;
+    // The failure-path test: a wait on a barrier that nothing arrives at
+    // runs out (after 2^10 polls), as a copy that never lands would.
+    if (P.test_stall) ok = __all_sync(kFull, mbar_wait(&bars[kBoxes], 0u, 1u << 10));
     // Reads row m (waiting for its box first when it is the box's first
     // row), and when m is its box's last row, gives the slot to the box
     // kBoxes later.
@@ -314,8 +317,10 @@ __global__ void __launch_bounds__(kWarps * 32, 6)
     // and takes row k + 2; unrolled by 4, every index is a constant.
     Row6 ring[4];
     float hr[4][4];
-    take(0, ring[0]);
-    take(1, ring[1]);
+    if (ok) {
+        take(0, ring[0]);
+        take(1, ring[1]);
+    }
     if constexpr (kHorn) {
         hdiff(ring[0], hr[0]);
         hdiff(ring[1], hr[1]);
@@ -381,9 +386,9 @@ int64_t launch_march(const LaunchParams& p, cudaStream_t s) {
     const int64_t w = p.out_x1 - p.out_x0, h = p.out_y1 - p.out_y0;
     const int64_t segs = (w + 127) / 128;
     const int64_t col_blocks = (segs + kWarps - 1) / kWarps;
-    // Strip height: enough warps for several waves over 148 SMs, at least
+    // Strip height: enough warps for several waves over the SMs, at least
     // 8 rows and at most 64 (the halo costs 2 rows a strip).
-    int64_t strip = segs > 0 ? (h * segs) / (148 * 48 * 4) : h;
+    int64_t strip = segs > 0 ? (h * segs) / ((int64_t)sm_count() * 48 * 4) : h;
     strip = strip < 8 ? 8 : (strip > 64 ? 64 : strip);
     const int64_t strips = (h + strip - 1) / strip;
     const int64_t blocks = col_blocks * strips;
@@ -428,7 +433,7 @@ int64_t launch_any(const LaunchParams& p, cudaStream_t s) {
     const int64_t w = p.out_x1 - p.out_x0, h = p.out_y1 - p.out_y0;
     const int64_t segs = (w + 127) / 128;
     const int64_t col_blocks = (segs + kWarps - 1) / kWarps;
-    int64_t strip = segs > 0 ? (h * segs) / (148 * 48 * 4) : h;
+    int64_t strip = segs > 0 ? (h * segs) / ((int64_t)sm_count() * 48 * 4) : h;
     strip = strip < 8 ? 8 : (strip > 64 ? 64 : strip);
     const int64_t blocks = col_blocks * ((h + strip - 1) / strip);
     march_any_kernel<OP, KIND, EPI><<<(unsigned)blocks, kWarps * 32, 0, s>>>(p, (int)strip, (int)col_blocks);
@@ -470,6 +475,7 @@ int64_t launch_march_any(const LaunchParams& p, cudaStream_t s) {
     switch (p.op) {
     case STRATA_OP_GRADIENT: return launch_any<STRATA_OP_GRADIENT, 0, false>(p, s);
     case STRATA_OP_SLOPE:
+        if (p.kind == kSlopeSquareClass) return launch_any<STRATA_OP_SLOPE, kSlopeSquareClass, false>(p, s);
         return p.kind ? launch_any_epi<STRATA_OP_SLOPE, 1>(p, s) : launch_any_epi<STRATA_OP_SLOPE, 0>(p, s);
     case STRATA_OP_ASPECT:
         return p.kind ? launch_any_epi<STRATA_OP_ASPECT, 1>(p, s) : launch_any_epi<STRATA_OP_ASPECT, 0>(p, s);
@@ -502,6 +508,7 @@ int64_t launch_march3(const LaunchParams& p, cudaStream_t s) {
     switch (p.op) {
     case STRATA_OP_GRADIENT: return launch_epi<STRATA_OP_GRADIENT, 0>(p, s);
     case STRATA_OP_SLOPE:
+        if (p.kind == kSlopeSquareClass) return launch_march<STRATA_OP_SLOPE, kSlopeSquareClass, false>(p, s);
         return p.kind ? launch_epi<STRATA_OP_SLOPE, 1>(p, s) : launch_epi<STRATA_OP_SLOPE, 0>(p, s);
     case STRATA_OP_ASPECT:
         return p.kind ? launch_epi<STRATA_OP_ASPECT, 1>(p, s) : launch_epi<STRATA_OP_ASPECT, 0>(p, s);

@@ -151,10 +151,6 @@ __device__ __forceinline__ void epi_stage4(const EpiStage& e, const float* ta, c
     }
 }
 
-// Breaks of a lone Reclass stage that the select chain below takes; the
-// folded Lookup -> Reclass tail of a slope classification has a handful.
-constexpr int kChainBreaks = 8;
-
 // A lone Reclass over four cells as a chain of selects against its breaks
 // in increasing order: the last break at or below v names the class, which
 // is the search's count for strictly increasing, NaN-free breaks (the host

@@ -31,9 +31,7 @@ void launch_r(const ValidityParams& v, cudaStream_t s) {
     const int64_t w = v.out_x1 - v.out_x0, h = v.out_y1 - v.out_y0;
     const int64_t strips = (w + kStripCells - 1) / kStripCells;
     // About 48 warps an SM in all, in bands of at least 8 rows.
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int sms = sm_count();
     int64_t bands = ((int64_t)sms * 48 + strips - 1) / strips;
     int64_t band = (h + bands - 1) / bands;
     if (band < 8) band = 8;

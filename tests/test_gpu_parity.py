@@ -280,6 +280,85 @@ def test_stencil_reclass_on_output_values(nb):
             check_case(make(), dem, 1, device, lay, f"nb={nb} masked={masked} device={device} layout={li}")
 
 
+def _slope_of_square(s, scale, take_atan):
+    """The oracle's slope of a squared gradient magnitude s."""
+    from oracle import oracle as orc
+
+    m = np.sqrt(np.asarray(s, np.float32))
+    t = orc.atan32_array(m) if take_atan else m
+    return (t * np.float32(scale)).astype(np.float32)
+
+
+def _square_thresholds(breaks, scale, take_atan):
+    """Per break, the least non-negative float s whose slope reaches it
+    (bisection over the floats in order with the oracle's arithmetic), or
+    None when no s does."""
+    out = []
+    for b in np.asarray(breaks, np.float32):
+        lo, hi = 0, 0x7F800000  # bit patterns of +0 and +Inf
+        f = lambda u: _slope_of_square(np.array([u], np.uint32).view(np.float32), scale, take_atan)[0]
+        if f(hi) < b:
+            out.append(None)
+            continue
+        if f(lo) >= b:
+            out.append(np.float32(0))
+            continue
+        while hi - lo > 1:
+            m = (lo + hi) // 2
+            if f(m) >= b:
+                hi = m
+            else:
+                lo = m
+        out.append(np.array([hi], np.uint32).view(np.float32)[0])
+    return out
+
+
+@pytest.mark.parametrize("units", [0, 1, 2])
+def test_slope_class_at_square_thresholds(units):
+    """A Slope followed by a Reclass (and the folded Slope -> Lookup ->
+    Reclass) runs on the squared gradient magnitude against thresholds the
+    host derives; on planes whose squared magnitude lies within a few
+    hundred float steps of every class threshold, on both sides of it, the
+    device equals the oracle's Slope -> Lookup -> Reclass bit for bit."""
+    cs = 10.0
+    opts = terrain.SlopeOptions(CellSize=cs, Units=units)
+    scale = {0: np.float32(180 / np.pi), 1: np.float32(100), 2: np.float32(1)}[units]
+    take_atan = units != 1
+    # class breaks in the slope's own unit: the bench's pipeline fold for
+    # degrees, spread values for the other units
+    breaks = {0: [3.4, 7.9, 15.2, 27.0], 1: [2.0, 9.5, 40.0, 150.0], 2: [0.05, 0.2, 0.6, 1.2]}[units]
+    values = [1, 2, 3, 4, 5]
+    ts = [t for t in _square_thresholds(breaks, scale, take_atan) if t is not None and t > 0]
+    assert len(ts) == len(breaks)
+    rng = np.random.default_rng(units)
+    bands = []
+    for t in ts:
+        g = np.sqrt(np.float64(t))
+        for phi in (0.0, 0.4, 1.1, 2.9):
+            ax, ay = cs * g * np.cos(phi), cs * g * np.sin(phi)
+            x0, y0, base = rng.uniform(0, 500), rng.uniform(0, 500), rng.uniform(500, 2500)
+            yy, xx = np.mgrid[0:5, 0:256]
+            bands.append((base + ax * (xx + x0) + ay * (yy + y0)).astype(np.float32))
+    dem = np.concatenate(bands, axis=0)
+    h, w = dem.shape
+    src = host_raster(dem)
+    slope_only = like(src, masked=False)
+    run_oracle(terrain.slope_stage(opts), src, [slope_only])
+    sl = slope_only.numpy()
+    for j, b in enumerate(breaks):
+        # the interior rows of the break's four planes
+        rows = [j * 20 + p * 5 + k for p in range(4) for k in (1, 2, 3)]
+        band = sl[rows][:, 1:-1]
+        assert (band < np.float32(b)).any() and (band >= np.float32(b)).any(), f"break {b} not straddled"
+    make = lambda: terrain.slope_stage(opts).extend(transfer.reclass_stage(breaks, values))
+    make_pipe = lambda: terrain.slope_stage(opts).extend(transfer.lookup_stage([0, 1e6], [0, 1e6])).extend(
+        transfer.reclass_stage(breaks, values))
+    for mk in (make, make_pipe):
+        for device in (False, True):
+            lay = dict(src=dict(stride=None, offset=0, valid=None), dst=dict(stride=None, offset=0, masked=False))
+            check_case(mk(), dem, 1, device, lay, f"units={units} device={device}")
+
+
 def test_pipeline_slope_lookup_reclass():
     """The fused Slope -> Lookup -> Reclass pass equals the oracle's three
     stages, which equal three separate calls (internal/exec/pipeline.go)."""

@@ -76,6 +76,13 @@ def test_atan32_accuracy_stride():
         assert np.abs(g - np.arctan(xs.astype(np.float64))).max() <= 1.5e-7
 
 
+def test_atan32_monotone_on_nonnegative_floats():
+    """Atan32 never falls as its argument grows, over every non-negative
+    float up to +Inf. The device backend classifies a Slope by its squared
+    gradient magnitude (api.cu fold_slope_square) on the strength of this."""
+    assert orc.atan32_drops(os.cpu_count() or 1) == 0
+
+
 def test_atan2f32_exact_table():
     for y, x, want in KAT["atan2f32_exact"]["rows"]:
         got = orc.atan2f32(f(y), f(x))

@@ -122,3 +122,57 @@ def test_noalloc_rejects_oversized_and_host_rasters():
     want = _run_existing(ctx, spec)
     for k in range(spec[0][3]):
         assert_same_raster(to_host(dsts[0][k]), to_host(want[0][k]), f"after rejections, output {k}")
+
+
+def test_noalloc_allocates_nothing_and_keeps_the_device():
+    """After a first call (which looks the scratch up and loads the batch
+    kernels), further calls leave the device's free memory exactly as it
+    was: no cudaMalloc, no pool growth, no graph. The caller's current
+    device is unchanged."""
+    import torch
+
+    ctx = engine.device_context(0)
+    L = _lib.lib()
+    spec = _set(14, 16)
+    dsts = _outputs(spec)
+    arr, _keep = _c_items(spec, dsts)
+    _lib.check(L.strata_batch_run_noalloc(ctx, arr, len(spec), None, 1))
+    torch.cuda.synchronize()
+    dev = torch.cuda.current_device()
+    free0 = torch.cuda.mem_get_info()[0]
+    for i in range(20):
+        _lib.check(L.strata_batch_run_noalloc(ctx, arr, len(spec), None, i % 2))
+    _lib.check(L.strata_batch_run_noalloc(ctx, arr, len(spec), None, 1))
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+    assert torch.cuda.current_device() == dev
+    want = _run_existing(ctx, spec)
+    for i, (_stages, _, src, nout, tile) in enumerate(spec):
+        for k in range(nout):
+            assert_same_raster(to_host(dsts[i][k]), to_host(want[i][k]), f"raster {i} output {k}")
+
+
+def test_noalloc_refuses_a_capturing_stream():
+    """A call on a stream that is being captured returns EINVAL (its
+    descriptor copies come from host staging that the next call rewrites)
+    and launches nothing."""
+    import torch
+
+    ctx = engine.device_context(0)
+    L = _lib.lib()
+    spec = _set(15, 2)
+    dsts = _outputs(spec)
+    arr, _keep = _c_items(spec, dsts)
+    _lib.check(L.strata_batch_run_noalloc(ctx, arr, len(spec), None, 1))  # the scratch set up before capture
+    s = torch.cuda.Stream()
+    g = torch.cuda.CUDAGraph()
+    x = torch.zeros(16, device="cuda")
+    rc = None
+    with torch.cuda.graph(g, stream=s):
+        x += 1
+        rc = L.strata_batch_run_noalloc(ctx, arr, len(spec), s.cuda_stream, 0)
+    assert rc == _lib.EINVAL
+    assert "capturing" in _lib.last_error()
+    del g
+    # the scratch still serves an ordinary call
+    _lib.check(L.strata_batch_run_noalloc(ctx, arr, len(spec), None, 1))
