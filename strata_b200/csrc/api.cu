@@ -983,16 +983,17 @@ extern "C" int strata_process(strata_ctx* c, const strata_stage* stages, int nst
         p.out_y0 = y0;
         p.out_y1 = y1;
         int64_t wc = 0;
-        int64_t t = strata::launch_data(p, st, &wc);
+        ValidityParams vp[2];
+        const ValidityParams* vs[2] = {nullptr, nullptr};
+        for (int i = 0; i < ndst; i++) {
+            if (!dst[i].valid) continue;
+            fill_validity(vp[i], ds, src[0].valid != nullptr, dd[i], span_cells(dst[i]), W, H, p.radius, y0, y1);
+            vs[i] = &vp[i];
+        }
+        int64_t t = strata::launch_stage(p, vs, st, &wc);
         if (t < 0) return fail(STRATA_ENOTSUP, "engine: op %d at radius %d has no device kernel", p.op, p.radius);
         bands += t;
         window += wc;
-        for (int i = 0; i < ndst; i++) {
-            if (!dst[i].valid) continue;
-            ValidityParams v;
-            fill_validity(v, ds, src[0].valid != nullptr, dd[i], span_cells(dst[i]), W, H, p.radius, y0, y1);
-            strata::launch_validity(v, st);
-        }
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
         if (cancel) {
@@ -1547,16 +1548,12 @@ extern "C" int strata_process_chunked(strata_ctx* c, const strata_stage* stages,
         q.height = H;
         q.status = c->d_status;
         int64_t wc = 0;
-        int64_t nt = strata::launch_data(q, st, &wc);
-        if (nt < 0) {
-            status = fail(STRATA_ENOTSUP, "engine: op %d at radius %d has no device kernel", p.op, p.radius);
-            break;
-        }
-        local.bands += nt;
-        local.kernel_read += wc * 4;
+        ValidityParams vp[2];
+        const ValidityParams* vs[2] = {nullptr, nullptr};
         for (int i = 0; i < ndst; i++) {
             if (!dst[i].masked) continue;
-            ValidityParams v;
+            ValidityParams& v = vp[i];
+            vs[i] = &v;
             memset(&v, 0, sizeof v);
             if (in_masked) {
                 v.src_bits = (const uint32_t*)s.d_in_bits.p;
@@ -1582,8 +1579,14 @@ extern "C" int strata_process_chunked(strata_ctx* c, const strata_stage* stages,
             int64_t oc = (y1 - y0 - 1) * s.out_stride[i] + (x1 - x0);
             v.dst_lo_word = 0;
             v.dst_words = (oc + 31) >> 5;
-            strata::launch_validity(v, st);
         }
+        int64_t nt = strata::launch_stage(q, vs, st, &wc);
+        if (nt < 0) {
+            status = fail(STRATA_ENOTSUP, "engine: op %d at radius %d has no device kernel", p.op, p.radius);
+            break;
+        }
+        local.bands += nt;
+        local.kernel_read += wc * 4;
         for (int i = 0; i < ndst && e == cudaSuccess; i++) {
             int64_t oc = (y1 - y0 - 1) * s.out_stride[i] + (x1 - x0);
             e = cudaMemcpyAsync(s.out_data[i].p, s.d_out_data[i].p, (size_t)oc * 4, cudaMemcpyDeviceToHost, st);
@@ -1709,19 +1712,21 @@ extern "C" int strata_process_features(strata_ctx* c, const strata_stage* stages
         p.out_y1 = H;
         p.status = c->d_status;
         int64_t wc = 0;
-        int64_t t = strata::launch_data(p, st, &wc);
+        ValidityParams vp[2];
+        const ValidityParams* vs[2] = {nullptr, nullptr};
+        for (int i = o; i < o + nouts[(size_t)f]; i++) {
+            if (!dst[i].valid) continue;
+            fill_validity(vp[i - o], ds, src[0].valid != nullptr, dd[(size_t)i], span_cells(dst[i]), W, H, p.radius,
+                          0, H);
+            vs[i - o] = &vp[i - o];
+        }
+        int64_t t = strata::launch_stage(p, vs, st, &wc);
         if (t < 0) {
             cleanup();
             return fail(STRATA_ENOTSUP, "engine: op %d at radius %d has no device kernel", p.op, p.radius);
         }
         bands += t;
         window += wc;
-        for (int i = o; i < o + nouts[(size_t)f]; i++) {
-            if (!dst[i].valid) continue;
-            ValidityParams v;
-            fill_validity(v, ds, src[0].valid != nullptr, dd[(size_t)i], span_cells(dst[i]), W, H, p.radius, 0, H);
-            strata::launch_validity(v, st);
-        }
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) {
             cleanup();

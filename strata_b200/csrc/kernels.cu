@@ -7,6 +7,8 @@
 // pointwise kernel below. Every kernel leaves the cells within the radius
 // of the raster's border NaN (internal/exec/halo.go:61-92); the validity of
 // the outputs is written by validity.cu.
+#include <cstring>
+
 #include "cellops.cuh"
 #include "launch.h"
 #include "ops3.cuh"
@@ -59,6 +61,40 @@ int64_t launch_data(const LaunchParams& p, cudaStream_t s, int64_t* window_cells
     }
     if (focal_eligible(p)) return launch_focal(p, s, window_cells);
     return -1;  // beyond the kernels' 32-bit index limits: the caller falls back to the CPU
+}
+
+int64_t launch_stage(LaunchParams p, const ValidityParams* const v[2], cudaStream_t s, int64_t* window_cells) {
+    memset(&p.vf, 0, sizeof p.vf);
+    const ValidityParams* any = v[0] ? v[0] : v[1];
+    bool fuse = any != nullptr && p.radius == 1 && march3_eligible(p);
+    for (int i = 0; i < 2 && fuse; i++) {
+        const ValidityParams* q = v[i];
+        if (!q) continue;
+        fuse = q->radius == 1 && q->src_bits == any->src_bits && q->src_off == any->src_off &&
+               q->src_stride == any->src_stride && q->src_x0 == p.src_x0 && q->src_y0 == p.src_y0 &&
+               q->dst_x0 == p.dst_x0 && q->dst_y0 == p.dst_y0 && q->out_x0 == p.out_x0 && q->out_x1 == p.out_x1 &&
+               q->out_y0 == p.out_y0 && q->out_y1 == p.out_y1 && q->width == p.width && q->height == p.height;
+    }
+    if (fuse) {
+        p.vf.src_bits = any->src_bits;
+        p.vf.src_off = any->src_off;
+        p.vf.src_stride = any->src_stride;
+        p.vf.src_lo_word = any->src_lo_word;
+        p.vf.src_hi_word = any->src_hi_word;
+        for (int i = 0; i < 2; i++) {
+            if (!v[i]) continue;
+            p.vf.dst_bits[i] = v[i]->dst_bits;
+            p.vf.dst_off[i] = v[i]->dst_off;
+            p.vf.dst_stride[i] = v[i]->dst_stride;
+            p.vf.n++;
+        }
+        return launch_data(p, s, window_cells);
+    }
+    const int64_t t = launch_data(p, s, window_cells);
+    if (t < 0) return t;
+    for (int i = 0; i < 2; i++)
+        if (v[i]) launch_validity(*v[i], s);
+    return t;
 }
 
 

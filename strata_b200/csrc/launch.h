@@ -44,6 +44,20 @@ struct EpiStage {
     float b[STRATA_MAX_KNOTS + 1];
 };
 
+// The output validity a radius-1 march writes beside its cells (n > 0):
+// the source mask (null: every source cell valid), whose cell (src_x0,
+// src_y0) of the launch is bit src_off, and each output's mask (null: the
+// output is unmasked), whose cell (dst_x0, dst_y0) is bit dst_off[i].
+struct FusedValidity {
+    const uint32_t* src_bits;
+    int64_t src_off, src_stride;
+    int64_t src_lo_word, src_hi_word;  // 32-bit words that hold the source's bits
+    uint32_t* dst_bits[2];
+    int64_t dst_off[2], dst_stride[2];
+    int n;
+    int pad_;
+};
+
 // Kernel parameters of one stage launch. Passed by value as a
 // __grid_constant__ parameter, so weights and tables sit in the constant
 // bank and every thread reads them through the broadcast path.
@@ -80,6 +94,7 @@ struct alignas(16) LaunchParams {
     float k[16];
     float w[kMaxWeights];  // CORRELATE weights (rotation applied); SEPARABLE row taps w[0..], column taps w[17..]
     EpiStage epi[kMaxEpilogue];
+    FusedValidity vf;  // set by launch_stage when the march writes the outputs' validity
 };
 
 // Validity of one output: bits of dst for the width x height raster,
@@ -167,6 +182,13 @@ int64_t launch_data(const LaunchParams& p, cudaStream_t stream, int64_t* window_
 
 // Launches the validity kernel for one output.
 void launch_validity(const ValidityParams& v, cudaStream_t stream);
+
+// Launches a stage and the validity of its masked outputs (v[i] for output
+// i, null when output i is unmasked). The radius-1 march on 16-byte aligned
+// rows writes the validity itself when every v[i] describes the launch's
+// own region and coordinates; otherwise the validity kernel runs after the
+// data kernel. Returns launch_data's count (-1: no kernel).
+int64_t launch_stage(LaunchParams p, const ValidityParams* const v[2], cudaStream_t stream, int64_t* window_cells);
 
 // The radius-1 marching kernel (march3.cu): whether it can run these
 // parameters (16-byte aligned rows at the region's first column, width a

@@ -92,6 +92,124 @@ __device__ __forceinline__ void store_row(const LaunchParams& P, Strip& S, const
 }
 
 // ---------------------------------------------------------------------------
+// Output validity written by the march (VAL kernels), so that no second
+// kernel walks the rows again: bit (x, y) of an output is the AND of the
+// source's bits over the 3x3 window at (x, y), cleared in the edge ring
+// (internal/stencil/mask.go:43-161, internal/exec/halo.go:213-229).
+//
+// At the start of its strip a warp copies the source words of every row
+// of the strip (the 130 bits of columns xs-1 .. xs+128, six 32-bit words a
+// row) into shared memory with 4-byte cp.async copies, all in flight at
+// once; they land while the warp marches the strip's cells. After the
+// march the warp writes the strip's validity in one short phase that holds
+// none of the march's registers: each lane owns the 32 cells xs+32j ..
+// xs+32j+31 (j = lane % 4) of 8 consecutive output rows, erodes each of
+// the 10 source rows they read across into one word (bit i: the AND of
+// columns x+i-1 .. x+i+1), and stores the AND of three of them with the
+// interior and region bits per output row. A destination word wholly the
+// lane's takes a plain store; words shared with other cells (another
+// lane's or warp's, another row's, another raster's) take atomics that
+// change only the lane's bits.
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ int64_t floor_div32_(int64_t b) { return b >= 0 ? b >> 5 : -((-b + 31) >> 5); }
+
+constexpr int kMaxStrip = 64;             // output rows of a warp's strip (the launchers cap it)
+constexpr int kVMaxRows = kMaxStrip + 2;  // source rows of a strip: its output rows and their halo rows
+constexpr int kVWords = 6;                // words holding a source row's 130 bits
+constexpr int kVRowsPerLane = kMaxStrip / 8;  // output rows a lane writes (8 lanes share a column word)
+
+// Sets the bits m of word w to those of val.
+__device__ __forceinline__ void put_word(uint32_t* w, uint32_t val, uint32_t m) {
+    if (m == 0xffffffffu) {
+        *w = val;
+    } else if (m) {
+        atomicAnd(w, ~m | val);
+        atomicOr(w, val & m);
+    }
+}
+
+// Bit of column xs - 1 of source row y0 - 1 (m = 0) of the warp's strip.
+__device__ __forceinline__ int64_t vbit0(const LaunchParams& P, int64_t xs, int64_t y0) {
+    return P.vf.src_off + (y0 - 1 - P.src_y0) * P.vf.src_stride + (xs - 1 - P.src_x0);
+}
+
+// Starts the copies of the source words of rows y0-1 .. y0+rows into w.
+__device__ __forceinline__ void valid_prefetch(const LaunchParams& P, int64_t xs, int64_t y0, int rows, uint32_t* w,
+                                               int lane) {
+    if (!P.vf.src_bits) return;
+    const int64_t bit0 = vbit0(P, xs, y0);
+    const int row0 = (int)(y0 - 1 - P.src_y0);
+    const int n = (rows + 2) * kVWords;
+    for (int i = lane; i < n; i += 32) {
+        const int m = i / kVWords, j = i - m * kVWords;
+        const int64_t k = floor_div32_(bit0 + (int64_t)m * P.vf.src_stride) + j;
+        uint32_t* d = w + i;
+        if ((unsigned)(row0 + m) < (unsigned)P.src_h && k >= P.vf.src_lo_word && k <= P.vf.src_hi_word)
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_addr(d)), "l"(P.vf.src_bits + k)
+                         : "memory");
+        else
+            *d = 0u;
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+// Waits for the copies (on every path, so none outlives the block).
+__device__ __forceinline__ void valid_wait(const LaunchParams& P) {
+    if (!P.vf.src_bits) return;
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    __syncwarp();
+}
+
+// The strip's validity: output rows y0 .. y0+rows-1 of columns xs ..
+// xs+127 (clipped to the region), from the words valid_prefetch copied.
+__device__ __forceinline__ void valid_strip(const LaunchParams& P, int64_t xs, int64_t y0, int rows,
+                                            const uint32_t* w, int lane) {
+    const int j = lane & 3, k0 = (lane >> 2) * kVRowsPerLane;
+    if (k0 >= rows) return;
+    const int64_t c0 = xs + 32 * j;
+    // cells c0 + i with 1 <= c0 + i < W - 1 (the edge ring's columns) and c0 + i < out_x1
+    const int64_t lo = 1 - c0, hi = (P.width - 1 < P.out_x1 ? P.width - 1 : P.out_x1) - c0;
+    const uint32_t keep = (lo <= 0 ? 0xffffffffu : (lo >= 32 ? 0u : ~((1u << lo) - 1u))) &
+                          (hi >= 32 ? 0xffffffffu : (hi <= 0 ? 0u : ((1u << hi) - 1u)));
+    const int64_t nreg = P.out_x1 - c0;
+    const uint32_t ours = nreg >= 32 ? 0xffffffffu : (nreg <= 0 ? 0u : ((1u << nreg) - 1u));
+    const int b31 = (int)(vbit0(P, xs, y0) & 31), s31 = (int)(P.vf.src_stride & 31);
+    auto eroded = [&](int m) -> uint32_t {
+        if (!P.vf.src_bits) return 0xffffffffu;
+        const int sh = (b31 + m * s31) & 31;
+        const uint32_t* r = w + m * kVWords + j;
+        const uint64_t x = (uint64_t)__funnelshift_r(r[0], r[1], sh) | ((uint64_t)__funnelshift_r(r[1], r[2], sh) << 32);
+        return (uint32_t)(x & (x >> 1) & (x >> 2));
+    };
+    uint32_t a = eroded(k0), b = eroded(k0 + 1);
+    const int kend = min(k0 + kVRowsPerLane, rows);
+    for (int k = k0; k < kend; k++) {
+        const uint32_t c = eroded(k + 2);
+        const int64_t y = y0 + k;
+        const uint32_t v = (y >= 1 && y < P.height - 1) ? (a & b & c & keep) : 0u;
+        a = b;
+        b = c;
+#pragma unroll
+        for (int i = 0; i < 2; i++) {
+            if (!P.vf.dst_bits[i]) continue;
+            const int64_t D = P.vf.dst_off[i] + (y - P.dst_y0) * P.vf.dst_stride[i] + (c0 - P.dst_x0);
+            const int64_t wb = D >> 5;
+            const int sh = (int)(D & 31);
+            if (sh == 0) {
+                put_word(P.vf.dst_bits[i] + wb, v, ours);
+            } else {
+                put_word(P.vf.dst_bits[i] + wb, v << sh, ours << sh);
+                put_word(P.vf.dst_bits[i] + wb + 1, v >> (32 - sh), ours >> (32 - sh));
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Loads straight into registers.
 
 struct Lane {
@@ -123,7 +241,7 @@ __device__ __forceinline__ Row6 load_row(Lane& L) {
 
 constexpr int kRing = 4;  // three window rows and one in flight
 
-template <int OP, int KIND, bool EPI>
+template <int OP, int KIND, bool EPI, bool VAL>
 __global__ void __launch_bounds__(kWarps * 32, 6) march3_kernel(const __grid_constant__ LaunchParams P, int strip,
                                                                  int col_blocks) {
     constexpr bool kHorn = kIsHorn<OP>;
@@ -147,9 +265,12 @@ __global__ void __launch_bounds__(kWarps * 32, 6) march3_kernel(const __grid_con
     const int rows = S.rows;
 
     // Ring slot m % kRing holds row y0 - 1 + m; output row y0 + k reads
-    // m = k .. k + 2, and row k + 3 loads while row k computes.
+    // m = k .. k + 2, and row k + 3 loads while row k computes. The
+    // validity ring (VAL) has the same slots and loads four rows ahead.
     Row6 ring[kRing];
     float hr[kRing][4];
+    __shared__ uint32_t vwords[VAL ? kWarps : 1][VAL ? kVMaxRows * kVWords : 1];
+    if constexpr (VAL) valid_prefetch(P, S.xs, S.y0, rows, vwords[threadIdx.x >> 5], S.lane);
 #pragma unroll
     for (int j = 0; j < 3; j++) {
         ring[j] = load_row(L);
@@ -172,6 +293,10 @@ __global__ void __launch_bounds__(kWarps * 32, 6) march3_kernel(const __grid_con
                                        o0, o1);
             store_row<OP>(P, S, o0, o1);
         }
+    }
+    if constexpr (VAL) {
+        valid_wait(P);
+        valid_strip(P, S.xs, S.y0, rows, vwords[threadIdx.x >> 5], S.lane);
     }
 }
 
@@ -234,7 +359,7 @@ __device__ __forceinline__ void tma_box(void* dst, const CUtensorMap* map, int x
         : "memory");
 }
 
-template <int OP, int KIND, bool EPI>
+template <int OP, int KIND, bool EPI, bool VAL>
 __global__ void __launch_bounds__(kWarps * 32, 6)
     march3_tma_kernel(const __grid_constant__ LaunchParams P, const __grid_constant__ CUtensorMap map, int strip,
                       int col_blocks) {
@@ -314,9 +439,12 @@ __global__ void __launch_bounds__(kWarps * 32, 6)
     };
 
     // Register slot m % 4 holds row m: output row k reads m = k .. k + 2
-    // and takes row k + 2; unrolled by 4, every index is a constant.
+    // and takes row k + 2; unrolled by 4, every index is a constant. The
+    // validity ring (VAL) has the same slots and loads four rows ahead.
     Row6 ring[4];
     float hr[4][4];
+    __shared__ uint32_t vwords[VAL ? kWarps : 1][VAL ? kVMaxRows * kVWords : 1];
+    if constexpr (VAL) valid_prefetch(P, S.xs, S.y0, rows, vwords[warp], lane);
     if (ok) {
         take(0, ring[0]);
         take(1, ring[1]);
@@ -339,6 +467,10 @@ __global__ void __launch_bounds__(kWarps * 32, 6)
                                        hr[(u + 1) % 4], hr[(u + 2) % 4], rowin, S.colin, o0, o1);
             if (ok) store_row<OP>(P, S, o0, o1);
         }
+    }
+    if constexpr (VAL) {  // waited for on every path, so no copy outlives the block
+        valid_wait(P);
+        if (ok) valid_strip(P, S.xs, S.y0, rows, vwords[warp], lane);
     }
     if (!ok) {
         // A copy did not land in time: report it, then wait (bounded) for
@@ -381,24 +513,30 @@ bool source_map(const LaunchParams& p, CUtensorMap* map) {
 
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
 
-template <int OP, int KIND, bool EPI>
-int64_t launch_march(const LaunchParams& p, cudaStream_t s) {
+template <int OP, int KIND, bool EPI, bool VAL>
+int64_t launch_march_v(const LaunchParams& p, cudaStream_t s) {
     const int64_t w = p.out_x1 - p.out_x0, h = p.out_y1 - p.out_y0;
     const int64_t segs = (w + 127) / 128;
     const int64_t col_blocks = (segs + kWarps - 1) / kWarps;
     // Strip height: enough warps for several waves over the SMs, at least
     // 8 rows and at most 64 (the halo costs 2 rows a strip).
     int64_t strip = segs > 0 ? (h * segs) / ((int64_t)sm_count() * 48 * 4) : h;
-    strip = strip < 8 ? 8 : (strip > 64 ? 64 : strip);
+    strip = strip < 8 ? 8 : (strip > kMaxStrip ? kMaxStrip : strip);
     const int64_t strips = (h + strip - 1) / strip;
     const int64_t blocks = col_blocks * strips;
     CUtensorMap map;
     if (source_map(p, &map))
-        march3_tma_kernel<OP, KIND, EPI><<<(unsigned)blocks, kWarps * 32, 0, s>>>(p, map, (int)strip,
-                                                                                 (int)col_blocks);
+        march3_tma_kernel<OP, KIND, EPI, VAL><<<(unsigned)blocks, kWarps * 32, 0, s>>>(p, map, (int)strip,
+                                                                                      (int)col_blocks);
     else
-        march3_kernel<OP, KIND, EPI><<<(unsigned)blocks, kWarps * 32, 0, s>>>(p, (int)strip, (int)col_blocks);
+        march3_kernel<OP, KIND, EPI, VAL><<<(unsigned)blocks, kWarps * 32, 0, s>>>(p, (int)strip,
+                                                                                  (int)col_blocks);
     return blocks;
+}
+
+template <int OP, int KIND, bool EPI>
+int64_t launch_march(const LaunchParams& p, cudaStream_t s) {
+    return p.vf.n ? launch_march_v<OP, KIND, EPI, true>(p, s) : launch_march_v<OP, KIND, EPI, false>(p, s);
 }
 
 template <int OP, int KIND>
@@ -434,7 +572,7 @@ int64_t launch_any(const LaunchParams& p, cudaStream_t s) {
     const int64_t segs = (w + 127) / 128;
     const int64_t col_blocks = (segs + kWarps - 1) / kWarps;
     int64_t strip = segs > 0 ? (h * segs) / ((int64_t)sm_count() * 48 * 4) : h;
-    strip = strip < 8 ? 8 : (strip > 64 ? 64 : strip);
+    strip = strip < 8 ? 8 : (strip > kMaxStrip ? kMaxStrip : strip);
     const int64_t blocks = col_blocks * ((h + strip - 1) / strip);
     march_any_kernel<OP, KIND, EPI><<<(unsigned)blocks, kWarps * 32, 0, s>>>(p, (int)strip, (int)col_blocks);
     return blocks;
