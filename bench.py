@@ -67,39 +67,98 @@ def hbm_peak():
 # ---------------------------------------------------------------------------
 # Workloads: (name, stage-list factory, outputs) per op, and the input.
 
-def terrain_ops(cell_size):
-    from strata_b200 import terrain, transfer
+def _synth():
+    """The synthetic-input generators (strata_b200/synth.py, numpy only),
+    loaded by file so that the reference arm never imports the device
+    package or maps its library."""
+    import importlib.util
 
-    o = dict(CellSize=cell_size)
+    spec = importlib.util.spec_from_file_location("strata_synth", os.path.join(ROOT, "strata_b200", "synth.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def _orc():
+    from oracle import oracle as orc
+
+    return orc
+
+
+# Each op of a workload: (name, device stages factory, oracle stages factory,
+# outputs). The oracle factories resolve the same options with the oracle's
+# own code (oracle/oracle.py), so the CPU legs load no device library.
+
+def terrain_ops(cell_size):
+    cs = cell_size
+
+    def dev(fn):
+        def mk():
+            from strata_b200 import terrain, transfer  # noqa: F401
+
+            return fn(terrain, transfer)
+        return mk
+
+    o = dict(CellSize=cs)
     return [
-        ("gradient", lambda: terrain.gradient_stage(terrain.GradientOptions(**o)), 2),
-        ("slope", lambda: terrain.slope_stage(terrain.SlopeOptions(**o)), 1),
-        ("aspect", lambda: terrain.aspect_stage(terrain.AspectOptions(**o)), 1),
-        ("hillshade", lambda: terrain.hillshade_stage(terrain.HillshadeOptions(Azimuth=315, Altitude=45,
-                                                                               ZFactor=1, **o)), 1),
-        ("curvature_profile", lambda: terrain.curvature_stage(terrain.CurvatureOptions(Type=0, **o)), 1),
-        ("curvature_plan", lambda: terrain.curvature_stage(terrain.CurvatureOptions(Type=1, **o)), 1),
-        ("curvature_mean", lambda: terrain.curvature_stage(terrain.CurvatureOptions(Type=2, **o)), 1),
-        ("tri", lambda: terrain.ruggedness_stage(terrain.RuggednessOptions(Type=0, Radius=1)), 1),
-        ("tpi", lambda: terrain.ruggedness_stage(terrain.RuggednessOptions(Type=2, Radius=1)), 1),
-        ("roughness", lambda: terrain.ruggedness_stage(terrain.RuggednessOptions(Type=3, Radius=1)), 1),
-        ("slope_lookup_reclass", lambda: terrain.slope_stage(terrain.SlopeOptions(**o))
-         .extend(transfer.lookup_stage(SLOPE_XS, SLOPE_YS)).extend(transfer.reclass_stage(BREAKS, VALUES)), 1),
+        ("gradient", dev(lambda t, _x: t.gradient_stage(t.GradientOptions(**o))),
+         lambda: [_orc().gradient_stage(cs)], 2),
+        ("slope", dev(lambda t, _x: t.slope_stage(t.SlopeOptions(**o))), lambda: [_orc().slope_stage(cs)], 1),
+        ("aspect", dev(lambda t, _x: t.aspect_stage(t.AspectOptions(**o))), lambda: [_orc().aspect_stage(cs)], 1),
+        ("hillshade", dev(lambda t, _x: t.hillshade_stage(t.HillshadeOptions(Azimuth=315, Altitude=45, ZFactor=1, **o))),
+         lambda: [_orc().hillshade_stage(cs, azimuth=315, altitude=45)], 1),
+        ("curvature_profile", dev(lambda t, _x: t.curvature_stage(t.CurvatureOptions(Type=0, **o))),
+         lambda: [_orc().curvature_stage(cs, kind=0)], 1),
+        ("curvature_plan", dev(lambda t, _x: t.curvature_stage(t.CurvatureOptions(Type=1, **o))),
+         lambda: [_orc().curvature_stage(cs, kind=1)], 1),
+        ("curvature_mean", dev(lambda t, _x: t.curvature_stage(t.CurvatureOptions(Type=2, **o))),
+         lambda: [_orc().curvature_stage(cs, kind=2)], 1),
+        ("tri", dev(lambda t, _x: t.ruggedness_stage(t.RuggednessOptions(Type=0, Radius=1))),
+         lambda: [_orc().ruggedness_stage(0, 1)], 1),
+        ("tpi", dev(lambda t, _x: t.ruggedness_stage(t.RuggednessOptions(Type=2, Radius=1))),
+         lambda: [_orc().ruggedness_stage(2, 1)], 1),
+        ("roughness", dev(lambda t, _x: t.ruggedness_stage(t.RuggednessOptions(Type=3, Radius=1))),
+         lambda: [_orc().ruggedness_stage(3, 1)], 1),
+        ("slope_lookup_reclass",
+         dev(lambda t, x: t.slope_stage(t.SlopeOptions(**o)).extend(x.lookup_stage(SLOPE_XS, SLOPE_YS))
+             .extend(x.reclass_stage(BREAKS, VALUES))),
+         lambda: [_orc().slope_stage(cs), _orc().lookup_stage(SLOPE_XS, SLOPE_YS), _orc().reclass_stage(BREAKS, VALUES)],
+         1),
     ]
 
 
 def focal_ops():
-    from strata_b200 import engine, focal, synth
-
+    synth = _synth()
     ops = []
     for r in range(1, 9):
         w = synth.uniform_weights((2 * r + 1) ** 2, 0x5EED0003 + r)
-        ops.append((f"correlate_r{r}", lambda w=w, r=r: focal.weights_stage(focal.WeightsOptions(r, w), False), 1))
-    g = focal.Gaussian(8, 2.5)
-    ops.append(("gaussian_r8", lambda: focal.separable_stage(focal.SeparableOptions(8, g, g)), 1))
+
+        def dev(w=w, r=r):
+            from strata_b200 import focal
+
+            return focal.weights_stage(focal.WeightsOptions(r, w), False)
+
+        ops.append((f"correlate_r{r}", dev, lambda w=w, r=r: [_orc().stage(_orc().CORRELATE, r, 0, (), [w])], 1))
+
+    def gdev():
+        from strata_b200 import focal
+
+        g = focal.Gaussian(8, 2.5)
+        return focal.separable_stage(focal.SeparableOptions(8, g, g))
+
+    def gorc():
+        g = _orc().gaussian(8, 2.5)
+        return [_orc().stage(_orc().SEPARABLE, 8, 0, (), [g, g])]
+
+    ops.append(("gaussian_r8", gdev, gorc, 1))
     for r in (3, 8):
-        for name, op in (("mean", engine._lib.OP_MEAN), ("min", engine._lib.OP_MIN), ("max", engine._lib.OP_MAX)):
-            ops.append((f"{name}_r{r}", lambda r=r, op=op: focal.box_stage(focal.BoxOptions(r), op), 1))
+        for name, code in (("mean", 9), ("min", 10), ("max", 11)):
+            def dev(r=r, code=code):
+                from strata_b200 import focal
+
+                return focal.box_stage(focal.BoxOptions(r), code)
+
+            ops.append((f"{name}_r{r}", dev, lambda r=r, code=code: [_orc().stage(code, r)], 1))
     return ops
 
 
@@ -116,43 +175,37 @@ def workload(name, side=None, only=None):
 
 
 def _workload(name, side=None):
-    from strata_b200 import synth
+    synth = _synth()
+
+    def slope_op(cs):
+        def dev():
+            from strata_b200 import terrain
+
+            return terrain.slope_stage(terrain.SlopeOptions(CellSize=cs))
+        return [("slope", dev, lambda: [_orc().slope_stage(cs)], 1)]
 
     if name == "terrain16k":
         n, seed, cs = side or 16384, 0x5EED0002, 10
         cells = synth.fbm_dem(n, n, seed)
         valid = synth.block_mask(n, n, seed, 0.02)
         return dict(name=f"terrain set on {n}x{n} f32 DEM", width=n, height=n, cells=cells, valid=valid,
-                    ops=terrain_ops(cs), cell_size=cs, mask="2% NoData in 8x8 blocks")
-    if name == "slope2k":
-        n, seed, cs = side or 2048, 0x5EED0001, 30
-        from strata_b200 import terrain
-
+                    ops=terrain_ops(cs), cell_size=cs, mask="2% NoData in 8x8 blocks", radius=1)
+    if name in ("slope2k", "slope8k"):
+        n, seed, cs = side or (2048 if name == "slope2k" else 8192), 0x5EED0001, 30
         return dict(name=f"Slope on {n}x{n} f32 DEM", width=n, height=n, cells=synth.fbm_dem(n, n, seed),
                     valid=synth.block_mask(n, n, seed, 0.02), cell_size=cs, mask="2% NoData in 8x8 blocks",
-                    ops=[("slope", lambda: terrain.slope_stage(terrain.SlopeOptions(CellSize=cs)), 1)])
-    if name == "slope8k":
-        n, seed, cs = side or 8192, 0x5EED0001, 30
-        from strata_b200 import terrain
-
-        return dict(name=f"Slope on {n}x{n} f32 DEM", width=n, height=n, cells=synth.fbm_dem(n, n, seed),
-                    valid=synth.block_mask(n, n, seed, 0.02), cell_size=cs, mask="2% NoData in 8x8 blocks",
-                    ops=[("slope", lambda: terrain.slope_stage(terrain.SlopeOptions(CellSize=cs)), 1)])
+                    ops=slope_op(cs), radius=1)
     if name == "pipeline8k":
         n, seed, cs = side or 8192, 0x5EED0002, 10
-        from strata_b200 import terrain, transfer
-
+        ops = [o for o in terrain_ops(cs) if o[0] == "slope_lookup_reclass"]
         return dict(name=f"Slope->Lookup->Reclass on {n}x{n} f32 DEM", width=n, height=n,
                     cells=synth.fbm_dem(n, n, seed), valid=synth.block_mask(n, n, seed, 0.02), cell_size=cs,
-                    mask="2% NoData in 8x8 blocks",
-                    ops=[("slope_lookup_reclass", lambda: terrain.slope_stage(terrain.SlopeOptions(CellSize=cs))
-                          .extend(transfer.lookup_stage(SLOPE_XS, SLOPE_YS))
-                          .extend(transfer.reclass_stage(BREAKS, VALUES)), 1)])
+                    mask="2% NoData in 8x8 blocks", ops=ops, radius=1)
     if name == "focal8k":
         n, seed = side or 8192, 0x5EED0003
         return dict(name=f"focal ops on {n}x{n} f32 raster", width=n, height=n, cells=synth.normal_trend(n, n, seed),
                     valid=synth.cell_mask(n, n, seed, 0.05), ops=focal_ops(), cell_size=None,
-                    mask="5% random NoData cells")
+                    mask="5% random NoData cells", radius=8)
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -215,32 +268,99 @@ class Clocks:
 
 
 # ---------------------------------------------------------------------------
-# The CPU leg: the oracle on a row band.
+# The CPU legs, on the oracle only (oracle/: the scalar restatement of the
+# reference's kernels and, with simd, the restated AVX2 lanes of the
+# reference's internal/stencil/simd_amd64.go).
 
-def cpu_run(wl, rows, nthreads, reps=1):
-    """Runs every op of the workload with the oracle over the first `rows`
-    rows of the input; returns (cells processed, seconds)."""
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    from helpers import host_raster, like, run_oracle
+def _band(wl, y0, y1):
+    """Rows [y0, y1) of the workload's input as an oracle raster (a raster
+    of its own: its first and last rows are its edge ring)."""
+    orc = _orc()
+    W = wl["width"]
+    cells = np.ascontiguousarray(wl["cells"][y0:y1])
+    valid = wl["valid"][y0:y1] if wl["valid"] is not None else None
+    return dict(data=cells.reshape(-1), width=W, height=y1 - y0, stride=W,
+                valid=orc.pack_mask(valid) if valid is not None else None, valid_offset=0)
 
-    src = host_raster(np.ascontiguousarray(wl["cells"][:rows]), wl["valid"][:rows])
-    outs = [like(src), like(src)]
+
+def _outs(src, n):
+    cells = src["width"] * src["height"]
+    return [dict(data=np.empty(cells, np.float32), width=src["width"], height=src["height"], stride=src["width"],
+                 valid=np.zeros((cells + 63) // 64, np.uint64) if src["valid"] is not None else None, valid_offset=0)
+            for _ in range(n)]
+
+
+def cpu_run(wl, src, nthreads, simd, reps=1):
+    """Every op of the workload with the oracle over the raster src;
+    returns (output cells, seconds)."""
+    orc = _orc()
+    outs = _outs(src, 2)
+    stages = [(mk(), nout) for _n, _d, mk, nout in wl["ops"]]
     total, t0 = 0, time.perf_counter()
     for _ in range(reps):
-        for _name, mk, nout in wl["ops"]:
-            run_oracle(mk(), src, outs[:nout], nthreads=nthreads)
-            total += src.width * src.height
+        for st, nout in stages:
+            orc.process(st, src, outs[:nout], nthreads, simd=simd)
+            total += src["width"] * src["height"]
     return total, time.perf_counter() - t0
 
 
-def cpu_baseline(wl, target_s=10.0):
+def cpu_baseline(wl, target_s=12.0):
+    """The restated AVX2 path on every host core over a bounded row band of
+    the workload (every op of the set), and the scalar oracle on one
+    thread beside it."""
     threads = os.cpu_count() or 1
-    rows = min(wl["height"], max(64, (1 << 22) // wl["width"]))
-    cells, secs = cpu_run(wl, rows, threads)
+    rows = min(wl["height"], max(64, (1 << 24) // wl["width"]))
+    src = _band(wl, 0, rows)
+    cells, secs = cpu_run(wl, src, threads, True)
     reps = max(1, int(target_s / max(secs, 1e-3)))
-    cells, secs = cpu_run(wl, rows, threads, reps)
-    return {"value": cells / secs / 1e6, "unit": "Mcells/s", "cores": threads, "kind": "port",
-            "sample": f"{rows} rows x {wl['width']} cells, every op of the set, {reps} pass(es), {secs:.1f} s"}
+    cells, secs = cpu_run(wl, src, threads, True, reps)
+    srows = max(8, rows // 16)
+    s1 = _band(wl, 0, srows)
+    c1, t1 = cpu_run(wl, s1, 1, False)
+    return {"value": round(cells / secs / 1e6, 1), "unit": "Mcells/s", "cores": threads, "kind": "restated-avx2",
+            "sample": f"{rows} rows x {wl['width']} cells of the workload, every op of the set, {reps} pass(es), "
+                      f"{secs:.1f} s; AVX2 lanes after internal/stencil/simd_amd64.go (radius-1 stencils), "
+                      f"the scalar kernels elsewhere",
+            "scalar_1thread": {"value": round(c1 / t1 / 1e6, 1), "unit": "Mcells/s", "cores": 1,
+                               "sample": f"{srows} rows x {wl['width']} cells, every op, scalar oracle"}}
+
+
+def parity_check(wl, fetch):
+    """The device's outputs against the oracle on two row bands of the
+    workload (its first rows, with the raster's top edge, and rows in the
+    middle): fetch(i, y0, y1) returns op i's output rows [y0, y1) as (data
+    rows, validity rows as bools or None), for each output. Each band runs
+    through the oracle as a raster of its own, so the band's interior rows
+    (the radius in from a band edge that is not the raster's) are compared,
+    every cell (rastertest.SameFloat: same bits, or both NaN) and every
+    validity bit."""
+    orc = _orc()
+    H, W, r = wl["height"], wl["width"], wl["radius"]
+    band = min(H, 64 + 2 * r)
+    mid = max(0, H // 2 - band // 2)
+    checked = cells = bad = vbad = 0
+    for i, (_name, _dev, mk, nout) in enumerate(wl["ops"]):
+        for y0 in sorted({0, mid}):
+            y1 = min(H, y0 + band)
+            src = _band(wl, y0, y1)
+            want = _outs(src, nout)
+            orc.process(mk(), src, want, os.cpu_count() or 1, simd=False)
+            lo = 0 if y0 == 0 else r
+            hi = (y1 - y0) if y1 == H else (y1 - y0) - r
+            got = fetch(i, y0, y1)
+            for k in range(nout):
+                g = got[k][0][lo:hi]
+                w = want[k]["data"].reshape(y1 - y0, W)[lo:hi]
+                same = (g.view(np.uint32) == w.view(np.uint32)) | (np.isnan(g) & np.isnan(w))
+                bad += int((~same).sum())
+                cells += same.size
+                if want[k]["valid"] is not None:
+                    wv = np.unpackbits(want[k]["valid"].view(np.uint8), bitorder="little")[:(y1 - y0) * W]
+                    wv = wv.reshape(y1 - y0, W)[lo:hi].astype(bool)
+                    vbad += int((got[k][1][lo:hi] != wv).sum())
+        checked += 1
+    return {"ops_checked": checked, "cells": cells, "mismatches": bad, "validity_mismatches": vbad,
+            "bands": f"rows 0..{band} and {mid}..{mid + band}, interior rows compared", "oracle": "scalar"}
 
 
 # ---------------------------------------------------------------------------
@@ -266,7 +386,7 @@ def run_ours(args, rank, world, local_rank):
                           torch.empty(words, dtype=torch.int64, device=dev), 0) for _ in range(2)]
     stream = torch.cuda.Stream(dev)
     opts = engine.Options(Stream=stream, Async=True, Device=local_rank)
-    ops = [(name, mk(), nout) for name, mk, nout in wl["ops"]]
+    ops = [(name, dev(), nout) for name, dev, _mk, nout in wl["ops"]]
 
     def step(events=None):
         for i, (name, stages, nout) in enumerate(ops):
@@ -371,7 +491,27 @@ def run_ours(args, rank, world, local_rank):
            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": round(e2e_s * 1e3, 2),
            "api": "engine.process_features (terrain.Features) over every op, host rasters"}
 
-    launches_per_step = sum(1 + (nout if masked else 0) for _n, _s, nout in ops)
+    # Parity at the benchmarked size: each op once more, its output rows of
+    # two bands against the oracle on the same rows.
+    state = {"op": -1}
+
+    def fetch(i, y0, y1):
+        if state["op"] != i:
+            assert engine.process(ops[i][1], outs[:ops[i][2]], [src], opts) is None
+            torch.cuda.synchronize()
+            state["op"] = i
+        res = []
+        for k in range(ops[i][2]):
+            d = outs[k].data[y0 * W:y1 * W].cpu().numpy().reshape(y1 - y0, W)
+            b0, b1 = y0 * W, y1 * W
+            words = outs[k].valid[b0 // 64:(b1 + 63) // 64].cpu().numpy().view(np.uint8)
+            bits = np.unpackbits(words, bitorder="little")[b0 - (b0 // 64) * 64:][:b1 - b0]
+            res.append((d, bits.reshape(y1 - y0, W).astype(bool)))
+        return res
+
+    parity = parity_check(wl, fetch) if rank == 0 else None
+
+    launches_per_step = len(ops)  # one kernel per op: the march writes the validity beside the cells
     line = {
         "metric": "Mcells/s (output cells of every op in the set per second)", "value": round(value, 1),
         "unit": "Mcells/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -381,12 +521,11 @@ def run_ours(args, rank, world, local_rank):
                    "ops": [o[0] for o in ops], "mask": wl["mask"], "l2": "inputs larger than L2 (no flush)",
                    "parallelism": f"independent rasters x{world}"},
         "roofline": roofline, "e2e": e2e, "gpu_launches": launches_per_step * args.steps,
-        "clocks": clk.summary(), "per_op": per,
+        "clocks": clk.summary(), "per_op": per, "parity": parity,
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(wl)
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+    return line
 
 
 def batch_rasters(seed=0x5EED0004, count=512):
@@ -472,6 +611,27 @@ def run_batch(args, rank, world, local_rank):
     torch.cuda.synchronize()
     plain_ms = (time.perf_counter() - t0) / args.steps * 1e3
     st, classes = b.stats()
+    # Parity: a sample of the batch's rasters (every 32nd, up to 2^20 cells
+    # each) against the oracle on the same raster, every cell and bit.
+    orc = _orc()
+    pbad = pv = pcells = pn = 0
+    for i in range(0, len(items), 32):
+        name, stg, c, v = rasters[i]
+        h, w = c.shape
+        if w * h > (1 << 20):
+            continue
+        src = dict(data=np.ascontiguousarray(c.reshape(-1)), width=w, height=h, stride=w,
+                   valid=orc.pack_mask(v), valid_offset=0)
+        want = _outs(src, 1)
+        orc.process([_orc_of(x) for x in stg.stages], src, want, os.cpu_count() or 1)
+        g = items[i].dst[0].data.cpu().numpy()
+        wv = np.unpackbits(want[0]["valid"].view(np.uint8), bitorder="little")[:w * h].astype(bool)
+        gv = np.unpackbits(items[i].dst[0].valid.cpu().numpy().view(np.uint8), bitorder="little")[:w * h].astype(bool)
+        same = (g.view(np.uint32) == want[0]["data"].view(np.uint32)) | (np.isnan(g) & np.isnan(want[0]["data"]))
+        pbad += int((~same).sum())
+        pv += int((gv != wv).sum())
+        pcells += w * h
+        pn += 1
     value = world * cells / (ms / 1e3) / 1e6
     plain = world * cells / (plain_ms / 1e3) / 1e6
     peak, peak_kind = hbm_peak()
@@ -489,10 +649,11 @@ def run_batch(args, rank, world, local_rank):
                      "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": round(alg / (ms / 1e3) / 1e9 / peak, 4), "traffic": None},
         "gpu_launches": classes * args.steps, "clocks": clk.summary(),
+        "parity": {"rasters_checked": pn, "cells": pcells, "mismatches": pbad, "validity_mismatches": pv,
+                   "sample": "every 32nd raster of at most 2^20 cells, against the scalar oracle"},
     }
     b.close()
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+    return line
 
 
 def serve_mosaic(n, seed, dev):
@@ -682,31 +843,78 @@ def run_serve(args, rank, world, local_rank):
         "served_over_plain": round(capacity / plain_rate, 2),
         "server": st, "clocks": clk.summary(),
     }
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+    return line
+
+
+def _orc_of(st):
+    """The oracle stage equal to one device stage (its op, radius, kind,
+    constants and tables)."""
+    import ctypes
+
+    tables = []
+    for i in range(4):
+        n = st.table_len[i]
+        tables.append(np.ctypeslib.as_array((ctypes.c_float * n).from_address(st.table[i])).copy()
+                      if st.table[i] and n > 0 else np.zeros(0, np.float32))
+    while tables and tables[-1].size == 0:
+        tables.pop()
+    return _orc().stage(st.op, st.radius, st.kind, list(st.k), tables)
+
+
+def _summary(line, keys):
+    return {k: line[k] for k in keys if k in line}
+
+
+def run_default(args, rank, world, local_rank):
+    """The headline workload (the terrain set on 16384 x 16384) and, on one
+    GPU, the other configurations' own figures beside it: the focal set on
+    8192 x 8192 (per op, roofline and parity), the batched form (512
+    rasters, batched over plain) and the served form (40000 x 40000
+    mosaic, served over plain, p50 / p99 latency)."""
+    import copy
+
+    line = run_ours(args, rank, world, local_rank)
+    if world == 1 and not args.no_extra and args.workload == "terrain16k" and not args.side and not args.ops:
+        sub = copy.copy(args)
+        sub.no_cpu = True
+        sub.workload = "focal8k"
+        f = run_ours(sub, rank, world, local_rank)
+        line["focal8k"] = _summary(f, ["config", "value", "unit", "ms_per_step", "roofline", "per_op", "parity", "e2e"])
+        sub.workload = "batch512"
+        b = run_batch(sub, rank, world, local_rank)
+        line["batch512"] = _summary(b, ["config", "value", "unit", "ms_per_step", "plain_launches",
+                                        "batched_over_plain", "roofline", "parity"])
+        sub.workload = "serve40k"
+        v = run_serve(sub, rank, world, local_rank)
+        line["serve40k"] = _summary(v, ["config", "value", "unit", "latency_ms", "plain_launches",
+                                        "served_over_plain", "server"])
+    return line
 
 
 def run_reference(args):
+    """The reference's CPU implementation of the path, timed on the host:
+    the reference (Go) cannot be built here, so this is its restatement,
+    the AVX2 lanes of internal/stencil/simd_amd64.go (radius-1 stencils;
+    the scalar kernels for the rest) in the reference's engine structure
+    (bands of 2^16 cells, word-level validity), on every host thread, over
+    the whole workload each step. It loads the oracle only."""
     wl = workload(args.workload, args.side, args.ops)
     threads = os.cpu_count() or 1
-    rows = min(wl["height"], max(64, (1 << 22) // wl["width"]))
+    src = _band(wl, 0, wl["height"])
     for _ in range(args.warmup):
-        cpu_run(wl, rows, threads)
-    cells, secs = 0, 0.0
-    for _ in range(args.steps):
-        c, s = cpu_run(wl, rows, threads)
-        cells += c
-        secs += s
+        cpu_run(wl, src, threads, True)
+    cells, secs = cpu_run(wl, src, threads, True, args.steps)
     value = cells / secs / 1e6
     line = {
         "impl": "reference", "metric": "Mcells/s (output cells of every op in the set per second)",
         "value": round(value, 1), "unit": "Mcells/s", "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(secs / args.steps * 1e3, 2), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": wl["name"], "width": wl["width"], "height": wl["height"],
+        "config": {"workload": wl["name"], "width": wl["width"], "height": wl["height"], "cell_size": wl["cell_size"],
                    "ops": [o[0] for o in wl["ops"]], "mask": wl["mask"]},
-        "cpu_baseline": {"value": round(value, 1), "unit": "Mcells/s", "cores": threads, "kind": "port",
-                         "sample": f"{rows} rows x {wl['width']} cells of the workload, every op, per step"},
+        "cpu_baseline": {"value": round(value, 1), "unit": "Mcells/s", "cores": threads, "kind": "restated-avx2",
+                         "sample": f"the whole workload ({wl['width']}x{wl['height']}, every op) per step; AVX2 lanes "
+                                   f"after internal/stencil/simd_amd64.go, scalar kernels elsewhere"},
         "e2e": {"value": round(value, 1), "unit": "Mcells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -722,6 +930,8 @@ def main():
                     choices=["terrain16k", "slope2k", "slope8k", "pipeline8k", "focal8k", "batch512", "serve40k"])
     ap.add_argument("--tune-cache", action="store_true", help="keep the batch autotuner's choices in a file")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="the headline workload alone (no focal, batched and served figures beside it)")
     ap.add_argument("--side", type=int, default=None, help="raster side override (profiling captures)")
     ap.add_argument("--band", type=int, default=None, help="serving: rows per unit of the radius-1 batch kernels")
     ap.add_argument("--ops", default=None, help="comma-separated ops of the workload to keep (profiling captures)")
@@ -743,11 +953,13 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     try:
         if args.workload == "batch512":
-            run_batch(args, rank, world, local_rank)
+            line = run_batch(args, rank, world, local_rank)
         elif args.workload == "serve40k":
-            run_serve(args, rank, world, local_rank)
+            line = run_serve(args, rank, world, local_rank)
         else:
-            run_ours(args, rank, world, local_rank)
+            line = run_default(args, rank, world, local_rank)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
     finally:
         if world > 1:
             import torch.distributed as dist

@@ -85,6 +85,9 @@ def lib():
         L.orc_process.restype = ctypes.c_int
         L.orc_process.argtypes = [ctypes.POINTER(Stage), ctypes.c_int, ctypes.POINTER(Raster),
                                   ctypes.POINTER(Raster), ctypes.c_int, ctypes.c_int]
+        L.orc_process_ex.restype = ctypes.c_int
+        L.orc_process_ex.argtypes = [ctypes.POINTER(Stage), ctypes.c_int, ctypes.POINTER(Raster),
+                                     ctypes.POINTER(Raster), ctypes.c_int, ctypes.c_int, ctypes.c_int]
         _lib = L
     return _lib
 
@@ -179,15 +182,80 @@ def _raster(data, width, height, stride, valid=None, valid_offset=0):
     return r
 
 
-def process(stages, src, dsts, nthreads=1):
+def process(stages, src, dsts, nthreads=1, simd=False):
     """Runs stages over src into dsts.
 
     stages: list of (Stage, keepalive) from stage().
     src, dsts[i]: dicts with keys data, width, height, stride, valid, valid_offset.
+    simd: run the radius-1 stencils through the restated AVX2 lanes
+    (strata_avx2.c, the reference's AVX2 path; the same bits).
     """
     st_arr = (Stage * len(stages))(*[s for s, _ in stages])
     s = _raster(**src)
     d_arr = (Raster * len(dsts))(*[_raster(**d) for d in dsts])
-    rc = lib().orc_process(st_arr, len(stages), ctypes.byref(s), d_arr, len(dsts), nthreads)
+    rc = lib().orc_process_ex(st_arr, len(stages), ctypes.byref(s), d_arr, len(dsts), nthreads, 1 if simd else 0)
     if rc != 0:
         raise ValueError(f"oracle: invalid call (rc={rc})")
+
+
+# ---------------------------------------------------------------------------
+# Stages from the terrain, focal and transfer options, resolved as the
+# reference's option code resolves them (terrain/stencil.go:16-49,
+# slope.go:84-95, aspect.go:97-102, hillshade.go:94-117, curvature.go:
+# 113-127, ruggedness.go:119-141, transfer/transfer.go:184-212), for
+# callers that must not load the device library (the benchmark's
+# reference arm). Defaults: cell size 1, z factor 1.
+
+def _cells(cell_size, cell_size_y, z_factor):
+    cx = cell_size or 1.0
+    cy = cell_size_y or cx
+    return cx, cy, (z_factor or 1.0)
+
+
+def gradient_stage(cell_size=1.0, cell_size_y=0.0, z_factor=1.0):
+    kx, ky = horn_scales(*_cells(cell_size, cell_size_y, z_factor))
+    return stage(GRADIENT, 1, 0, [kx, ky])
+
+
+def slope_stage(cell_size=1.0, cell_size_y=0.0, z_factor=1.0, units=0):
+    """units: 0 degrees, 1 percent, 2 radians (terrain.SlopeUnits)."""
+    kx, ky = horn_scales(*_cells(cell_size, cell_size_y, z_factor))
+    scale, take_atan = {0: (np.float32(180 / np.pi), 1), 1: (np.float32(100), 0), 2: (np.float32(1), 1)}[units]
+    return stage(SLOPE, 1, take_atan, [kx, ky, scale])
+
+
+def aspect_stage(cell_size=1.0, cell_size_y=0.0, z_factor=1.0, zero_for_flat=False, trigonometric=False):
+    kx, ky = horn_scales(*_cells(cell_size, cell_size_y, z_factor))
+    return stage(ASPECT, 1, 1 if trigonometric else 0, [kx, ky, 0.0 if zero_for_flat else -1.0])
+
+
+def hillshade_stage(cell_size=1.0, cell_size_y=0.0, z_factor=1.0, azimuth=315.0, altitude=45.0):
+    kx, ky = horn_scales(*_cells(cell_size, cell_size_y, z_factor))
+    c, bx, by = hillshade_light(azimuth, altitude)
+    return stage(HILLSHADE, 1, 0, [kx, ky, c, bx, by])
+
+
+def curvature_stage(cell_size=1.0, cell_size_y=0.0, z_factor=1.0, kind=0):
+    return stage(CURVATURE, 1, kind, zt_scales(*_cells(cell_size, cell_size_y, z_factor)))
+
+
+def ruggedness_stage(kind=0, radius=1):
+    return stage(RUGGEDNESS, radius, kind)
+
+
+def lookup_stage(xs, ys):
+    return stage(LOOKUP, 0, 0, (), [np.asarray(xs, np.float32), np.asarray(ys, np.float32)])
+
+
+def reclass_stage(breaks, values):
+    return stage(RECLASS, 0, 0, (), [np.asarray(breaks, np.float32), np.asarray(values, np.float32)])
+
+
+def pack_mask(valid: np.ndarray) -> np.ndarray:
+    """A (h, w) bool validity mask as LSB-first 64-bit words, row-major with
+    stride w (raster/mask.go's layout)."""
+    bits = np.packbits(np.asarray(valid, bool).reshape(-1), bitorder="little")
+    pad = (-bits.size) % 8
+    if pad:
+        bits = np.concatenate([bits, np.zeros(pad, np.uint8)])
+    return bits.view(np.uint64).copy()

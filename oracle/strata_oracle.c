@@ -572,6 +572,7 @@ typedef struct {
     int64_t band_rows;
     int64_t nbands;
     int64_t next; /* atomic band counter */
+    int simd;     /* run the radius-1 stencils' rows through the restated AVX2 lanes (strata_avx2.c) */
 } job_t;
 
 /* The interior cells [x0, x1) of one row, with the op chosen once per
@@ -642,6 +643,74 @@ static void stencil_row(const orc_stage *st, const float *row, int64_t s, int64_
     }
 }
 
+/* The baseline's validity of one output row at word level, as the
+ * reference's engine computes it (internal/stencil/mask.go:55-82, ErodeBox
+ * and shrink2Row): the AND of the 2r+1 source rows' words, shrunk by 2r
+ * cells with shifted copies, the edge ring's cells cleared, and the row's
+ * W bits deposited at the destination's offset (atomically only in words
+ * shared with other rows). acc and out hold (W + 63) / 64 + 1 words. The
+ * bits equal run_rows's cell-by-cell validity. */
+static void validity_row_words(const job_t *jb, const orc_raster *D, int64_t y, uint64_t *acc, uint64_t *out)
+{
+    const orc_raster *src = jb->src;
+    const int64_t W = src->width, H = src->height, s = src->stride;
+    const int r = jb->r;
+    const int64_t nw = (W + 63) >> 6;
+    const int yin = y >= r && y < H - r;
+    for (int64_t k = 0; k <= nw; k++) out[k] = 0;
+    if (yin && W > 2 * r) {
+        for (int64_t k = 0; k <= nw; k++) acc[k] = ~(uint64_t)0;
+        if (src->valid)
+            for (int j = -r; j <= r; j++) {
+                const int64_t off = src->valid_offset + (y + j) * s;
+                const int64_t last = (off + W - 1) >> 6;
+                for (int64_t k = 0; k < nw; k++) {
+                    const int64_t b = off + 64 * k, w = b >> 6;
+                    const int sh = (int)(b & 63);
+                    uint64_t v = src->valid[w] >> sh;
+                    if (sh && w + 1 <= last) v |= src->valid[w + 1] << (64 - sh);
+                    acc[k] &= v;
+                }
+            }
+        if (W & 63) acc[nw - 1] &= ((uint64_t)1 << (W & 63)) - 1;
+        acc[nw] = 0;
+        /* e bit x: the AND of acc bits x .. x + 2r; the output cell x + r. */
+        for (int64_t k = 0; k < nw; k++) {
+            uint64_t e = acc[k];
+            for (int d = 1; d <= 2 * r; d++) e &= (acc[k] >> d) | (acc[k + 1] << (64 - d));
+            out[k] = e;
+        }
+        /* shift up by r into column positions, then keep columns r .. W-r-1 */
+        for (int64_t k = nw; k > 0; k--) out[k] = (out[k] << r) | (out[k - 1] >> (64 - r));
+        out[0] <<= r;
+        for (int64_t x = 0; x < r; x++) out[x >> 6] &= ~((uint64_t)1 << (x & 63));
+        for (int64_t x = W - r; x < W; x++) out[x >> 6] &= ~((uint64_t)1 << (x & 63));
+    }
+    /* deposit W bits at D's offset for row y */
+    const int64_t base = D->valid_offset + y * D->stride;
+    int64_t x = 0;
+    while (x < W) {
+        const int64_t b = base + x;
+        const int sh = (int)(b & 63);
+        int64_t take = 64 - sh;
+        if (take > W - x) take = W - x;
+        const int64_t k = x >> 6, o = x & 63;
+        uint64_t v = out[k] >> o;
+        if (o && k + 1 <= nw) v |= out[k + 1] << (64 - o);
+        if (take < 64) v &= ((uint64_t)1 << take) - 1;
+        const uint64_t bits = v << sh;
+        const uint64_t own = take == 64 ? ~(uint64_t)0 : ((((uint64_t)1 << take) - 1) << sh);
+        uint64_t *w = &D->valid[b >> 6];
+        if (own == ~(uint64_t)0) {
+            *w = bits;
+        } else {
+            __atomic_fetch_and(w, ~own | bits, __ATOMIC_RELAXED);
+            __atomic_fetch_or(w, bits, __ATOMIC_RELAXED);
+        }
+        x += take;
+    }
+}
+
 static void run_rows(const job_t *jb, int64_t y0, int64_t y1, unsigned char *colok)
 {
     const orc_raster *src = jb->src;
@@ -671,7 +740,11 @@ static void run_rows(const job_t *jb, int64_t y0, int64_t y1, unsigned char *col
                 if (o1) o1[x] = nanf_;
             }
             if (x0 < x1) {
-                stencil_row(st, row, s, x0, x1, o0, o1);
+                int64_t xs = x0;
+                if (jb->simd && r == 1)
+                    xs += orc_avx2_row(st, o0 + x0, o1 ? o1 + x0 : NULL, row - s + x0 - 1, row + x0 - 1,
+                                       row + s + x0 - 1, x1 - x0);
+                if (xs < x1) stencil_row(st, row, s, xs, x1, o0, o1);
                 for (int i = 1; i < jb->nstages; i++)
                     for (int64_t x = x0; x < x1; x++) o0[x] = pointwise(&jb->stages[i], o0[x]);
             }
@@ -681,6 +754,11 @@ static void run_rows(const job_t *jb, int64_t y0, int64_t y1, unsigned char *col
         for (int d = 0; d < jb->ndst; d++) {
             const orc_raster *D = &jb->dst[d];
             if (!D->valid) continue;
+            if (jb->simd && stencil && r >= 1 && r < 64) {
+                uint64_t *acc = (uint64_t *)(colok + 3 * W + 72 - ((uintptr_t)(colok + 3 * W + 64) & 7));
+                validity_row_words(jb, D, y, acc, acc + ((W + 63) >> 6) + 1);
+                continue;
+            }
             unsigned char *vbuf = colok + W + 1;
             if (!stencil) {
                 for (int64_t x = 0; x < W; x++)
@@ -743,7 +821,9 @@ static void run_rows(const job_t *jb, int64_t y0, int64_t y1, unsigned char *col
 static void *worker(void *arg)
 {
     job_t *jb = (job_t *)arg;
-    unsigned char *colok = (unsigned char *)malloc(3 * (size_t)jb->src->width + 64);
+    /* bytes of the cell-by-cell validity, then the word rows of the baseline's */
+    unsigned char *colok = (unsigned char *)malloc(3 * (size_t)jb->src->width + 128 +
+                                                   2 * 8 * (((size_t)jb->src->width + 63) / 64 + 2));
     for (;;) {
         int64_t b = __atomic_fetch_add(&jb->next, 1, __ATOMIC_RELAXED);
         if (b >= jb->nbands) break;
@@ -758,6 +838,12 @@ static void *worker(void *arg)
 
 int orc_process(const orc_stage *stages, int nstages, const orc_raster *src,
                 const orc_raster *dst, int ndst, int nthreads)
+{
+    return orc_process_ex(stages, nstages, src, dst, ndst, nthreads, 0);
+}
+
+int orc_process_ex(const orc_stage *stages, int nstages, const orc_raster *src,
+                   const orc_raster *dst, int ndst, int nthreads, int simd)
 {
     if (nstages < 1 || !src || !dst) return -1;
     const orc_stage *st = &stages[0];
@@ -784,6 +870,7 @@ int orc_process(const orc_stage *stages, int nstages, const orc_raster *src,
     jb.src = src;
     jb.dst = dst;
     jb.ndst = ndst;
+    jb.simd = simd;
     jb.r = (st->op == ORC_LOOKUP || st->op == ORC_RECLASS) ? 0 : (st->op <= ORC_HILLSHADE || st->op == ORC_CURVATURE ? 1 : st->radius);
     /* Bands of about 2^16 cells, whole rows, as internal/exec/tile.go:21-27. */
     int64_t rows = (int64_t)65536 / (src->width > 0 ? src->width : 1);

@@ -77,6 +77,20 @@ void orc_gaussian(int radius, double sigma, float *taps);
 int orc_process(const orc_stage *stages, int nstages, const orc_raster *src,
                 const orc_raster *dst, int ndst, int nthreads);
 
+/* orc_process with simd != 0: the radius-1 stencils' interior rows run
+ * through the restated AVX2 lanes of strata_avx2.c (the reference's
+ * internal/stencil/simd_amd64.go), with the scalar kernels on each row's
+ * last n % 8 cells, as the reference runs them on AVX2 hardware. The
+ * results are the same bits; this is the timed CPU baseline. */
+int orc_process_ex(const orc_stage *stages, int nstages, const orc_raster *src,
+                   const orc_raster *dst, int ndst, int nthreads, int simd);
+
+/* The restated AVX2 lanes of one interior row (strata_avx2.c): the first
+ * multiple of eight of the n cells; returns how many it wrote. r0, r1, r2
+ * point at column x0 - 1 of the rows above, at and below. */
+int64_t orc_avx2_row(const orc_stage *st, float *o0, float *o1, const float *r0, const float *r1,
+                     const float *r2, int64_t n);
+
 #ifdef __cplusplus
 }
 #endif
