@@ -387,8 +387,19 @@ def run_ours(args, rank, world, local_rank):
     stream = torch.cuda.Stream(dev)
     opts = engine.Options(Stream=stream, Async=True, Device=local_rank)
     ops = [(name, dev(), nout) for name, dev, _mk, nout in wl["ops"]]
+    n_outs = sum(nout for _n, _s, nout in ops)
+    # Every output of the set, device-resident: the timed step is one
+    # terrain.Features call over the set (engine.process_features), which
+    # runs the memory-bound radius-1 ops as one fused pass over the input
+    # and the others as their own launches.
+    all_outs = [Float32Raster(torch.empty(n, dtype=torch.float32, device=dev), W, H, W,
+                              torch.empty(words, dtype=torch.int64, device=dev), 0) for _ in range(n_outs)]
+    feats = [st for _n, st, _o in ops]
 
-    def step(events=None):
+    def step():
+        assert engine.process_features(feats, all_outs, src, opts) is None
+
+    def separate(events=None):
         for i, (name, stages, nout) in enumerate(ops):
             if events is not None:
                 events[i][0].record(stream)
@@ -400,6 +411,7 @@ def run_ours(args, rank, world, local_rank):
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
             step()
+            separate()
     torch.cuda.synchronize()
 
     import torch.distributed as dist
@@ -410,10 +422,11 @@ def run_ours(args, rank, world, local_rank):
 
     per_op = [[torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)] for _ in ops]
     op_ms = [0.0] * len(ops)
-    # Per-op durations, from a separate pass of K steps with events between ops.
+    # Per-op durations, each op run alone (engine.process), from a separate
+    # pass of K steps with events between ops.
     with torch.cuda.stream(stream):
         for _ in range(args.steps):
-            step(per_op)
+            separate(per_op)
             torch.cuda.synchronize()
             for i in range(len(ops)):
                 op_ms[i] += per_op[i][0].elapsed_time(per_op[i][1]) / args.steps
@@ -444,26 +457,78 @@ def run_ours(args, rank, world, local_rank):
         gbs = b / (op_ms[i] / 1e3) / 1e9
         per.append({"op": name, "ms": round(op_ms[i], 4), "mcells_s": round(n / (op_ms[i] / 1e3) / 1e6, 1),
                     "gbs": round(gbs, 1), "frac_hbm": round(gbs / peak, 4)})
-    top = max(range(len(ops)), key=lambda i: op_ms[i])
-    traffic = None
+    traffic_db = {}
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         try:
-            traffic = json.load(open(tpath)).get(args.workload, {}).get(ops[top][0])
+            traffic_db = json.load(open(tpath)).get(args.workload, {})
         except Exception:
-            traffic = None
-    top_bytes = alg_bytes(n, ops[top][2], masked)
-    achieved = top_bytes / (op_ms[top] / 1e3) / 1e9
-    roofline = {"bound": "hbm", "kernel": ops[top][0], "achieved": round(achieved, 1), "peak": peak,
-                "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
-                "alg_bytes_per_launch": int(top_bytes)}
+            traffic_db = {}
+    fused = [i for i, (_nm, st, _o) in enumerate(ops) if _fusable(st)]
+    firsts = np.cumsum([0] + [nout for _n, _s, nout in ops])
+    fused_ms = None
+    if len(fused) >= 2:
+        # The fused pass alone (the step's one kernel for those features).
+        f_outs = [all_outs[int(firsts[i]) + k] for i in fused for k in range(ops[i][2])]
+        f_feats = [ops[i][1] for i in fused]
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            assert engine.process_features(f_feats, f_outs, src, opts) is None
+            ev0.record(stream)
+            for _ in range(args.steps):
+                assert engine.process_features(f_feats, f_outs, src, opts) is None
+            ev1.record(stream)
+        torch.cuda.synchronize()
+        fused_ms = ev0.elapsed_time(ev1) / args.steps
+    # The step's kernels: the fused pass, and each other op's own launch.
+    kernels = [(ops[i][0], op_ms[i], alg_bytes(n, ops[i][2], masked)) for i in range(len(ops))
+               if fused_ms is None or i not in fused]
+    if fused_ms is not None:
+        f_nout = sum(ops[i][2] for i in fused)
+        kernels.append((f"features_tma_kernel (the fused pass: {', '.join(ops[i][0] for i in fused)})", fused_ms,
+                        n * 4 * (1 + f_nout) + (n * (1 + f_nout) / 8.0 if masked else 0)))
+    kname, kms, top_bytes = max(kernels, key=lambda k: k[1])
+    achieved = top_bytes / (kms / 1e3) / 1e9
+    roofline = {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1), "peak": peak,
+                "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                "traffic": traffic_db.get("features" if kname.startswith("features_tma") else kname),
+                "alg_bytes_per_launch": int(top_bytes), "ms": round(kms, 4)}
+    launches_per_step = len(kernels)
+    fused_line = None
+    if fused_ms is not None:
+        fb = kernels[-1][2]
+        fused_line = {"ops": [ops[i][0] for i in fused], "ms": round(fused_ms, 4),
+                      "separate_ms": round(sum(op_ms[i] for i in fused), 4),
+                      "gbs": round(fb / (fused_ms / 1e3) / 1e9, 1),
+                      "frac_hbm": round(fb / (fused_ms / 1e3) / 1e9 / peak, 4)}
+    separate_ms = sum(op_ms)
+
+    # Parity at the benchmarked size: the timed call's outputs (every op of
+    # the set from one Features call), two row bands of each against the
+    # oracle on the same rows.
+    with torch.cuda.stream(stream):
+        step()
+    torch.cuda.synchronize()
+
+    def fetch(i, y0, y1):
+        res = []
+        for k in range(ops[i][2]):
+            o = all_outs[int(firsts[i]) + k]
+            d = o.data[y0 * W:y1 * W].cpu().numpy().reshape(y1 - y0, W)
+            b0, b1 = y0 * W, y1 * W
+            wd = o.valid[b0 // 64:(b1 + 63) // 64].cpu().numpy().view(np.uint8)
+            bits = np.unpackbits(wd, bitorder="little")[b0 - (b0 // 64) * 64:][:b1 - b0]
+            res.append((d, bits.reshape(y1 - y0, W).astype(bool)))
+        return res
+
+    parity = parity_check(wl, fetch) if rank == 0 else None
 
     # e2e: the public API with host (page-locked) buffers, every copy inside
     # the timed region: one process_features call (terrain.Features) for
     # every op of the set, the pipeline included, so the DEM crosses once
     # and each output's copy back overlaps the next op's kernels.
     host_src = Float32Raster(host_cells.numpy(), W, H, W, host_mask.numpy().view(np.uint64), 0)
-    n_outs = sum(nout for _n, _s, nout in ops)
+    del all_outs
     host_outs = [Float32Raster(torch.empty(n, dtype=torch.float32).pin_memory().numpy(), W, H, W,
                                torch.zeros(words, dtype=torch.int64).pin_memory().numpy().view(np.uint64), 0)
                  for _ in range(n_outs)]
@@ -491,27 +556,7 @@ def run_ours(args, rank, world, local_rank):
            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": round(e2e_s * 1e3, 2),
            "api": "engine.process_features (terrain.Features) over every op, host rasters"}
 
-    # Parity at the benchmarked size: each op once more, its output rows of
-    # two bands against the oracle on the same rows.
-    state = {"op": -1}
 
-    def fetch(i, y0, y1):
-        if state["op"] != i:
-            assert engine.process(ops[i][1], outs[:ops[i][2]], [src], opts) is None
-            torch.cuda.synchronize()
-            state["op"] = i
-        res = []
-        for k in range(ops[i][2]):
-            d = outs[k].data[y0 * W:y1 * W].cpu().numpy().reshape(y1 - y0, W)
-            b0, b1 = y0 * W, y1 * W
-            words = outs[k].valid[b0 // 64:(b1 + 63) // 64].cpu().numpy().view(np.uint8)
-            bits = np.unpackbits(words, bitorder="little")[b0 - (b0 // 64) * 64:][:b1 - b0]
-            res.append((d, bits.reshape(y1 - y0, W).astype(bool)))
-        return res
-
-    parity = parity_check(wl, fetch) if rank == 0 else None
-
-    launches_per_step = len(ops)  # one kernel per op: the march writes the validity beside the cells
     line = {
         "metric": "Mcells/s (output cells of every op in the set per second)", "value": round(value, 1),
         "unit": "Mcells/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -522,6 +567,10 @@ def run_ours(args, rank, world, local_rank):
                    "parallelism": f"independent rasters x{world}"},
         "roofline": roofline, "e2e": e2e, "gpu_launches": launches_per_step * args.steps,
         "clocks": clk.summary(), "per_op": per, "parity": parity,
+        "fused_pass": fused_line,
+        "separate_calls": {"value": round(world * cells_per_step / (separate_ms / 1e3) / 1e6, 1), "unit": "Mcells/s",
+                           "ms_per_step": round(separate_ms, 4),
+                           "api": "engine.process per op (each op alone, its own read of the input)"},
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(wl)
@@ -844,6 +893,20 @@ def run_serve(args, rank, world, local_rank):
         "server": st, "clocks": clk.summary(),
     }
     return line
+
+
+def _fusable(stages):
+    """Whether a feature runs in the fused multi-output pass (the library
+    decides, features.cu; this mirrors it for the launch count): Gradient,
+    Slope in percent or followed by a Reclass, and Wilson's TRI, TPI and
+    roughness at radius 1."""
+    st = stages.stages[0]
+    tail = [x.op for x in stages.stages[1:]]
+    folds = bool(tail) and tail[-1] == 13 and all(t in (12, 13) for t in tail)
+    if tail and not folds:
+        return False
+    return (st.op == 1 or (st.op == 2 and (st.kind == 0 or folds)) or
+            (st.op == 6 and st.radius == 1 and st.kind in (1, 2, 3)))
 
 
 def _orc_of(st):

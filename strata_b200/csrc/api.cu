@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <cstring>
 #include <limits>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -1689,6 +1690,27 @@ extern "C" int strata_process_features(strata_ctx* c, const strata_stage* stages
         for (auto e : events) cudaEventDestroy(e);
     };
     int64_t bands = 0, window = 0;
+    // Starts the copies back of outputs [o, o + n) once the work queued on st
+    // so far is done, on the copy stream, so they overlap the next kernels.
+    auto copy_back = [&](int o, int n) -> int {
+        bool any_host = false;
+        for (int i = o; i < o + n; i++) any_host = any_host || !dst[i].on_device;
+        if (!any_host) return STRATA_OK;
+        cudaEvent_t ev;
+        cudaError_t e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+        if (e != cudaSuccess) return cuda_fail(e, "event");
+        events.push_back(ev);
+        cudaEventRecord(ev, st);
+        cudaStreamWaitEvent(cs, ev, 0);
+        for (int i = o; i < o + n; i++) {
+            if (dst[i].on_device) continue;
+            const DevOperand& d = dd[(size_t)i];
+            e = data_back(dst[i], d, cs);
+            if (e == cudaSuccess && dst[i].valid) e = mask_back(dst[i], d, c->h_edges + 2 * i, cs);
+            if (e != cudaSuccess) return cuda_fail(e, "copy to host");
+        }
+        return STRATA_OK;
+    };
     for (int f = 0; f < nfeatures; f++) {
         LaunchParams& p = plans[(size_t)f];
         const int o = first[(size_t)f];
@@ -1711,6 +1733,80 @@ extern "C" int strata_process_features(strata_ctx* c, const strata_stage* stages
         p.out_y0 = 0;
         p.out_y1 = H;
         p.status = c->d_status;
+    }
+    // The memory-bound radius-1 features whose rows the TMA march takes run
+    // as one fused pass (one read of the source, Horn's differences formed
+    // once; features.cu says which); the others, and all of them when fewer
+    // than two fuse, run one by one.
+    std::vector<char> done((size_t)nfeatures, 0);
+    {
+        std::unique_ptr<strata::FeaturesParams> fp(new strata::FeaturesParams);
+        memset(fp.get(), 0, sizeof(strata::FeaturesParams));
+        std::vector<int> group;
+        for (int f = 0; f < nfeatures; f++) {
+            const LaunchParams& p = plans[(size_t)f];
+            if (!strata::feature_fusable(p) || fp->nfeat == strata::kMaxFeatures ||
+                fp->nout + nouts[(size_t)f] > strata::kMaxFeatures + 1)
+                continue;
+            strata::FeatureSpec& F = fp->f[fp->nfeat++];
+            F.op = p.op;
+            F.kind = p.kind;
+            F.out = fp->nout;
+            memcpy(F.k, p.k, sizeof F.k);
+            if (p.nepi == 1) {
+                F.nb = p.epi[0].n;
+                memcpy(F.t, p.epi[0].a, sizeof(float) * (size_t)F.nb);
+                memcpy(F.v, p.epi[0].b, sizeof(float) * (size_t)(F.nb + 1));
+            }
+            if (p.op == STRATA_OP_GRADIENT || p.op == STRATA_OP_SLOPE) fp->horn = 1;
+            for (int k = 0; k < nouts[(size_t)f]; k++) {
+                const int i = first[(size_t)f] + k;
+                strata::FeatureOut& O = fp->o[fp->nout++];
+                O.data = dd[(size_t)i].data;
+                O.stride = dd[(size_t)i].stride;
+                if (dst[i].valid) {
+                    O.bits = dd[(size_t)i].bits;
+                    O.bit_off = dd[(size_t)i].bit_off;
+                    O.bit_stride = dd[(size_t)i].stride;
+                }
+            }
+            group.push_back(f);
+        }
+        if (group.size() >= 2) {
+            fp->g = plans[(size_t)group[0]];
+            LaunchParams& g = fp->g;
+            memset(&g.vf, 0, sizeof g.vf);
+            if (src[0].valid) {
+                g.vf.src_bits = ds.bits;
+                g.vf.src_off = ds.bit_off;
+                g.vf.src_stride = ds.stride;
+                g.vf.src_lo_word = ds.lo_word;
+                g.vf.src_hi_word = ds.hi_word;
+            }
+            int64_t wc = 0;
+            const int64_t t = strata::launch_features(*fp, st, &wc);
+            if (t >= 0) {
+                bands += t;
+                window += wc;
+                cudaError_t e = cudaGetLastError();
+                if (e != cudaSuccess) {
+                    cleanup();
+                    return cuda_fail(e, "kernel launch");
+                }
+                for (int f : group) {
+                    done[(size_t)f] = 1;
+                    if ((rc = copy_back(first[(size_t)f], nouts[(size_t)f]))) {
+                        cleanup();
+                        return rc;
+                    }
+                }
+            }
+        }
+    }
+    for (int f = 0; f < nfeatures; f++) {
+        if (done[(size_t)f]) continue;
+        LaunchParams& p = plans[(size_t)f];
+        const int o = first[(size_t)f];
         int64_t wc = 0;
         ValidityParams vp[2];
         const ValidityParams* vs[2] = {nullptr, nullptr};
@@ -1733,26 +1829,9 @@ extern "C" int strata_process_features(strata_ctx* c, const strata_stage* stages
             return cuda_fail(e, "kernel launch");
         }
         // The outputs' copies back overlap the next feature's kernels.
-        bool any_host = false;
-        for (int i = o; i < o + nouts[(size_t)f]; i++) any_host = any_host || !dst[i].on_device;
-        if (!any_host) continue;
-        cudaEvent_t ev;
-        if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) {
+        if ((rc = copy_back(o, nouts[(size_t)f]))) {
             cleanup();
-            return cuda_fail(e, "event");
-        }
-        events.push_back(ev);
-        cudaEventRecord(ev, st);
-        cudaStreamWaitEvent(cs, ev, 0);
-        for (int i = o; i < o + nouts[(size_t)f]; i++) {
-            if (dst[i].on_device) continue;
-            const DevOperand& d = dd[(size_t)i];
-            e = data_back(dst[i], d, cs);
-            if (e == cudaSuccess && dst[i].valid) e = mask_back(dst[i], d, c->h_edges + 2 * i, cs);
-            if (e != cudaSuccess) {
-                cleanup();
-                return cuda_fail(e, "copy to host");
-            }
+            return rc;
         }
     }
     cudaError_t e = cudaStreamSynchronize(cs);

@@ -548,6 +548,67 @@ def test_features_equal_separate_calls():
             assert_same_raster(to_host(got), want, f"features {type(op).__name__} device={device}")
 
 
+def _fused_feature_set():
+    """Every radius-1 op and kind, with Reclass epilogues (folded on the
+    squared magnitude for Slope), and one radius-3 op: the memory-bound
+    ones run in the fused pass, the others as their own launches."""
+    o = dict(CellSize=10)
+    return [
+        terrain.gradient_stage(terrain.GradientOptions(CellSize=10, CellSizeY=12)),
+        terrain.slope_stage(terrain.SlopeOptions(**o)),
+        terrain.slope_stage(terrain.SlopeOptions(CellSize=3, Units=terrain.SlopePercent)),
+        terrain.aspect_stage(terrain.AspectOptions(**o)),
+        terrain.aspect_stage(terrain.AspectOptions(CellSize=5, ZeroForFlat=True, Trigonometric=True)),
+        terrain.hillshade_stage(terrain.HillshadeOptions(CellSize=10, Azimuth=200, Altitude=30)),
+        terrain.curvature_stage(terrain.CurvatureOptions(Type=0, **o)),
+        terrain.curvature_stage(terrain.CurvatureOptions(Type=1, **o)),
+        terrain.curvature_stage(terrain.CurvatureOptions(Type=2, **o)),
+        terrain.ruggedness_stage(terrain.RuggednessOptions(Type=0)),
+        terrain.ruggedness_stage(terrain.RuggednessOptions(Type=1)),
+        terrain.ruggedness_stage(terrain.RuggednessOptions(Type=2)),
+        terrain.ruggedness_stage(terrain.RuggednessOptions(Type=3)),
+        terrain.slope_stage(terrain.SlopeOptions(**o)).extend(transfer.lookup_stage(SLOPE_XS, SLOPE_YS)).extend(
+            transfer.reclass_stage(BREAKS, VALUES)),
+        terrain.slope_stage(terrain.SlopeOptions(CellSize=2, Units=terrain.SlopePercent)).extend(
+            transfer.reclass_stage([5, 15, 60], [1, 2, 3, 4])),
+        terrain.aspect_stage(terrain.AspectOptions(**o)).extend(transfer.reclass_stage([90, 180, 270], [1, 2, 3, 4])),
+        terrain.ruggedness_stage(terrain.RuggednessOptions(Type=2, Radius=3)),
+    ]
+
+
+@pytest.mark.parametrize("w,h", [(256, 70), (516, 37), (1028, 9)])
+def test_fused_features_equal_separate_calls_and_oracle(w, h):
+    """One Features call over every radius-1 op (the memory-bound ones in
+    the fused multi-output pass) writes each output's own bits and validity:
+    the same as the op run alone and as the oracle, masked and unmasked,
+    host and device operands, compact and strided outputs with bit offsets."""
+    cells = dem_cells(w, h, w + h)
+    for masked, device, strided in itertools.product((False, True), (False, True), (False, True)):
+        src = host_raster(cells, synth.block_mask(w, h, w, 0.05) if masked else None)
+        feats = _fused_feature_set()
+        nouts = [2 if f.stages[0].op == engine._lib.OP_GRADIENT else 1 for f in feats]
+        st, off = (w + 8, 40) if strided else (None, 0)
+        outs = [like(src, st, off) for _ in range(sum(nouts))]
+        before = [Float32Raster(np.array(g.data), g.width, g.height, g.stride,
+                                None if g.valid is None else np.array(g.valid), g.valid_offset) for g in outs]
+        s_ = to_device(src) if device else src
+        o_ = [to_device(x) for x in outs] if device else outs
+        assert engine.process_features(feats, o_, s_) is None
+        got = [to_host(x) for x in o_] if device else outs
+        k = 0
+        for f, n in zip(_fused_feature_set(), nouts):
+            alone = [like(src, st, off) for _ in range(n)]
+            assert engine.process(f, alone, [src]) is None
+            want = [like(src, st, off) for _ in range(n)]
+            run_oracle(f, src, want)
+            for i in range(n):
+                what = f"{w}x{h} masked={masked} device={device} strided={strided} feature op {f.stages[0].op} out{i}"
+                assert_same_raster(got[k + i], alone[i], what + " vs alone")
+                assert_same_raster(got[k + i], want[i], what + " vs oracle")
+                assert_padding_untouched(before[k + i], got[k + i], what)
+            k += n
+
+
 def test_surface_equals_separate_calls():
     w, h = 128, 40
     src = host_raster(dem_cells(w, h, 13), synth.cell_mask(w, h, 13))
