@@ -1745,29 +1745,27 @@ extern "C" int strata_process_features(strata_ctx* c, const strata_stage* stages
         std::vector<int> group;
         for (int f = 0; f < nfeatures; f++) {
             const LaunchParams& p = plans[(size_t)f];
-            if (!strata::feature_fusable(p) || fp->nfeat == strata::kMaxFeatures ||
-                fp->nout + nouts[(size_t)f] > strata::kMaxFeatures + 1)
-                continue;
-            strata::FeatureSpec& F = fp->f[fp->nfeat++];
-            F.op = p.op;
-            F.kind = p.kind;
-            F.out = fp->nout;
+            const int q = strata::feature_slot(p);
+            if (q < 0 || fp->f[q].on) continue;
+            strata::FeatureSlot& F = fp->f[q];
+            F.on = 1;
             memcpy(F.k, p.k, sizeof F.k);
             if (p.nepi == 1) {
                 F.nb = p.epi[0].n;
                 memcpy(F.t, p.epi[0].a, sizeof(float) * (size_t)F.nb);
                 memcpy(F.v, p.epi[0].b, sizeof(float) * (size_t)(F.nb + 1));
             }
-            if (p.op == STRATA_OP_GRADIENT || p.op == STRATA_OP_SLOPE) fp->horn = 1;
+            if (q == strata::kFGradient || q == strata::kFSlopeClass || q == strata::kFSlopePercent) fp->horn = 1;
+            else fp->window = 1;
             for (int k = 0; k < nouts[(size_t)f]; k++) {
                 const int i = first[(size_t)f] + k;
-                strata::FeatureOut& O = fp->o[fp->nout++];
-                O.data = dd[(size_t)i].data;
-                O.stride = dd[(size_t)i].stride;
+                F.data[k] = dd[(size_t)i].data;
+                F.stride[k] = dd[(size_t)i].stride;
                 if (dst[i].valid) {
-                    O.bits = dd[(size_t)i].bits;
-                    O.bit_off = dd[(size_t)i].bit_off;
-                    O.bit_stride = dd[(size_t)i].stride;
+                    F.bits[k] = dd[(size_t)i].bits;
+                    F.bit_off[k] = dd[(size_t)i].bit_off;
+                    F.bit_stride[k] = dd[(size_t)i].stride;
+                    fp->masked = 1;
                 }
             }
             group.push_back(f);

@@ -16,11 +16,9 @@
 //     128 columns (focal.cuh, in batch_focal.cu).
 // Each raster keeps its own descriptor (the block stages it in shared
 // memory when it reaches the raster's units) and its own band height (the
-// autotuner's choice for its class). The radius-1 march units write their
-// outputs' validity themselves, right after their cells (validity.cuh
-// march_unit_validity); the validity of the wider windows' outputs runs in
-// persistent kernels of its own, one per radius, a warp a unit of 1024
-// cells by a band of rows.
+// autotuner's choice for its class). The validity of every masked output
+// runs in persistent kernels of its own, one per radius, a warp a unit of
+// 1024 cells by a band of rows (validity.cuh).
 #include <algorithm>
 
 #include "batch.cuh"
@@ -61,13 +59,7 @@ __global__ void __launch_bounds__(kBatchThreads, 5) batch_march_kernel(const Bat
         }
         const BatchUnit b = batch_unit(items[it], P, u);
         const int64_t xs = b.x + 128 * warp;
-        if (xs < P.out_x1) {
-            march_warp<OP, KIND, EPI>(P, T, xs, b.y0, b.rows, b.vec);
-            // The unit's validity beside its cells (batch_plan_validity
-            // leaves the radius-1 items' masks to this kernel).
-            const int nv = items[it].nvalid;
-            for (int k = 0; k < nv; k++) march_unit_validity(items[it].v[k], xs, b.y0, b.rows, threadIdx.x & 31);
-        }
+        if (xs < P.out_x1) march_warp<OP, KIND, EPI>(P, T, xs, b.y0, b.rows, b.vec);
     }
 }
 
@@ -231,7 +223,6 @@ int batch_plan_validity(const BatchItem* items, int n, ValidityItem* vitems, Val
         ValidityClass c{r, nv, 0, 0};
         for (int i = 0; i < n; i++)
             for (int k = 0; k < items[i].nvalid; k++) {
-                if (key_of(items[i].p).family == 0) continue;  // the march kernel writes it
                 const ValidityParams& v = items[i].v[k];
                 if (v.radius != r || v.dst_words <= 0 || v.out_x1 <= v.out_x0 || v.out_y1 <= v.out_y0) continue;
                 ValidityItem& it = vitems[nv++];

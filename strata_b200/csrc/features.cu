@@ -36,9 +36,9 @@ namespace {
 
 using namespace cell;
 
-// A lone Reclass over four cells (ops3.cuh reclass_chain4) from a feature's
+// A lone Reclass over four cells (ops3.cuh reclass_chain4) from a slot's
 // breaks and values; NaN passes through.
-__device__ __forceinline__ void feature_chain(const FeatureSpec& F, float (&v)[4]) {
+__device__ __forceinline__ void feature_chain(const FeatureSlot& F, float (&v)[4]) {
     float r[4];
 #pragma unroll
     for (int c = 0; c < 4; c++) r[c] = F.v[0];
@@ -53,20 +53,37 @@ __device__ __forceinline__ void feature_chain(const FeatureSpec& F, float (&v)[4
     for (int c = 0; c < 4; c++) v[c] = v[c] != v[c] ? v[c] : r[c];
 }
 
-// Every feature's four cells of one output row (global row y) from the
-// window rows a, b, c and their horizontal differences.
+// Masks the edge ring (NaN), takes the slot's epilogue and stores the
+// lane's four cells of output k of the slot.
+__device__ __forceinline__ void feature_store(const FeatureSlot& F, int k, const Strip& S, const bool (&in)[4],
+                                              int64_t rowoff, int64_t coloff, float (&o)[4]) {
+    const float nan = nanf32();
+#pragma unroll
+    for (int i = 0; i < 4; i++) o[i] = in[i] ? o[i] : nan;
+    // The epilogue maps NaN to itself, so the edge ring stays NaN.
+    if (F.nb > 0) feature_chain(F, o);
+    if (S.active) *reinterpret_cast<float4*>(F.data[k] + rowoff * F.stride[k] + coloff) = make_float4(o[0], o[1], o[2], o[3]);
+}
+
+// Every slot's four cells of one output row (global row y) from the window
+// rows a, b, c and their horizontal differences. The slots are walked in a
+// fixed order with their parameters at fixed places.
 __device__ __forceinline__ void features_row(const FeaturesParams& F, const Strip& S, int64_t y, const Row6& a,
                                              const Row6& b, const Row6& c, const float (&ha)[4],
                                              const float (&hb)[4], const float (&hc)[4], bool rowin) {
     const LaunchParams& P = F.g;
-    const float nan = nanf32();
-    // Horn's differences, unscaled (internal/stencil/horn.go:152-160), in
-    // the lane's pairs of cells (0, 1) and (2, 3), as march.cuh forms them.
-    F2 DX[2], DY[2];
+    bool in[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) in[i] = rowin && S.colin[i];
+    const int64_t rowoff = y - P.dst_y0;
+    const int64_t coloff = S.x - P.dst_x0;
     if (F.horn) {
+        // Horn's differences, unscaled (internal/stencil/horn.go:152-160),
+        // in the lane's pairs of cells (0, 1) and (2, 3), as march.cuh forms them.
         const F2 V12 = sub2(pk(c.v[1], c.v[2]), pk(a.v[1], a.v[2]));
         const F2 V34 = sub2(pk(c.v[3], c.v[4]), pk(a.v[3], a.v[4]));
         const float V0 = sub(c.v[0], a.v[0]), V5 = sub(c.v[5], a.v[5]);
+        F2 DX[2], DY[2];
         DY[0] = add2(pk(add(V0, hi(V12)), add(lo(V12), lo(V34))), add2(V12, V12));
         DY[1] = add2(pk(add(hi(V12), hi(V34)), add(lo(V34), V5)), add2(V34, V34));
 #pragma unroll
@@ -74,77 +91,70 @@ __device__ __forceinline__ void features_row(const FeaturesParams& F, const Stri
             const F2 hb2 = pk(hb[2 * p], hb[2 * p + 1]);
             DX[p] = add2(add2(pk(ha[2 * p], ha[2 * p + 1]), pk(hc[2 * p], hc[2 * p + 1])), add2(hb2, hb2));
         }
-    }
-    bool in[4];
-#pragma unroll
-    for (int i = 0; i < 4; i++) in[i] = rowin && S.colin[i];
-    const int64_t rowoff = y - P.dst_y0;
-    const int64_t coloff = S.x - P.dst_x0;
-    for (int f = 0; f < F.nfeat; f++) {
-        const FeatureSpec& s = F.f[f];
-        float o0[4], o1[4] = {nan, nan, nan, nan};
-        const int op = s.op;
-        // One branch per op and kind, each with its own loop over the cells,
-        // so that no feature evaluates another's arithmetic (selects between
-        // finished values would compute every kind).
-        if (op == STRATA_OP_RUGGEDNESS) {
-            if (s.kind == STRATA_RUG_TPI) {
-#pragma unroll
-                for (int i = 0; i < 4; i++)
-                    o0[i] = rugged3(a.v[i], a.v[i + 1], a.v[i + 2], b.v[i], b.v[i + 1], b.v[i + 2], c.v[i],
-                                    c.v[i + 1], c.v[i + 2], STRATA_RUG_TPI);
-            } else if (s.kind == STRATA_RUG_ROUGHNESS) {
-#pragma unroll
-                for (int i = 0; i < 4; i++)
-                    o0[i] = rugged3(a.v[i], a.v[i + 1], a.v[i + 2], b.v[i], b.v[i + 1], b.v[i + 2], c.v[i],
-                                    c.v[i + 1], c.v[i + 2], STRATA_RUG_ROUGHNESS);
-            } else {
-#pragma unroll
-                for (int i = 0; i < 4; i++)
-                    o0[i] = rugged3(a.v[i], a.v[i + 1], a.v[i + 2], b.v[i], b.v[i + 1], b.v[i + 2], c.v[i],
-                                    c.v[i + 1], c.v[i + 2], STRATA_RUG_TRI_WILSON);
-            }
-        } else if (op == STRATA_OP_GRADIENT) {
+        if (F.f[kFGradient].on) {
+            const FeatureSlot& Q = F.f[kFGradient];
+            float o0[4], o1[4];
 #pragma unroll
             for (int p = 0; p < 2; p++) {
-                const F2 gx = mul2(DX[p], splat(s.k[0])), gy = mul2(DY[p], splat(s.k[1]));
+                const F2 gx = mul2(DX[p], splat(Q.k[0])), gy = mul2(DY[p], splat(Q.k[1]));
                 o0[2 * p] = lo(gx);
                 o0[2 * p + 1] = hi(gx);
                 o1[2 * p] = lo(gy);
                 o1[2 * p + 1] = hi(gy);
             }
-        } else if (s.kind == kSlopeSquareClass) {
+            feature_store(Q, 0, S, in, rowoff, coloff, o0);
+            feature_store(Q, 1, S, in, rowoff, coloff, o1);
+        }
+        if (F.f[kFSlopeClass].on) {
+            const FeatureSlot& Q = F.f[kFSlopeClass];
+            float o[4];
 #pragma unroll
             for (int p = 0; p < 2; p++) {
-                const F2 gx = mul2(DX[p], splat(s.k[0])), gy = mul2(DY[p], splat(s.k[1]));
+                const F2 gx = mul2(DX[p], splat(Q.k[0])), gy = mul2(DY[p], splat(Q.k[1]));
                 const F2 r = add_p(mul2(gx, gx), mul2(gy, gy));  // magnitude's radicand (horn.go:220-222)
-                o0[2 * p] = lo(r);
-                o0[2 * p + 1] = hi(r);
+                o[2 * p] = lo(r);
+                o[2 * p + 1] = hi(r);
             }
-        } else {
+            feature_store(Q, 0, S, in, rowoff, coloff, o);
+        }
+        if (F.f[kFSlopePercent].on) {
+            const FeatureSlot& Q = F.f[kFSlopePercent];
+            float o[4];
 #pragma unroll
             for (int p = 0; p < 2; p++) {
-                const F2 gx = mul2(DX[p], splat(s.k[0])), gy = mul2(DY[p], splat(s.k[1]));
-                const F2 r = slope2(gx, gy, splat(s.k[2]), false);  // percent: no arctangent
-                o0[2 * p] = lo(r);
-                o0[2 * p + 1] = hi(r);
+                const F2 gx = mul2(DX[p], splat(Q.k[0])), gy = mul2(DY[p], splat(Q.k[1]));
+                const F2 r = slope2(gx, gy, splat(Q.k[2]), false);  // percent: no arctangent
+                o[2 * p] = lo(r);
+                o[2 * p + 1] = hi(r);
             }
+            feature_store(Q, 0, S, in, rowoff, coloff, o);
         }
+    }
+    if (F.window) {
+        // The ruggedness measures at radius 1 (rugged3's float32 kinds).
+        if (F.f[kFTpi].on) {
+            float o[4];
 #pragma unroll
-        for (int i = 0; i < 4; i++) {
-            o0[i] = in[i] ? o0[i] : nan;
-            o1[i] = in[i] ? o1[i] : nan;
+            for (int i = 0; i < 4; i++)
+                o[i] = rugged3(a.v[i], a.v[i + 1], a.v[i + 2], b.v[i], b.v[i + 1], b.v[i + 2], c.v[i], c.v[i + 1],
+                               c.v[i + 2], STRATA_RUG_TPI);
+            feature_store(F.f[kFTpi], 0, S, in, rowoff, coloff, o);
         }
-        // The epilogue maps NaN to itself, so the edge ring stays NaN.
-        if (s.nb > 0) feature_chain(s, o0);
-        if (S.active) {
-            const FeatureOut& O = F.o[s.out];
-            *reinterpret_cast<float4*>(O.data + rowoff * O.stride + coloff) = make_float4(o0[0], o0[1], o0[2], o0[3]);
-            if (op == STRATA_OP_GRADIENT) {
-                const FeatureOut& O1 = F.o[s.out + 1];
-                *reinterpret_cast<float4*>(O1.data + rowoff * O1.stride + coloff) =
-                    make_float4(o1[0], o1[1], o1[2], o1[3]);
-            }
+        if (F.f[kFRoughness].on) {
+            float o[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+                o[i] = rugged3(a.v[i], a.v[i + 1], a.v[i + 2], b.v[i], b.v[i + 1], b.v[i + 2], c.v[i], c.v[i + 1],
+                               c.v[i + 2], STRATA_RUG_ROUGHNESS);
+            feature_store(F.f[kFRoughness], 0, S, in, rowoff, coloff, o);
+        }
+        if (F.f[kFWilson].on) {
+            float o[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+                o[i] = rugged3(a.v[i], a.v[i + 1], a.v[i + 2], b.v[i], b.v[i + 1], b.v[i + 2], c.v[i], c.v[i + 1],
+                               c.v[i + 2], STRATA_RUG_TRI_WILSON);
+            feature_store(F.f[kFWilson], 0, S, in, rowoff, coloff, o);
         }
     }
 }
@@ -239,12 +249,16 @@ __global__ void __launch_bounds__(kWarps * 32, 5)
         if (ok)
             valid_strip_emit(P, S.xs, S.y0, rows, vwords[warp], lane,
                              [&](int64_t y, int64_t c0, uint32_t v, uint32_t ours) {
-                                 for (int i = 0; i < F.nout; i++) {
-                                     const FeatureOut& O = F.o[i];
-                                     if (O.bits)
-                                         put_bits(O.bits, O.bit_off + (y - P.dst_y0) * O.bit_stride + (c0 - P.dst_x0),
-                                                  v, ours);
-                                 }
+#pragma unroll
+                                 for (int q = 0; q < kFSlots; q++)
+#pragma unroll
+                                     for (int k = 0; k < 2; k++) {
+                                         const FeatureSlot& Q = F.f[q];
+                                         if (Q.on && Q.bits[k])
+                                             put_bits(Q.bits[k],
+                                                      Q.bit_off[k] + (y - P.dst_y0) * Q.bit_stride[k] + (c0 - P.dst_x0),
+                                                      v, ours);
+                                     }
                              });
     }
     if (!ok) {
@@ -257,12 +271,16 @@ bool aligned16_(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) ==
 
 }  // namespace
 
-bool feature_fusable(const LaunchParams& p) {
-    const bool light = p.op == STRATA_OP_GRADIENT || (p.op == STRATA_OP_SLOPE && p.kind != 1) ||
-                       (p.op == STRATA_OP_RUGGEDNESS && p.radius == 1 && p.kind != STRATA_RUG_TRI_RILEY);
-    if (!light) return false;
-    if (p.nepi > 1 || (p.nepi == 1 && (p.epi[0].op != STRATA_OP_RECLASS || p.epi[0].n > kChainBreaks))) return false;
-    return march3_eligible(p);
+int feature_slot(const LaunchParams& p) {
+    if (p.nepi > 1 || (p.nepi == 1 && (p.epi[0].op != STRATA_OP_RECLASS || p.epi[0].n > kChainBreaks))) return -1;
+    int q = -1;
+    if (p.op == STRATA_OP_GRADIENT) q = kFGradient;
+    else if (p.op == STRATA_OP_SLOPE && p.kind == kSlopeSquareClass) q = kFSlopeClass;
+    else if (p.op == STRATA_OP_SLOPE && p.kind == 0) q = kFSlopePercent;
+    else if (p.op == STRATA_OP_RUGGEDNESS && p.radius == 1 && p.kind == STRATA_RUG_TRI_WILSON) q = kFWilson;
+    else if (p.op == STRATA_OP_RUGGEDNESS && p.radius == 1 && p.kind == STRATA_RUG_TPI) q = kFTpi;
+    else if (p.op == STRATA_OP_RUGGEDNESS && p.radius == 1 && p.kind == STRATA_RUG_ROUGHNESS) q = kFRoughness;
+    return q >= 0 && march3_eligible(p) ? q : -1;
 }
 
 int64_t launch_features(const FeaturesParams& f, cudaStream_t s, int64_t* window_cells) {
@@ -273,8 +291,9 @@ int64_t launch_features(const FeaturesParams& f, cudaStream_t s, int64_t* window
         return 0;
     }
     if ((w & 3) || (p.src_stride & 3) || !aligned16_(p.src) || ((p.out_x0 - p.src_x0) & 3)) return -1;
-    for (int i = 0; i < f.nout; i++)
-        if ((f.o[i].stride & 3) || !aligned16_(f.o[i].data)) return -1;
+    for (int q = 0; q < kFSlots; q++)
+        for (int k = 0; k < 2 && f.f[q].on; k++)
+            if (f.f[q].data[k] && ((f.f[q].stride[k] & 3) || !aligned16_(f.f[q].data[k]))) return -1;
     CUtensorMap map;
     if (!source_map(p, &map)) return -1;
     const int64_t segs = (w + 127) / 128;
@@ -282,9 +301,7 @@ int64_t launch_features(const FeaturesParams& f, cudaStream_t s, int64_t* window
     int64_t strip = (h * segs) / ((int64_t)sm_count() * 40 * 4);
     strip = strip < 8 ? 8 : (strip > kMaxStrip ? kMaxStrip : strip);
     const int64_t blocks = col_blocks * ((h + strip - 1) / strip);
-    bool val = false;
-    for (int i = 0; i < f.nout; i++) val = val || f.o[i].bits != nullptr;
-    if (val)
+    if (f.masked)
         features_tma_kernel<true><<<(unsigned)blocks, kWarps * 32, 0, s>>>(f, map, (int)strip, (int)col_blocks);
     else
         features_tma_kernel<false><<<(unsigned)blocks, kWarps * 32, 0, s>>>(f, map, (int)strip, (int)col_blocks);

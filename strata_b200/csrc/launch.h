@@ -99,35 +99,35 @@ struct alignas(16) LaunchParams {
 
 // The fused multi-output pass (features.cu): several radius-1 ops over one
 // source in one march, terrain.Features / terrain.Surface's outputs from
-// one read of the DEM and one set of Horn differences.
-constexpr int kMaxFeatures = 16;
-struct FeatureSpec {
-    int op, kind;  // the op and its kind (Slope: 0 percent, kSlopeSquareClass)
-    int out;       // its first output (two for a gradient)
-    int nb;        // breaks of its Reclass epilogue (0: none)
-    float k[5];    // the op's constants, as LaunchParams.k
-    float t[kChainBreaks];      // the breaks (a squared magnitude's thresholds for kSlopeSquareClass)
+// one read of the DEM and one set of Horn differences. Each kind of
+// feature it takes has a slot of its own, so the kernel reads every
+// parameter at a fixed place.
+enum { kFGradient, kFSlopeClass, kFSlopePercent, kFWilson, kFTpi, kFRoughness, kFSlots };
+struct FeatureSlot {
+    int on;     // the slot holds a feature
+    int nb;     // breaks of its Reclass epilogue (0: none)
+    float k[5];  // the op's constants, as LaunchParams.k
+    float t[kChainBreaks];      // the breaks (a squared magnitude's thresholds for the classified Slope)
     float v[kChainBreaks + 1];  // the class values
-};
-struct FeatureOut {
-    float* data;
-    int64_t stride;
-    uint32_t* bits;  // null: unmasked
-    int64_t bit_off, bit_stride;
+    float* data[2];       // its outputs (two for a gradient)
+    int64_t stride[2];
+    uint32_t* bits[2];    // null: unmasked
+    int64_t bit_off[2], bit_stride[2];
 };
 struct alignas(16) FeaturesParams {
     LaunchParams g;  // the source, region and status word; g.vf: the source mask (op, constants unused)
-    int nfeat, nout;
-    int horn;  // some feature takes Horn's differences
+    FeatureSlot f[kFSlots];
+    int horn;    // some feature takes Horn's differences
+    int window;  // some feature takes the 3x3 window (ruggedness)
+    int masked;  // some output is masked
     int pad_;
-    FeatureSpec f[kMaxFeatures];
-    FeatureOut o[kMaxFeatures + 1];
 };
-// Whether a planned stage runs in the fused pass: one whose own kernel is
-// bound by memory (Gradient, Slope in percent or classified on its squared
-// magnitude, Wilson's TRI, TPI and roughness at radius 1), with at most one
-// Reclass of kChainBreaks breaks after it, on rows the TMA march takes.
-bool feature_fusable(const LaunchParams& p);
+// The slot of a planned stage in the fused pass, or -1 when it does not
+// run there: only the features whose own kernel is bound by memory
+// (Gradient, Slope in percent or classified on its squared magnitude,
+// Wilson's TRI, TPI and roughness at radius 1), with at most one Reclass
+// of kChainBreaks breaks after it, on rows the TMA march takes.
+int feature_slot(const LaunchParams& p);
 // Launches the fused pass; returns the blocks launched (-1: no kernel) and
 // sets *window_cells to the cells they read.
 int64_t launch_features(const FeaturesParams& p, cudaStream_t stream, int64_t* window_cells);

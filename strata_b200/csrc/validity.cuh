@@ -238,63 +238,5 @@ __device__ __forceinline__ void validity_strip(const ValidityParams& v, int64_t 
     }
 }
 
-// The radius-1 validity of one warp's march unit (the batch kernels): the
-// output cells [xs, xs + 128) (clipped to the region) of rows [y0, y0 +
-// rows), written by the warp right after it marched their cells, so no
-// validity kernel of its own walks them again. Lane l owns the 32 cells
-// xs + 32 (l % 4) .. +31 of every eighth output row from y0 + l / 4: it
-// loads the three source words holding each source row's 34 bits
-// (columns c0-1 .. c0+32) straight from the mask, erodes them across,
-// ANDs three rows, clears the edge ring, and writes the 32 bits at the
-// destination's bit offset (plain stores for words wholly its own,
-// atomics on words shared with other cells).
-__device__ __forceinline__ void march_unit_validity(const ValidityParams& v, int64_t xs, int64_t y0, int rows,
-                                                    int lane) {
-    const int j = lane & 3;
-    const int64_t c0 = xs + 32 * j;
-    const int64_t W = v.width, H = v.height;
-    const int64_t lo = 1 - c0, hi = (W - 1 < v.out_x1 ? W - 1 : v.out_x1) - c0;
-    const uint32_t keep = (lo <= 0 ? 0xffffffffu : (lo >= 32 ? 0u : ~((1u << lo) - 1u))) &
-                          (hi >= 32 ? 0xffffffffu : (hi <= 0 ? 0u : ((1u << hi) - 1u)));
-    const int64_t nreg = v.out_x1 - c0;
-    const uint32_t ours = nreg >= 32 ? 0xffffffffu : (nreg <= 0 ? 0u : ((1u << nreg) - 1u));
-    if (!ours) return;
-    // Row y's source bits eroded across: bit i is the AND of columns c0+i-1 .. c0+i+1.
-    auto eroded = [&](int64_t y) -> uint32_t {
-        if (!v.src_bits) return 0xffffffffu;
-        const int64_t b = v.src_off + (y - v.src_y0) * v.src_stride + (c0 - 1 - v.src_x0);
-        const int64_t w = floor_div32(b);
-        const int sh = (int)(b - w * 32);
-        const uint32_t* m = v.src_bits;
-        const uint32_t a0 = (w >= v.src_lo_word && w <= v.src_hi_word) ? m[w] : 0u;
-        const uint32_t a1 = (w + 1 >= v.src_lo_word && w + 1 <= v.src_hi_word) ? m[w + 1] : 0u;
-        const uint32_t a2 = (w + 2 >= v.src_lo_word && w + 2 <= v.src_hi_word) ? m[w + 2] : 0u;
-        const uint64_t x = (uint64_t)__funnelshift_r(a0, a1, sh) | ((uint64_t)__funnelshift_r(a1, a2, sh) << 32);
-        return (uint32_t)(x & (x >> 1) & (x >> 2));
-    };
-    for (int k = lane >> 2; k < rows; k += 8) {
-        const int64_t y = y0 + k;
-        uint32_t val = 0u;
-        if (y >= 1 && y < H - 1) val = eroded(y - 1) & eroded(y) & eroded(y + 1) & keep;
-        const int64_t D = v.dst_off + (y - v.dst_y0) * v.dst_stride + (c0 - v.dst_x0);
-        const int64_t wb = floor_div32(D);
-        const int sh = (int)(D - wb * 32);
-        auto put = [&](uint32_t* w, uint32_t bits, uint32_t mk) {
-            if (mk == 0xffffffffu) {
-                *w = bits;
-            } else if (mk) {
-                atomicAnd(w, ~mk | bits);
-                atomicOr(w, bits & mk);
-            }
-        };
-        if (sh == 0) {
-            put(v.dst_bits + wb, val, ours);
-        } else {
-            put(v.dst_bits + wb, val << sh, ours << sh);
-            put(v.dst_bits + wb + 1, val >> (32 - sh), ours >> (32 - sh));
-        }
-    }
-}
-
 }  // namespace
 }  // namespace strata
