@@ -16,14 +16,19 @@
 //     128 columns (focal.cuh, in batch_focal.cu).
 // Each raster keeps its own descriptor (the block stages it in shared
 // memory when it reaches the raster's units) and its own band height (the
-// autotuner's choice for its class). The validity of every masked output
-// runs in persistent kernels of its own, one per radius, a warp a unit of
-// 1024 cells by a band of rows (validity.cuh).
+// autotuner's choice for its class). Radius-1 march units of at most 64
+// rows write their outputs' validity themselves after their cells, from
+// mask words copied to shared memory during the march (march_tma.cuh, as
+// the single-raster march does); the other masked outputs' validity runs in
+// persistent kernels of its own, one per radius, a warp a unit of 1024
+// cells by a band of rows (validity.cuh).
 #include <algorithm>
+#include <cstring>
 
 #include "batch.cuh"
 #include "launch.h"
 #include "march.cuh"
+#include "march_tma.cuh"
 #include "validity.cuh"
 
 namespace strata {
@@ -42,8 +47,10 @@ template <int OP, int KIND, bool EPI>
 __global__ void __launch_bounds__(kBatchThreads, 5) batch_march_kernel(const BatchItem* __restrict__ items, int n,
                                                                     int64_t total) {
     __shared__ __align__(16) LaunchParams P;
+    __shared__ uint32_t vwords[kWarps][kVMaxRows * kVWords];
     EpiTables* T = EpiSmem<EPI>::get();
     const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
     int cur = -1;
     for (int64_t u = blockIdx.x; u < total; u += gridDim.x) {
         const int it = batch_item_of(items, n, u);
@@ -59,7 +66,19 @@ __global__ void __launch_bounds__(kBatchThreads, 5) batch_march_kernel(const Bat
         }
         const BatchUnit b = batch_unit(items[it], P, u);
         const int64_t xs = b.x + 128 * warp;
-        if (xs < P.out_x1) march_warp<OP, KIND, EPI>(P, T, xs, b.y0, b.rows, b.vec);
+        if (xs < P.out_x1) {
+            // Units of at most kMaxStrip rows write their outputs' validity
+            // beside their cells (batch_plan sets P.vf for them), from the
+            // source words copied to shared memory while the warp marches.
+            const bool vfused = P.vf.n > 0;
+            if (vfused) valid_prefetch(P, xs, b.y0, b.rows, vwords[warp], lane);
+            march_warp<OP, KIND, EPI>(P, T, xs, b.y0, b.rows, b.vec);
+            if (vfused) {
+                valid_wait(P);
+                valid_strip(P, xs, b.y0, b.rows, vwords[warp], lane);
+                __syncwarp();  // every lane has read the words before the next unit's copies
+            }
+        }
     }
 }
 
@@ -165,6 +184,31 @@ int batch_plan(BatchItem* items, int n, int* order, BatchClass* cls, int64_t* wi
         if (k.family == 0) {
             b.tw = 512;
             b.th = b.th > 0 ? b.th : 32;
+            // A march unit of at most kMaxStrip rows writes its outputs'
+            // validity itself (the kernel's P.vf); batch_plan_validity then
+            // leaves the item out.
+            memset(&b.p.vf, 0, sizeof b.p.vf);
+            bool fuse = b.th <= kMaxStrip && b.nvalid > 0;
+            for (int v = 0; v < b.nvalid && fuse; v++)
+                fuse = b.v[v].radius == 1 && b.v[v].src_x0 == p.src_x0 && b.v[v].src_y0 == p.src_y0 &&
+                       b.v[v].dst_x0 == p.dst_x0 && b.v[v].dst_y0 == p.dst_y0 && b.v[v].out_x0 == p.out_x0 &&
+                       b.v[v].out_x1 == p.out_x1 && b.v[v].width == p.width && b.v[v].height == p.height &&
+                       b.v[v].src_bits == b.v[0].src_bits && b.v[v].src_off == b.v[0].src_off &&
+                       b.v[v].src_stride == b.v[0].src_stride;
+            if (fuse) {
+                FusedValidity& f = b.p.vf;
+                f.src_bits = b.v[0].src_bits;
+                f.src_off = b.v[0].src_off;
+                f.src_stride = b.v[0].src_stride;
+                f.src_lo_word = b.v[0].src_lo_word;
+                f.src_hi_word = b.v[0].src_hi_word;
+                for (int v = 0; v < b.nvalid; v++) {
+                    f.dst_bits[v] = b.v[v].dst_bits;
+                    f.dst_off[v] = b.v[v].dst_off;
+                    f.dst_stride[v] = b.v[v].dst_stride;
+                }
+                f.n = b.nvalid;
+            }
         } else {
             batch_focal_shape(p.op, p.radius, p.kind, b.th, &b.tw, &b.th);
         }
@@ -223,6 +267,7 @@ int batch_plan_validity(const BatchItem* items, int n, ValidityItem* vitems, Val
         ValidityClass c{r, nv, 0, 0};
         for (int i = 0; i < n; i++)
             for (int k = 0; k < items[i].nvalid; k++) {
+                if (items[i].p.vf.n > 0) continue;  // the march units write it
                 const ValidityParams& v = items[i].v[k];
                 if (v.radius != r || v.dst_words <= 0 || v.out_x1 <= v.out_x0 || v.out_y1 <= v.out_y0) continue;
                 ValidityItem& it = vitems[nv++];
