@@ -22,6 +22,8 @@ LIB_PATH = os.path.join(HERE, "liboracle.so")
 
 GRADIENT, SLOPE, ASPECT, HILLSHADE, CURVATURE, RUGGEDNESS = 1, 2, 3, 4, 5, 6
 CORRELATE, SEPARABLE, MEAN, MIN, MAX, LOOKUP, RECLASS = 7, 8, 9, 10, 11, 12, 13
+HEATLOAD, ORIENTATION = 14, 15
+STAGE_FIT = 2  # the derivatives from Wood's quadratic fit over the (2 radius + 1)^2 window
 
 
 class Stage(ctypes.Structure):
@@ -158,10 +160,10 @@ def gaussian(radius, sigma):
 # ---------------------------------------------------------------------------
 # Whole-raster calls.
 
-def stage(op, radius=0, kind=0, k=(), tables=()):
+def stage(op, radius=0, kind=0, k=(), tables=(), flags=0):
     """Builds a Stage; returns (stage, keepalive) so table arrays outlive it."""
     st = Stage()
-    st.op, st.radius, st.kind = op, radius, kind
+    st.op, st.radius, st.kind, st.flags = op, radius, kind, flags
     for i, v in enumerate(k):
         st.k[i] = float(v)
     keep = []
@@ -259,3 +261,74 @@ def pack_mask(valid: np.ndarray) -> np.ndarray:
     if pad:
         bits = np.concatenate([bits, np.zeros(pad, np.uint8)])
     return bits.view(np.uint64).copy()
+
+
+# McCune and Keon's regressions (terrain/heatload.go:104-108): K0, the
+# cos(S) coefficient, the cos(A')sin(S) and sin(S) latitude terms, the
+# folded term and Equation 3's constant.
+HEATLOAD_COEFFICIENTS = [
+    (-1.467, 1.582, -1.500, -0.262, 0.607, 0.0),
+    (-1.236, 1.350, -1.376, -0.331, 0.375, 0.0),
+    (0.339, 0.808, 0.0, -0.196, 0.0, -0.482),
+]
+
+
+def heatload_terms(latitude, equation=0, radiation=False, linear=False):
+    """heatLoadTerms (terrain/heatload.go:110-142): K0, A, BX, BY, E, F, CX,
+    CY in float64, and whether exp is taken."""
+    import math
+
+    k = HEATLOAD_COEFFICIENTS[equation]
+    lat = abs(latitude) * math.pi / 180
+    sin_l, cos_l = math.sin(lat), math.cos(lat)
+    h = math.sqrt(2) / 2
+    cos_c, sin_c = h, h
+    south = latitude < 0
+    if radiation and not south:
+        cos_c, sin_c = 1.0, 0.0
+    elif radiation and south:
+        cos_c, sin_c = -1.0, 0.0
+    elif south:
+        cos_c, sin_c = -h, h
+    kc = k[2] * sin_l + k[5]
+    terms = [k[0], k[1] * cos_l, -kc * sin_c, kc * cos_c, k[3] * sin_l, k[4], cos_c, sin_c]
+    return np.array(terms, np.float64), bool(linear and equation != 2)
+
+
+def fit_scales(fit_radius, cx, cy, z):
+    """newWoodFit's factors kp, kq, kr, kt, ks (terrain/fit.go:38-60), each
+    computed in float64 and rounded once."""
+    r = fit_radius
+    q = float(sum((3 * i * i - r * (r + 1)) ** 2 for i in range(-r, r + 1)))
+    k = float(2 * r + 1)
+    s = float(r * (r + 1) * (2 * r + 1)) / 3
+    return [np.float32(z / (k * s * cx)), np.float32(z / (k * s * cy)), np.float32(6 * z / (k * q * cx * cx)),
+            np.float32(6 * z / (k * q * cy * cy)), np.float32(z / (s * s * cx * cy))]
+
+
+def heatload_stage(cell_size=1.0, cell_size_y=0.0, z_factor=1.0, latitude=45.0, equation=0, radiation=False,
+                   linear=False, fit_radius=0):
+    terms, ex = heatload_terms(latitude, equation, radiation, linear)
+    table = terms.view(np.float32)
+    cx, cy, z = _cells(cell_size, cell_size_y, z_factor)
+    if fit_radius:
+        return stage(HEATLOAD, fit_radius, int(ex), fit_scales(fit_radius, cx, cy, z), [table], STAGE_FIT)
+    kx, ky = horn_scales(cx, cy, z)
+    return stage(HEATLOAD, 1, int(ex), [kx, ky], [table])
+
+
+def orientation_stage(cell_size=1.0, cell_size_y=0.0, z_factor=1.0, east=False, unweighted=False, fit_radius=0):
+    kind = (1 if east else 0) | (2 if unweighted else 0)
+    cx, cy, z = _cells(cell_size, cell_size_y, z_factor)
+    if fit_radius:
+        return stage(ORIENTATION, fit_radius, kind, fit_scales(fit_radius, cx, cy, z), [], STAGE_FIT)
+    kx, ky = horn_scales(cx, cy, z)
+    return stage(ORIENTATION, 1, kind, [kx, ky])
+
+
+def fit_stage(op, fit_radius, cell_size=1.0, cell_size_y=0.0, z_factor=1.0, kind=0, consts=()):
+    """A product of Wood's fit: op GRADIENT, SLOPE (consts: scale; kind: take
+    the arctangent), ASPECT (flat; kind: trigonometric), HILLSHADE (c, bx,
+    by) or CURVATURE (kind)."""
+    cx, cy, z = _cells(cell_size, cell_size_y, z_factor)
+    return stage(op, fit_radius, kind, fit_scales(fit_radius, cx, cy, z) + list(consts), [], STAGE_FIT)

@@ -284,6 +284,7 @@ static int64_t ruggedness_lanes(float *dst, const float *r0, const float *r1, co
 int64_t orc_avx2_row(const orc_stage *st, float *o0, float *o1, const float *r0, const float *r1, const float *r2,
                      int64_t n)
 {
+    if (st->flags & ORC_STAGE_FIT) return 0; /* Wood's fit: the scalar kernels */
     switch (st->op) {
     case ORC_GRADIENT: return gradient_lanes(o0, o1, r0, r1, r2, n, st->k);
     case ORC_SLOPE: return slope_lanes(o0, r0, r1, r2, n, st->k, st->kind != 0);

@@ -251,6 +251,8 @@ static inline float shade(float gx, float gy, float c, float bx, float by)
 /* Per-cell kernels over a window. p points at the window's centre cell;  */
 /* cell (dx, dy) of the window is p[dy * s + dx].                          */
 
+static inline float zt_finish(float P, float Q, float R, float S, float T, int kind);
+
 /* ZT curvature, curvature.go:79-129. */
 static inline float zt_curvature(const float *p, int64_t s, const float *k, int kind)
 {
@@ -265,6 +267,14 @@ static inline float zt_curvature(const float *p, int64_t s, const float *k, int 
     float R = ((z4 + z6) - c) * kr;
     float T = ((z2 + z8) - c) * kt;
     float S = ((z1 + z9) - (z3 + z7)) * ks;
+    return zt_finish(P, Q, R, S, T, kind);
+}
+
+/* CurvatureFromDerivsRow (internal/stencil/curvature.go:138-185): ZT's
+ * formulas from derivatives already computed (ZTCurvatureRow's second
+ * half, so a window's ztDerivs followed by this is ZTCurvatureRow). */
+static inline float zt_finish(float P, float Q, float R, float S, float T, int kind)
+{
     float p2 = P * P, q2 = Q * Q;
     float pq = P * Q;
     if (kind == 0) { /* profile, curvature.go:94-106 */
@@ -287,6 +297,86 @@ static inline float zt_curvature(const float *p, int64_t s, const float *k, int 
     float num = ((1.0f + q2) * R - (pq + pq) * S) + (1.0f + p2) * T;
     float d = w * (float)sqrt((double)w);
     return 0.0f - num / (d + d);
+}
+
+/* heatLoad (internal/stencil/heatload.go:43-53): McCune and Keon's
+ * regression from a gradient, in float64 with every product rounded
+ * before it is added, rounded to float32 once. t holds K0, A, BX, BY, E,
+ * F, CX, CY. */
+static inline float heat_load(float gx, float gy, const double *t, int exp_)
+{
+    const double dx = gx, dy = gy;
+    const double g2 = dx * dx + dy * dy;
+    const double w = 1.0 / sqrt(1.0 + g2);
+    const double fold = fabs(t[6] * dx + t[7] * dy);
+    const double sum = t[1] + t[2] * dx + t[3] * dy + t[4] * sqrt(g2) + t[5] * fold;
+    double v = t[0] + w * sum;
+    if (exp_) v = exp(v);
+    return (float)v;
+}
+
+/* orientation (internal/stencil/orientation.go:31-45): northness (gy) or
+ * eastness (-gx) over sqrt(1 + g2), or over sqrt(g2) unweighted (0 when
+ * flat), in float64, rounded to float32 once. */
+static inline float orientation(float gx, float gy, int east, int unweighted)
+{
+    const double dx = gx, dy = gy;
+    const double c = east ? -dx : dy;
+    const double g2 = dx * dx + dy * dy;
+    if (!unweighted) return (float)(c / sqrt(1.0 + g2));
+    if (g2 == 0) return 0.0f;
+    return (float)(c / sqrt(g2));
+}
+
+/* The 8 float64 terms of a heat load stage, from its table's raw bits. */
+static inline void heat_terms(const orc_stage *st, double *t)
+{
+    memcpy(t, st->table[0], 8 * sizeof(double));
+}
+
+/* Wood's quadratic fit (terrain/fit.go:111-170): the derivatives of the
+ * (2r+1)^2 window around p by the column folds ColumnSum and
+ * ColumnCorrelate (top to bottom) and the row fold RowCorrelate (left to
+ * right) with the integer taps i and 3i^2 - r(r+1), each scaled by its
+ * factor (internal/focalrow/focalrow.go:214-263). want_curv also forms r,
+ * s and t. */
+static void wood_derivs(const float *p, int64_t s, int r, const float *k, int want_curv, float *d)
+{
+    float cs[2 * 8 + 1], cj[2 * 8 + 1], ct[2 * 8 + 1];
+    const float q1 = (float)(r * (r + 1));
+    for (int c = -r; c <= r; c++) {
+        float sum = p[-r * s + c];
+        float cor = (float)(-r) * p[-r * s + c];
+        float co2 = (3.0f * (float)(r * r) - q1) * p[-r * s + c];
+        for (int j = -r + 1; j <= r; j++) {
+            const float v = p[j * s + c];
+            sum = sum + v;
+            cor = cor + (float)j * v;
+            co2 = co2 + ((float)(3 * j * j) - q1) * v;
+        }
+        cs[c + r] = sum;
+        cj[c + r] = cor;
+        ct[c + r] = co2;
+    }
+    /* RowCorrelate from the first product */
+    float P = (float)(-r) * cs[0], Q = 1.0f * cj[0];
+    for (int c = 1; c <= 2 * r; c++) {
+        P = P + (float)(c - r) * cs[c];
+        Q = Q + 1.0f * cj[c];
+    }
+    d[0] = P * k[0];
+    d[1] = Q * k[1];
+    if (!want_curv) return;
+    float R = (3.0f * (float)(r * r) - q1) * cs[0], T = 1.0f * ct[0], S = (float)(-r) * cj[0];
+    for (int c = 1; c <= 2 * r; c++) {
+        const int i = c - r;
+        R = R + ((float)(3 * i * i) - q1) * cs[c];
+        T = T + 1.0f * ct[c];
+        S = S + (float)i * cj[c];
+    }
+    d[2] = R * k[2];
+    d[3] = S * k[4];
+    d[4] = T * k[3];
 }
 
 static inline double sq64(float d) { double x = (double)d; return x * x; }
@@ -500,7 +590,51 @@ static inline float pointwise(const orc_stage *st, float v)
 static inline void stencil_cell(const orc_stage *st, const float *p, int64_t s, float *out)
 {
     const float *k = st->k;
+    if (st->flags & ORC_STAGE_FIT) {
+        /* fitKernel.Process (terrain/fit.go:111-170): the fit's gradient
+         * (p, q) into the from-gradient finishers, or p..t into ZT's
+         * curvature formulas. Constants: k[0..4] the fit's factors, then
+         * the product's (slope scale, aspect flat, hillshade c, bx, by). */
+        float d[5] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+        wood_derivs(p, s, st->radius, k, st->op == ORC_CURVATURE, d);
+        const float gx = d[0], gy = d[1];
+        switch (st->op) {
+        case ORC_GRADIENT: out[0] = gx; out[1] = gy; return;
+        case ORC_SLOPE: out[0] = (st->kind ? orc_atan32(magnitude(gx, gy)) : magnitude(gx, gy)) * k[5]; return;
+        case ORC_ASPECT:
+            out[0] = st->kind ? aspect_degrees(gy, 0.0f - gx, k[5]) : aspect_degrees(0.0f - gx, gy, k[5]);
+            return;
+        case ORC_HILLSHADE: out[0] = shade(gx, gy, k[5], k[6], k[7]); return;
+        case ORC_HEATLOAD: {
+            double t[8];
+            heat_terms(st, t);
+            out[0] = heat_load(gx, gy, t, st->kind & 1);
+            return;
+        }
+        case ORC_ORIENTATION: out[0] = orientation(gx, gy, st->kind & 1, (st->kind >> 1) & 1); return;
+        default: out[0] = zt_finish(d[0], d[1], d[2], d[3], d[4], st->kind); return;
+        }
+    }
     switch (st->op) {
+    case ORC_HEATLOAD:
+    case ORC_ORIENTATION: {
+        /* heatLoadKernel / orientationKernel (terrain/heatload.go:147-160,
+         * terrain/orientation.go:83-95): Horn's gradient, then the
+         * from-gradient equation. */
+        float z1 = p[-s - 1], z2 = p[-s], z3 = p[-s + 1];
+        float z4 = p[-1], z6 = p[1];
+        float z7 = p[s - 1], z8 = p[s], z9 = p[s + 1];
+        float gx = horn_dx(z1, z3, z4, z6, z7, z9) * k[0];
+        float gy = horn_dy(z1, z2, z3, z7, z8, z9) * k[1];
+        if (st->op == ORC_HEATLOAD) {
+            double t[8];
+            heat_terms(st, t);
+            out[0] = heat_load(gx, gy, t, st->kind & 1);
+        } else {
+            out[0] = orientation(gx, gy, st->kind & 1, (st->kind >> 1) & 1);
+        }
+        return;
+    }
     case ORC_GRADIENT:
     case ORC_SLOPE:
     case ORC_ASPECT:
@@ -588,6 +722,15 @@ static void stencil_row(const orc_stage *st, const float *row, int64_t s, int64_
 {
     const float *k = st->k;
     int r = st->radius;
+    if (st->flags & ORC_STAGE_FIT) { /* Wood's fit: cell by cell */
+        for (int64_t x = x0; x < x1; x++) {
+            float out[2];
+            stencil_cell(st, row + x, s, out);
+            o0[x] = out[0];
+            if (o1) o1[x] = out[1];
+        }
+        return;
+    }
     switch (st->op) {
     case ORC_GRADIENT:
         for (int64_t x = x0; x < x1; x++) {
@@ -847,7 +990,9 @@ int orc_process_ex(const orc_stage *stages, int nstages, const orc_raster *src,
 {
     if (nstages < 1 || !src || !dst) return -1;
     const orc_stage *st = &stages[0];
-    if (st->op < ORC_GRADIENT || st->op > ORC_RECLASS) return -1;
+    if (st->op < ORC_GRADIENT || st->op > ORC_ORIENTATION) return -1;
+    if ((st->flags & ORC_STAGE_FIT) && (st->radius < 1 || st->radius > 8)) return -1;
+    if ((st->op == ORC_HEATLOAD) && (!st->table[0] || st->table_len[0] != 16)) return -1;
     for (int i = 1; i < nstages; i++)
         if (stages[i].op != ORC_LOOKUP && stages[i].op != ORC_RECLASS) return -1;
     /* Pointwise tables: Lookup's knots and values pair up (at least one);
@@ -871,7 +1016,10 @@ int orc_process_ex(const orc_stage *stages, int nstages, const orc_raster *src,
     jb.dst = dst;
     jb.ndst = ndst;
     jb.simd = simd;
-    jb.r = (st->op == ORC_LOOKUP || st->op == ORC_RECLASS) ? 0 : (st->op <= ORC_HILLSHADE || st->op == ORC_CURVATURE ? 1 : st->radius);
+    jb.r = (st->op == ORC_LOOKUP || st->op == ORC_RECLASS) ? 0
+           : (st->flags & ORC_STAGE_FIT) ? st->radius
+           : (st->op <= ORC_HILLSHADE || st->op == ORC_CURVATURE || st->op >= ORC_HEATLOAD) ? 1
+           : st->radius;
     /* Bands of about 2^16 cells, whole rows, as internal/exec/tile.go:21-27. */
     int64_t rows = (int64_t)65536 / (src->width > 0 ? src->width : 1);
     jb.band_rows = rows < 1 ? 1 : rows;

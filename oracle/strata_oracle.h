@@ -31,8 +31,14 @@ enum {
     ORC_MIN = 10,
     ORC_MAX = 11,
     ORC_LOOKUP = 12,
-    ORC_RECLASS = 13
+    ORC_RECLASS = 13,
+    ORC_HEATLOAD = 14,
+    ORC_ORIENTATION = 15
 };
+
+/* orc_stage.flags: the stage's derivatives come from Wood's quadratic fit
+ * over the (2 radius + 1)^2 window (terrain/fit.go), not Horn's 3x3. */
+#define ORC_STAGE_FIT 2
 
 /* One stage of a call. k[] holds the op's float constants, table[] its
  * weights, taps or knots (see include/strata_cuda.h for the slot meaning). */

@@ -208,6 +208,42 @@ cases["nan_payload"] = {
     "src": ["0x7fc00001", "0xffc00000"],
 }
 
+# terrain/heatload_test.go:15-47 (mcCuneKeonTest, TestHeatLoadMcCuneKeon,
+# :66-109): McCune and Keon's spreadsheet, latitude, slope and aspect in
+# degrees, then Equations 1-3 for radiation and for heat load, each as the
+# equation gives it (ln for 1 and 2), held to 2e-6 on a 5x5 plane on unit
+# cells (z = +-tan(slope) * row).
+cases["heatload_mccune_keon"] = {
+    "cite": "terrain/heatload_test.go:15-47,66-109",
+    "tol": 2e-6,
+    "rows": [
+        [40, 0, 0, [-0.25511769098577686, -0.20184000178937955, 0.9579639100401343],
+         [-0.25511769098577686, -0.20184000178937955, 0.9579639100401343]],
+        [40, 30, 0, [-0.9837750181305804, -0.8890103948393941, 0.5710452843712215],
+         [-0.6279670110295916, -0.6268993985409437, 0.6416325501052635]],
+        [40, 30, 180, [-0.01959360360077163, -0.00453464391071629, 1.0530452843712215],
+         [0.053812205478473735, -0.001480597264211625, 0.9824580186371794]],
+        [60, 0, 0, [-0.6759999999999998, -0.5609999999999998, 0.7430000000000001],
+         [-0.6759999999999998, -0.5609999999999998, 0.7430000000000001]],
+        [60, 30, 0, [-1.544942286340599, -1.3905855345755218, 0.36300377355803837],
+         [-1.1400956521839989, -1.0834897710580573, 0.4335910392920804]],
+        [60, 30, 180, [-0.24590418066394135, -0.19893457896813463, 0.8450037735580384],
+         [-0.22153699864030738, -0.24086529954064415, 0.7744165078239963]],
+    ],
+}
+
+# terrain/orientation_test.go:76-101 (TestOrientationCardinal): planes
+# z = a*x + b*y + 100 on unit cells; at cell (2, 2) of a 5x5 DEM the
+# unweighted and weighted components are exactly these float32 values.
+cases["orientation_cardinal"] = {
+    "cite": "terrain/orientation_test.go:76-101",
+    "rows": [
+        {"a": 0, "b": 3, "north": b(1), "east": b(0), "northW": b(3 / math.sqrt(10)), "eastW": b(0)},
+        {"a": 0, "b": -3, "north": b(-1), "east": b(0), "northW": b(-3 / math.sqrt(10)), "eastW": b(0)},
+        {"a": -2, "b": 0, "north": b(0), "east": b(1), "northW": b(0), "eastW": b(2 / math.sqrt(5))},
+    ],
+}
+
 if __name__ == "__main__":
     out = os.path.join(HERE, "kat.json")
     with open(out, "w") as f:

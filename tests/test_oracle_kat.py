@@ -361,3 +361,116 @@ def test_pointwise_tables_checked():
     for st in bad:
         with pytest.raises(ValueError):
             run([st], src)
+
+
+# ---------------------------------------------------------------------------
+# HeatLoad, Orientation and Wood's fit (terrain/heatload.go, orientation.go,
+# fit.go): the reference's known answers and closed forms.
+
+def _run1(stage, cells, nout=1):
+    h, w = cells.shape
+    src = dict(data=np.ascontiguousarray(cells, np.float32).reshape(-1), width=w, height=h, stride=w, valid=None,
+               valid_offset=0)
+    outs = [dict(data=np.full(w * h, 7.0, np.float32), width=w, height=h, stride=w, valid=None, valid_offset=0)
+            for _ in range(nout)]
+    orc.process([stage], src, outs)
+    return [o["data"].reshape(h, w) for o in outs]
+
+
+def _plane(w, h, a, b_, cs=1.0, csy=1.0):
+    """terrain/terrain_test.go:28-36: z = a*x*cs + b*y*csy + 100, as float32."""
+    y, x = np.mgrid[0:h, 0:w].astype(np.float64)
+    return (a * x * cs + b_ * y * csy + 100).astype(np.float32)
+
+
+def test_heatload_mccune_keon_table():
+    """TestHeatLoadMcCuneKeon (terrain/heatload_test.go:66-109): all 36
+    values of the authors' spreadsheet and the arithmetic-scale column."""
+    case = KAT["heatload_mccune_keon"]
+    for lat, slope, aspect, rad, heat in case["rows"]:
+        t = math.tan(slope * math.pi / 180) * (-1 if aspect == 180 else 1)
+        dem = np.array([[t * y for _x in range(5)] for y in range(5)], np.float32)
+        for eq in range(3):
+            for radiation in (True, False):
+                want = (rad if radiation else heat)[eq]
+                for linear in (False, True):
+                    w = math.exp(want) if linear and eq < 2 else want
+                    (got,) = _run1(orc.heatload_stage(1.0, latitude=lat, equation=eq, radiation=radiation,
+                                                      linear=linear), dem)
+                    assert np.isnan(got[0]).all() and np.isnan(got[:, 0]).all()
+                    inner = got[1:-1, 1:-1].astype(np.float64)
+                    assert np.abs(inner - w).max() <= case["tol"], (lat, slope, aspect, eq, radiation, linear)
+
+
+def test_orientation_cardinal_exact():
+    """TestOrientationCardinal (terrain/orientation_test.go:76-101)."""
+    for row in KAT["orientation_cardinal"]["rows"]:
+        dem = _plane(5, 5, row["a"], row["b"])
+        for unweighted in (True, False):
+            for east, key in ((False, "north"), (True, "east")):
+                (got,) = _run1(orc.orientation_stage(1.0, east=east, unweighted=unweighted), dem)
+                want = f(row[key] if unweighted else row[key + "W"])
+                assert got[2, 2] == want, (row, east, unweighted, got[2, 2], want)
+
+
+def test_orientation_planes():
+    """TestOrientationPlanes (terrain/orientation_test.go:41-74): the eight
+    compass directions at four steepnesses against the closed form."""
+    for da, db in ((0, 1), (1, 1), (1, 0), (1, -1), (0, -1), (-1, -1), (-1, 0), (-1, 1)):
+        for steep in (0.05, 0.5, 1, 4):
+            a, b_ = da * steep, db * steep
+            dem = _plane(7, 6, a, b_, 10, 10)
+            for east in (False, True):
+                for unweighted in (False, True):
+                    comp = -a if east else b_
+                    want = comp / (math.hypot(a, b_) if unweighted else math.sqrt(1 + a * a + b_ * b_))
+                    (got,) = _run1(orc.orientation_stage(10.0, east=east, unweighted=unweighted), dem)
+                    assert np.abs(got[1:-1, 1:-1] - want).max() <= 1e-6
+
+
+def test_fit_plane():
+    """TestFitPlane (terrain/fit_test.go:36-72): on a plane the fit's
+    gradient is the plane's and every curvature is +0, edges NaN."""
+    for a, b_ in ((0, 0), (1, 0), (0, -3), (2, 5), (-7, 4)):
+        for r in range(1, 9):
+            dem = _plane(2 * r + 5, 2 * r + 4, a, b_)
+            gx, gy = _run1(orc.fit_stage(orc.GRADIENT, r, 1.0), dem, 2)
+            inner = (slice(r, -r), slice(r, -r))
+            assert np.isnan(gx[:r]).all() and np.isnan(gy[:, :r]).all()
+            assert np.abs(gx[inner] - a).max() <= 1e-6 * abs(a)
+            assert np.abs(gy[inner] - b_).max() <= 1e-6 * abs(b_)
+            for kind in range(3):
+                (cv,) = _run1(orc.fit_stage(orc.CURVATURE, r, 1.0, kind=kind), dem)
+                assert (cv[inner].view(np.uint32) == 0).all(), (a, b_, r, kind)
+
+
+def test_fit_quadratic():
+    """TestFitQuadratic (terrain/fit_test.go:74-132): least squares fits a
+    quadratic exactly, so the fit's gradient and curvatures are the
+    surface's, within the float32 rounding of the elevations' sums."""
+    w, h = 40, 36
+    cx, cy, zf = 2.0, 3.0, 1.5
+    c = (0.03, -0.02, 0.01, 0.4, -0.25, 50)
+    yy, xx = np.mgrid[0:h, 0:w].astype(np.float64)
+    X, Y = xx * cx, yy * cy
+    dem = (c[0] * X * X + c[1] * Y * Y + c[2] * X * Y + c[3] * X + c[4] * Y + c[5]).astype(np.float32)
+    zmax = float(np.abs(dem).max())
+    for r in (1, 2, 4, 8):
+        gx, gy = _run1(orc.fit_stage(orc.GRADIENT, r, cx, cy, zf), dem, 2)
+        k = 2 * r + 1
+        e = 4 * k * k * zmax * 2.0 ** -24
+        s2 = r * (r + 1) * (2 * r + 1) / 3
+        inner = (slice(r, h - r), slice(r, w - r))
+        p = zf * (2 * c[0] * X + c[2] * Y + c[3])[inner]
+        q = zf * (2 * c[1] * Y + c[2] * X + c[4])[inner]
+        assert (np.abs(gx[inner] - p) <= zf * e * r * k / (k * s2 * cx) + 1e-6 * np.abs(p)).all()
+        assert (np.abs(gy[inner] - q) <= zf * e * r * k / (k * s2 * cy) + 1e-6 * np.abs(q)).all()
+        rr, tt, ss = zf * 2 * c[0], zf * 2 * c[1], zf * c[2]
+        g = p * p + q * q
+        want = [-(p * p * rr + 2 * p * q * ss + q * q * tt) / (g * (1 + g) ** 1.5),
+                -(q * q * rr - 2 * p * q * ss + p * p * tt) / g ** 1.5,
+                -((1 + q * q) * rr - 2 * p * q * ss + (1 + p * p) * tt) / (2 * (1 + g) ** 1.5)]
+        for kind in range(3):
+            (cv,) = _run1(orc.fit_stage(orc.CURVATURE, r, cx, cy, zf, kind=kind), dem)
+            got = cv[inner].astype(np.float64)
+            assert (np.abs(got - want[kind]) <= 2e-3 * np.abs(want[kind]) + 1e-6).all(), (r, kind)
