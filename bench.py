@@ -914,6 +914,8 @@ def _orc_of(st):
     constants and tables)."""
     import ctypes
 
+    from strata_b200 import _lib
+
     tables = []
     for i in range(4):
         n = st.table_len[i]
@@ -921,7 +923,7 @@ def _orc_of(st):
                       if st.table[i] and n > 0 else np.zeros(0, np.float32))
     while tables and tables[-1].size == 0:
         tables.pop()
-    return _orc().stage(st.op, st.radius, st.kind, list(st.k), tables)
+    return _orc().stage(st.op, st.radius, st.kind, list(st.k), tables, flags=st.flags & _lib.STAGE_FIT)
 
 
 def _summary(line, keys):

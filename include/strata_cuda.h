@@ -60,7 +60,9 @@ enum {
     STRATA_OP_MIN = 10,       /* focal.Min, radius 1..8 */
     STRATA_OP_MAX = 11,       /* focal.Max, radius 1..8 */
     STRATA_OP_LOOKUP = 12,    /* transfer.Lookup, pointwise */
-    STRATA_OP_RECLASS = 13    /* transfer.Reclass, pointwise */
+    STRATA_OP_RECLASS = 13,   /* transfer.Reclass, pointwise */
+    STRATA_OP_HEATLOAD = 14,  /* terrain.HeatLoad (McCune and Keon), radius 1 */
+    STRATA_OP_ORIENTATION = 15 /* terrain.Orientation (northness / eastness), radius 1 */
 };
 
 /* strata_stage.kind for STRATA_OP_CURVATURE (stencil.CurvatureKind). */
@@ -70,6 +72,7 @@ enum { STRATA_RUG_TRI_RILEY = 0, STRATA_RUG_TRI_WILSON = 1, STRATA_RUG_TPI = 2, 
 
 /* strata_stage.flags. */
 #define STRATA_STAGE_ROTATE180 1 /* correlate with the weights rotated by 180 degrees (Convolve) */
+#define STRATA_STAGE_FIT 2       /* the derivatives from Wood's quadratic fit over the (2 radius + 1)^2 window */
 
 /* Largest tables a stage may carry. */
 #define STRATA_MAX_RADIUS 8
@@ -107,6 +110,15 @@ typedef struct {
  *   MEAN/MIN/MAX radius
  *   LOOKUP     table[0]=xs table[1]=ys (table_len[0] knots)
  *   RECLASS    table[0]=breaks (table_len[0]) table[1]=values (table_len[0]+1)
+ *   HEATLOAD   k[0]=kx k[1]=ky, table[0]=the regression's eight float64
+ *              terms K0 A BX BY E F CX CY as 16 floats, kind=1 takes exp
+ *   ORIENTATION k[0]=kx k[1]=ky, kind bit 0 eastness, bit 1 unweighted
+ * With flags STRATA_STAGE_FIT (terrain/fit.go, FitRadius > 0) a GRADIENT,
+ * SLOPE, ASPECT, HILLSHADE, HEATLOAD, ORIENTATION or CURVATURE stage takes
+ * its derivatives from Wood's quadratic fit: radius is the fit's,
+ * k[0..4]=kp kq kr kt ks its factors, and the product's constants follow
+ * from k[5] (SLOPE scale; ASPECT flat; HILLSHADE c bx by); kind and
+ * table[0] mean what they mean without the flag.
  * Tables are host memory, read during the call only.
  */
 typedef struct {
@@ -380,6 +392,28 @@ typedef struct { int32_t radius; int32_t nweights; const float *weights; } strat
 typedef struct { int32_t radius; int32_t nrow; const float *row; int32_t ncol; int32_t reserved; const float *col; } strata_separable_options;
 typedef struct { int32_t radius; } strata_box_options;
 
+/* equation: 0..2 (terrain.HeatLoadEquation); latitude in degrees. The
+ * builder writes the regression's terms into terms, and the stage points
+ * at them: the options must outlive the stage's use. */
+typedef struct {
+    double cell_size, cell_size_y, z_factor;
+    int32_t fit_radius;
+    int32_t equation;
+    double latitude;
+    int32_t radiation, linear;
+    double terms[8];
+} strata_heatload_options;
+/* component: 0 northness, 1 eastness (terrain.OrientationComponent) */
+typedef struct {
+    double cell_size, cell_size_y, z_factor;
+    int32_t fit_radius;
+    int32_t component;
+    int32_t unweighted;
+    int32_t reserved;
+} strata_orientation_options;
+
+/* The builders of the terrain ops take fit_radius 1..8 as the reference
+ * does (terrain/fit.go:187-226, newWoodFit :38-66): Wood's quadratic fit. */
 /* terrain.newGradientKernel (terrain/gradient.go:70-73). */
 int strata_stage_gradient(const strata_gradient_options *o, strata_stage *out);
 /* terrain.newSlopeKernel / slopeScale (terrain/slope.go:76-95). */
@@ -404,6 +438,10 @@ int strata_stage_lookup(const float *xs, const float *ys, int32_t n, strata_stag
 /* transfer.newReclassKernel (transfer/transfer.go:187-195). */
 int strata_stage_reclass(const float *breaks, int32_t nbreaks, const float *values, int32_t nvalues,
                          strata_stage *out);
+/* terrain.heatLoadOp / heatLoadTerms (terrain/heatload.go:110-146). */
+int strata_stage_heatload(strata_heatload_options *o, strata_stage *out);
+/* terrain.orientationOp (terrain/orientation.go:55-76). */
+int strata_stage_orientation(const strata_orientation_options *o, strata_stage *out);
 /* focal.Gaussian (focal/separable.go:59-76): 2*radius+1 taps into taps. */
 int strata_focal_gaussian(int32_t radius, double sigma, float *taps);
 

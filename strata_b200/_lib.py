@@ -19,7 +19,9 @@ OK, EINVAL, ECUDA, ENOMEM, ECANCELED, ETIMEDOUT, EIO, ENOTSUP = 0, -1, -2, -3, -
 
 OP_GRADIENT, OP_SLOPE, OP_ASPECT, OP_HILLSHADE, OP_CURVATURE, OP_RUGGEDNESS = 1, 2, 3, 4, 5, 6
 OP_CORRELATE, OP_SEPARABLE, OP_MEAN, OP_MIN, OP_MAX, OP_LOOKUP, OP_RECLASS = 7, 8, 9, 10, 11, 12, 13
+OP_HEATLOAD, OP_ORIENTATION = 14, 15
 STAGE_ROTATE180 = 1
+STAGE_FIT = 2
 EXEC_ASYNC = 1
 MAX_RADIUS = 8
 MAX_KNOTS = 64
@@ -123,6 +125,17 @@ class CurvatureOptions(ctypes.Structure):
                 ("fit_radius", c_i32), ("type", c_i32)]
 
 
+class HeatLoadOptions(ctypes.Structure):
+    _fields_ = [("cell_size", c_f64), ("cell_size_y", c_f64), ("z_factor", c_f64),
+                ("fit_radius", c_i32), ("equation", c_i32), ("latitude", c_f64),
+                ("radiation", c_i32), ("linear", c_i32), ("terms", c_f64 * 8)]
+
+
+class OrientationOptions(ctypes.Structure):
+    _fields_ = [("cell_size", c_f64), ("cell_size_y", c_f64), ("z_factor", c_f64),
+                ("fit_radius", c_i32), ("component", c_i32), ("unweighted", c_i32), ("reserved", c_i32)]
+
+
 class RuggednessOptions(ctypes.Structure):
     _fields_ = [("type", c_i32), ("radius", c_i32)]
 
@@ -191,6 +204,8 @@ SIGNATURES = [
     ("strata_stage_box", ctypes.c_int, [ctypes.POINTER(BoxOptions), ctypes.c_uint32, ctypes.POINTER(Stage)]),
     ("strata_stage_lookup", ctypes.c_int, [c_p, c_p, c_i32, ctypes.POINTER(Stage)]),
     ("strata_stage_reclass", ctypes.c_int, [c_p, c_i32, c_p, c_i32, ctypes.POINTER(Stage)]),
+    ("strata_stage_heatload", ctypes.c_int, [ctypes.POINTER(HeatLoadOptions), ctypes.POINTER(Stage)]),
+    ("strata_stage_orientation", ctypes.c_int, [ctypes.POINTER(OrientationOptions), ctypes.POINTER(Stage)]),
     ("strata_focal_gaussian", ctypes.c_int, [c_i32, c_f64, ctypes.POINTER(c_f32)]),
 ]
 

@@ -154,6 +154,11 @@ struct strata_ctx {
 
 namespace {
 
+// Context buffer slots: 0 and 1 a host source's cells and mask, 2 + 2i
+// and 3 + 2i host destination i's; from kFitScratchSlot the raw sums of
+// Wood's fit.
+constexpr int kFitScratchSlot = 128;
+
 int ensure(strata_ctx* c, int slot, size_t bytes, void** out) {
     if ((int)c->bufs.size() <= slot) c->bufs.resize(slot + 1);
     auto& b = c->bufs[slot];
@@ -362,7 +367,10 @@ bool bit_spans(const strata_raster& a, const strata_raster& b) {
 bool is_pointwise(uint32_t op) { return op == STRATA_OP_LOOKUP || op == STRATA_OP_RECLASS; }
 
 int op_radius(const strata_stage& s) {
+    if (s.flags & STRATA_STAGE_FIT) return s.radius;
     switch (s.op) {
+    case STRATA_OP_HEATLOAD:
+    case STRATA_OP_ORIENTATION:
     case STRATA_OP_GRADIENT:
     case STRATA_OP_SLOPE:
     case STRATA_OP_ASPECT:
@@ -404,6 +412,19 @@ int fill_stage(const strata_stage& s, LaunchParams& p, int epi_index) {
     p.op = (int)s.op;
     p.radius = op_radius(s);
     p.kind = s.kind;
+    p.fit = 0;
+    if (s.flags & STRATA_STAGE_FIT) {
+        const bool product = (s.op >= STRATA_OP_GRADIENT && s.op <= STRATA_OP_CURVATURE) ||
+                             s.op == STRATA_OP_HEATLOAD || s.op == STRATA_OP_ORIENTATION;
+        if (!product || s.radius < 1 || s.radius > STRATA_MAX_RADIUS)
+            return fail(STRATA_EINVAL, "terrain: FitRadius must be 0 to %d, got %d", STRATA_MAX_RADIUS, s.radius);
+        p.fit = s.radius;
+    }
+    if (s.op == STRATA_OP_HEATLOAD) {
+        if (!s.table[0] || s.table_len[0] != 16)
+            return fail(STRATA_EINVAL, "engine: a heat load stage carries its 8 float64 terms in 16 table slots");
+        memcpy(p.w, s.table[0], 16 * sizeof(float));
+    }
     // Slope and Aspect read their kind as a flag (take the arctangent;
     // trigonometric angles).
     if (s.op == STRATA_OP_SLOPE || s.op == STRATA_OP_ASPECT) p.kind = s.kind != 0;
@@ -653,7 +674,7 @@ float host_slope_of_square(float s, float scale, bool take_atan) {
 void fold_slope_square(LaunchParams& p) {
     if (p.op != STRATA_OP_SLOPE || p.nepi != 1 || p.epi[0].op != STRATA_OP_RECLASS) return;
     EpiStage& e = p.epi[0];
-    const float scale = p.k[2];
+    const float scale = p.k[p.fit ? 5 : 2];  // a fit's product constants follow its five factors
     if (e.n > strata::kChainBreaks || !(scale > 0) || std::isinf(scale)) return;
     const bool take_atan = p.kind != 0;
     const float inf = std::numeric_limits<float>::infinity();
@@ -683,7 +704,7 @@ int plan_stages(const strata_stage* stages, int nstages, LaunchParams& p, int* n
     if (!stages || nstages < 1) return fail(STRATA_EINVAL, "engine: nil kernel");
     memset(&p, 0, sizeof p);
     const strata_stage& s0 = stages[0];
-    if (s0.op < STRATA_OP_GRADIENT || s0.op > STRATA_OP_RECLASS)
+    if (s0.op < STRATA_OP_GRADIENT || s0.op > STRATA_OP_ORIENTATION)
         return fail(STRATA_EINVAL, "engine: unknown op %u", s0.op);
     int epi = 0;
     int rc;
@@ -915,6 +936,64 @@ void fill_validity(ValidityParams& v, const DevOperand& s, bool src_masked, cons
 
 
 
+// Wood's fit on the device (terrain/fit.go:111-170). Each raw fit sum is a
+// separable correlation of the window: the column fold ColumnSum is the
+// column correlation with unit taps (1·z is z exactly, so copying the first
+// row and adding the rest gives the same bits), so p's sum is
+// CorrelateSeparable with column taps 1 and row taps i, q's with column
+// taps i and row taps 1, and curvature's r, s, t with (1, 3i²-r(r+1)),
+// (i, i) and (3i²-r(r+1), 1): the separable kernels compute them in the
+// reference's fold orders. The sums land in context scratch with the
+// output's geometry, then the finishing pass scales them and applies the
+// product (launch_fit_finish), and the validity kernel erodes the mask by
+// the fit's radius.
+int64_t launch_fit(strata_ctx* c, const LaunchParams& p, const ValidityParams* const v[2], cudaStream_t st,
+                   int64_t* window) {
+    const int r = p.fit;
+    const int nd = p.op == STRATA_OP_CURVATURE ? 5 : 2;
+    const int64_t ds = p.out_x1 - p.dst_x0, rows = p.out_y1 - p.dst_y0;
+    float* d[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    for (int i = 0; i < nd; i++) {
+        void* q;
+        if (ensure(c, kFitScratchSlot + i, (size_t)(rows * ds) * 4, &q)) return -2;
+        d[i] = static_cast<float*>(q);
+    }
+    float ti[2 * STRATA_MAX_RADIUS + 1], t2[2 * STRATA_MAX_RADIUS + 1], ones[2 * STRATA_MAX_RADIUS + 1];
+    for (int i = -r; i <= r; i++) {
+        ti[i + r] = (float)i;
+        t2[i + r] = (float)(3 * i * i - r * (r + 1));
+        ones[i + r] = 1.0f;
+    }
+    // (column taps, row taps) of p, q, r, s, t
+    const float* taps[5][2] = {{ones, ti}, {ti, ones}, {ones, t2}, {ti, ti}, {t2, ones}};
+    int64_t blocks = 0, cells = 0;
+    for (int i = 0; i < nd; i++) {
+        LaunchParams q = p;
+        q.op = STRATA_OP_SEPARABLE;
+        q.kind = 0;
+        q.fit = 0;
+        q.nepi = 0;
+        memset(&q.vf, 0, sizeof q.vf);
+        for (int j = 0; j <= 2 * r; j++) {
+            q.w[j] = taps[i][1][j];
+            q.w[17 + j] = taps[i][0][j];
+        }
+        q.dst0 = d[i];
+        q.dst0_stride = ds;
+        q.dst1 = nullptr;
+        int64_t wc = 0;
+        const int64_t t = strata::launch_data(q, st, &wc);
+        if (t < 0) return -1;
+        blocks += t;
+        cells += wc;
+    }
+    strata::launch_fit_finish(p, d, ds, st);
+    for (int i = 0; i < 2; i++)
+        if (v[i]) strata::launch_validity(*v[i], st);
+    if (window) *window = cells;
+    return blocks;
+}
+
 // The failure-path test's switch (STRATA_TEST_STALL_FIRST_WAIT=1): the TMA
 // march then reports a bounded wait that ran out, with nothing faulted.
 bool test_stall_requested() {
@@ -991,7 +1070,8 @@ extern "C" int strata_process(strata_ctx* c, const strata_stage* stages, int nst
             fill_validity(vp[i], ds, src[0].valid != nullptr, dd[i], span_cells(dst[i]), W, H, p.radius, y0, y1);
             vs[i] = &vp[i];
         }
-        int64_t t = strata::launch_stage(p, vs, st, &wc);
+        int64_t t = p.fit ? launch_fit(c, p, vs, st, &wc) : strata::launch_stage(p, vs, st, &wc);
+        if (t == -2) return fail(STRATA_ENOMEM, "engine: no device memory for the fit's sums");
         if (t < 0) return fail(STRATA_ENOTSUP, "engine: op %d at radius %d has no device kernel", p.op, p.radius);
         bands += t;
         window += wc;
@@ -1070,10 +1150,71 @@ int horn_scales(double cs, double csy, double z, float* kx, float* ky) {
 // The fit-radius switch of terrain/fit.go:187-226: 0 is Horn's 3x3
 // kernel, 1..8 Wood's fit (checked at terrain/fit.go:37-40).
 int fit_radius(int32_t fr) {
-    if (fr == 0) return STRATA_OK;
     if (fr < 0 || fr > STRATA_MAX_RADIUS)
         return fail(STRATA_EINVAL, "terrain: FitRadius must be 0 to %d, got %d", STRATA_MAX_RADIUS, fr);
-    return fail(STRATA_ENOTSUP, "terrain: FitRadius %d (Wood's quadratic fit) is not on the gpu backend", fr);
+    return STRATA_OK;
+}
+
+// newWoodFit (terrain/fit.go:38-66): the fit's factors kp, kq, kr, kt, ks,
+// each computed in float64 and rounded once.
+int wood_fit(int r, double cs, double csy, double zf, float* k) {
+    double cx, cy, z;
+    int rc = resolve_cells(cs, csy, zf, &cx, &cy, &z);
+    if (rc) return rc;
+    double q = 0;
+    for (int i = -r; i <= r; i++) {
+        const double w = 3.0 * i * i - r * (r + 1);
+        q += w * w;
+    }
+    const double kk = 2 * r + 1, s = (double)(r * (r + 1) * (2 * r + 1)) / 3;
+    k[0] = (float)(z / (kk * s * cx));
+    k[1] = (float)(z / (kk * s * cy));
+    k[2] = (float)(6 * z / (kk * q * cx * cx));
+    k[3] = (float)(6 * z / (kk * q * cy * cy));
+    k[4] = (float)(z / (s * s * cx * cy));
+    for (int i = 0; i < 5; i++)
+        if (!usable(k[i]))
+            return fail(STRATA_EINVAL,
+                        "terrain: the quadratic fit's factors ZFactor/(K·S·CellSize), 6·ZFactor/(K·Q·CellSize²) and "
+                        "ZFactor/(S²·CellSize·CellSizeY), and the same for CellSizeY, must be finite and non-zero as "
+                        "float32, got %s, %s, %s, %s and %s for CellSize %s, CellSizeY %s, ZFactor %s and FitRadius %d",
+                        fmt_v(k[0], true).c_str(), fmt_v(k[1], true).c_str(), fmt_v(k[2], true).c_str(),
+                        fmt_v(k[3], true).c_str(), fmt_v(k[4], true).c_str(), fmt_v(cs).c_str(), fmt_v(csy).c_str(),
+                        fmt_v(zf).c_str(), r);
+    return STRATA_OK;
+}
+
+// The derivative part of a terrain stage: Horn's 3x3 scales (kx, ky in
+// k[0..1], radius 1) when fr is 0, else Wood's fit (fit_stage); *base is
+// where the product's constants go (2 for Horn, 5 for the fit).
+int fit_stage(uint32_t op, int r, double cs, double csy, double z, strata_stage* out);
+int deriv_stage(uint32_t op, int fr, double cs, double csy, double z, strata_stage* out, int* base) {
+    if (fr) {
+        *base = 5;
+        return fit_stage(op, fr, cs, csy, z, out);
+    }
+    float kx, ky;
+    int rc = horn_scales(cs, csy, z, &kx, &ky);
+    if (rc) return rc;
+    stage_init(out, op);
+    out->radius = 1;
+    out->k[0] = kx;
+    out->k[1] = ky;
+    *base = 2;
+    return STRATA_OK;
+}
+
+// A product of Wood's fit (terrain/fit.go:187-226): the op, the fit's
+// radius and factors; the caller adds the product's constants from k[5].
+int fit_stage(uint32_t op, int r, double cs, double csy, double z, strata_stage* out) {
+    float k[5];
+    int rc = wood_fit(r, cs, csy, z, k);
+    if (rc) return rc;
+    stage_init(out, op);
+    out->radius = r;
+    out->flags = STRATA_STAGE_FIT;
+    for (int i = 0; i < 5; i++) out->k[i] = k[i];
+    return STRATA_OK;
 }
 
 int check_focal_radius(int r) {
@@ -1107,6 +1248,8 @@ extern "C" int strata_stage_gradient(const strata_gradient_options* o, strata_st
     if (!o || !out) return fail(STRATA_EINVAL, "terrain: nil options");
     int rc = fit_radius(o->fit_radius);
     if (rc) return rc;
+    if (o->fit_radius)
+        return fit_stage(STRATA_OP_GRADIENT, o->fit_radius, o->cell_size, o->cell_size_y, o->z_factor, out);
     float kx, ky;
     if ((rc = horn_scales(o->cell_size, o->cell_size_y, o->z_factor, &kx, &ky))) return rc;
     stage_init(out, STRATA_OP_GRADIENT);
@@ -1120,8 +1263,9 @@ extern "C" int strata_stage_slope(const strata_slope_options* o, strata_stage* o
     if (!o || !out) return fail(STRATA_EINVAL, "terrain: nil options");
     int rc = fit_radius(o->fit_radius);
     if (rc) return rc;
-    float kx, ky;
-    if ((rc = horn_scales(o->cell_size, o->cell_size_y, o->z_factor, &kx, &ky))) return rc;
+    int base;
+    if ((rc = deriv_stage(STRATA_OP_SLOPE, o->fit_radius, o->cell_size, o->cell_size_y, o->z_factor, out, &base)))
+        return rc;
     // terrain.slopeScale (terrain/slope.go:84-95).
     float scale;
     int take_atan;
@@ -1131,12 +1275,8 @@ extern "C" int strata_stage_slope(const strata_slope_options* o, strata_stage* o
     case 1: scale = 100; take_atan = 0; break;
     default: return fail(STRATA_EINVAL, "terrain: unknown SlopeUnits %d", o->units);
     }
-    stage_init(out, STRATA_OP_SLOPE);
-    out->radius = 1;
     out->kind = take_atan;
-    out->k[0] = kx;
-    out->k[1] = ky;
-    out->k[2] = scale;
+    out->k[base] = scale;
     return STRATA_OK;
 }
 
@@ -1144,14 +1284,11 @@ extern "C" int strata_stage_aspect(const strata_aspect_options* o, strata_stage*
     if (!o || !out) return fail(STRATA_EINVAL, "terrain: nil options");
     int rc = fit_radius(o->fit_radius);
     if (rc) return rc;
-    float kx, ky;
-    if ((rc = horn_scales(o->cell_size, o->cell_size_y, o->z_factor, &kx, &ky))) return rc;
-    stage_init(out, STRATA_OP_ASPECT);
-    out->radius = 1;
+    int base;
+    if ((rc = deriv_stage(STRATA_OP_ASPECT, o->fit_radius, o->cell_size, o->cell_size_y, o->z_factor, out, &base)))
+        return rc;
     out->kind = o->trigonometric ? 1 : 0;
-    out->k[0] = kx;
-    out->k[1] = ky;
-    out->k[2] = o->zero_for_flat ? 0.0f : -1.0f;  // terrain.aspectFlat, AspectFlat = -1
+    out->k[base] = o->zero_for_flat ? 0.0f : -1.0f;  // terrain.aspectFlat, AspectFlat = -1
     return STRATA_OK;
 }
 
@@ -1159,8 +1296,10 @@ extern "C" int strata_stage_hillshade(const strata_hillshade_options* o, strata_
     if (!o || !out) return fail(STRATA_EINVAL, "terrain: nil options");
     int rc = fit_radius(o->fit_radius);
     if (rc) return rc;
-    float kx, ky;
-    if ((rc = horn_scales(o->cell_size, o->cell_size_y, o->z_factor, &kx, &ky))) return rc;
+    int base;
+    if ((rc = deriv_stage(STRATA_OP_HILLSHADE, o->fit_radius, o->cell_size, o->cell_size_y, o->z_factor, out,
+                          &base)))
+        return rc;
     // terrain.hillshadeLight (terrain/hillshade.go:94-117).
     double az = o->azimuth, alt = o->altitude;
     if (std::isnan(az) || std::isinf(az))
@@ -1173,13 +1312,9 @@ extern "C" int strata_stage_hillshade(const strata_hillshade_options* o, strata_
     az = std::fmod(az, 360);
     az = az * M_PI / 180;
     alt = alt * M_PI / 180;
-    stage_init(out, STRATA_OP_HILLSHADE);
-    out->radius = 1;
-    out->k[0] = kx;
-    out->k[1] = ky;
-    out->k[2] = (float)(255 * std::sin(alt));
-    out->k[3] = (float)(-255 * std::cos(alt) * std::sin(az));
-    out->k[4] = (float)(255 * std::cos(alt) * std::cos(az));
+    out->k[base] = (float)(255 * std::sin(alt));
+    out->k[base + 1] = (float)(-255 * std::cos(alt) * std::sin(az));
+    out->k[base + 2] = (float)(255 * std::cos(alt) * std::cos(az));
     return STRATA_OK;
 }
 
@@ -1187,6 +1322,13 @@ extern "C" int strata_stage_curvature(const strata_curvature_options* o, strata_
     if (!o || !out) return fail(STRATA_EINVAL, "terrain: nil options");
     int rc = fit_radius(o->fit_radius);
     if (rc) return rc;
+    if (o->fit_radius) {
+        if ((rc = fit_stage(STRATA_OP_CURVATURE, o->fit_radius, o->cell_size, o->cell_size_y, o->z_factor, out)))
+            return rc;
+        if (o->type < 0 || o->type > 2) return fail(STRATA_EINVAL, "terrain: unknown CurvatureType %d", o->type);
+        out->kind = o->type;
+        return STRATA_OK;
+    }
     double cx, cy, z;
     if ((rc = resolve_cells(o->cell_size, o->cell_size_y, o->z_factor, &cx, &cy, &z))) return rc;
     if (o->type < 0 || o->type > 2) return fail(STRATA_EINVAL, "terrain: unknown CurvatureType %d", o->type);
@@ -1309,6 +1451,58 @@ extern "C" int strata_stage_reclass(const float* breaks, int32_t nbreaks, const 
     return STRATA_OK;
 }
 
+// McCune and Keon's coefficients (terrain/heatload.go:104-108).
+static const double kHeatLoadCoef[3][6] = {
+    {-1.467, 1.582, -1.500, -0.262, 0.607, 0},
+    {-1.236, 1.350, -1.376, -0.331, 0.375, 0},
+    {0.339, 0.808, 0, -0.196, 0, -0.482},
+};
+
+extern "C" int strata_stage_heatload(strata_heatload_options* o, strata_stage* out) {
+    if (!o || !out) return fail(STRATA_EINVAL, "terrain: nil options");
+    // heatLoadTerms (terrain/heatload.go:110-142), checked first as heatLoadOp does.
+    if (o->equation < 0 || o->equation > 2)
+        return fail(STRATA_EINVAL, "terrain: unknown HeatLoadEquation %d", o->equation);
+    if (!(o->latitude >= -90 && o->latitude <= 90))
+        return fail(STRATA_EINVAL, "terrain: Latitude must be in [-90, 90], got %s", fmt_v(o->latitude).c_str());
+    const double* k = kHeatLoadCoef[o->equation];
+    const double lat = std::fabs(o->latitude) * M_PI / 180;
+    const double sin_l = std::sin(lat), cos_l = std::cos(lat);
+    const double h = std::sqrt(2.0) / 2;
+    double cos_c = h, sin_c = h;  // northeast
+    const bool south = o->latitude < 0;
+    if (o->radiation && !south) cos_c = 1, sin_c = 0;
+    else if (o->radiation && south) cos_c = -1, sin_c = 0;
+    else if (south) cos_c = -h, sin_c = h;
+    const double kc = k[2] * sin_l + k[5];
+    const double t[8] = {k[0], k[1] * cos_l, -kc * sin_c, kc * cos_c, k[3] * sin_l, k[4], cos_c, sin_c};
+    memcpy(o->terms, t, sizeof t);
+    int rc = fit_radius(o->fit_radius);
+    if (rc) return rc;
+    int base;
+    if ((rc = deriv_stage(STRATA_OP_HEATLOAD, o->fit_radius, o->cell_size, o->cell_size_y, o->z_factor, out, &base)))
+        return rc;
+    out->kind = (o->linear && o->equation != 2) ? 1 : 0;
+    out->table[0] = reinterpret_cast<const float*>(o->terms);
+    out->table_len[0] = 16;
+    return STRATA_OK;
+}
+
+extern "C" int strata_stage_orientation(const strata_orientation_options* o, strata_stage* out) {
+    if (!o || !out) return fail(STRATA_EINVAL, "terrain: nil options");
+    // orientationEast (terrain/orientation.go:45-53), checked first as orientationOp does.
+    if (o->component != 0 && o->component != 1)
+        return fail(STRATA_EINVAL, "terrain: unknown OrientationComponent %d", o->component);
+    int rc = fit_radius(o->fit_radius);
+    if (rc) return rc;
+    int base;
+    if ((rc = deriv_stage(STRATA_OP_ORIENTATION, o->fit_radius, o->cell_size, o->cell_size_y, o->z_factor, out,
+                          &base)))
+        return rc;
+    out->kind = (o->component ? 1 : 0) | (o->unweighted ? 2 : 0);
+    return STRATA_OK;
+}
+
 extern "C" int strata_focal_gaussian(int32_t radius, double sigma, float* taps) {
     int rc = check_focal_radius(radius);
     if (rc) return rc;
@@ -1394,6 +1588,7 @@ extern "C" int strata_process_chunked(strata_ctx* c, const strata_stage* stages,
     int nout = 0;
     int rc = plan_stages(stages, nstages, p, &nout);
     if (rc) return rc;
+    if (p.fit) return fail(STRATA_ENOTSUP, "engine: Wood's fit (FitRadius > 0) has no chunked form on the gpu backend");
     if ((rc = check_opts(opts))) return rc;
     if (nsrc != 1 || ndst != nout || !src || !dst)
         return fail(STRATA_EINVAL, "engine: kernel takes 1 inputs and %d outputs, got %d and %d", nout, nsrc, ndst);
@@ -1814,9 +2009,10 @@ extern "C" int strata_process_features(strata_ctx* c, const strata_stage* stages
                           0, H);
             vs[i - o] = &vp[i - o];
         }
-        int64_t t = strata::launch_stage(p, vs, st, &wc);
+        int64_t t = p.fit ? launch_fit(c, p, vs, st, &wc) : strata::launch_stage(p, vs, st, &wc);
         if (t < 0) {
             cleanup();
+            if (t == -2) return fail(STRATA_ENOMEM, "engine: no device memory for the fit's sums");
             return fail(STRATA_ENOTSUP, "engine: op %d at radius %d has no device kernel", p.op, p.radius);
         }
         bands += t;
@@ -1872,6 +2068,8 @@ int fill_batch_item(strata_ctx* c, const strata_batch_item& it, int i, strata::B
         return fail(STRATA_EINVAL, "engine: batch raster %d: the rasters of a batch must be on the device", i);
     if (p.op == STRATA_OP_LOOKUP || p.op == STRATA_OP_RECLASS)
         return fail(STRATA_ENOTSUP, "engine: batch raster %d: a pointwise op alone has no batch kernel", i);
+    if (p.fit || p.op == STRATA_OP_HEATLOAD || p.op == STRATA_OP_ORIENTATION)
+        return fail(STRATA_ENOTSUP, "engine: batch raster %d: op %d has no batch kernel", i, p.op);
     if (it.tile_height < 0 || it.tile_height > 1024)
         return fail(STRATA_EINVAL, "engine: batch raster %d: band of %d rows (0 to 1024)", i, it.tile_height);
     DevOperand ds, dd[2];
@@ -2475,6 +2673,8 @@ Request* prepare_request(strata_server* S, const strata_stage* stages, int nstag
     int rc = plan_stages(r->stages.data(), (int)r->stages.size(), r->p, &r->nout);
     if (rc == STRATA_OK && (r->p.op == STRATA_OP_LOOKUP || r->p.op == STRATA_OP_RECLASS))
         rc = fail(STRATA_ENOTSUP, "engine: a pointwise op alone has no batch kernel");
+    if (rc == STRATA_OK && (r->p.fit || r->p.op == STRATA_OP_HEATLOAD || r->p.op == STRATA_OP_ORIENTATION))
+        rc = fail(STRATA_ENOTSUP, "engine: op %d has no batch kernel", r->p.op);
     if (rc) {
         delete r;
         *rc_out = rc;

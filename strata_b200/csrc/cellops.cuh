@@ -139,6 +139,8 @@ __device__ __forceinline__ float shade(float gx, float gy, float c, float bx, fl
     return v;
 }
 
+__device__ __forceinline__ float zt_finish(float P, float Q, float R, float S, float T, int kind);
+
 // Zevenbergen-Thorne curvature (internal/stencil/curvature.go:79-129):
 // ztDerivs, then the profile (0), plan (1) or mean (2) formula.
 __device__ __forceinline__ float zt_curvature(float z1, float z2, float z3, float z4, float z5, float z6,
@@ -149,6 +151,13 @@ __device__ __forceinline__ float zt_curvature(float z1, float z2, float z3, floa
     float R = mul(sub(add(z4, z6), c), k[2]);
     float T = mul(sub(add(z2, z8), c), k[3]);
     float S = mul(sub(add(z1, z9), add(z3, z7)), k[4]);
+    return zt_finish(P, Q, R, S, T, kind);
+}
+
+// CurvatureFromDerivsRow (internal/stencil/curvature.go:138-185): ZT's
+// formulas from the derivatives p, q, r, s, t, however estimated (ZT's
+// 3x3 window above, or Wood's fit).
+__device__ __forceinline__ float zt_finish(float P, float Q, float R, float S, float T, int kind) {
     float p2 = mul(P, P), q2 = mul(Q, Q);
     float pq = mul(P, Q);
     float pq2 = add(pq, pq);
@@ -343,6 +352,45 @@ __device__ __forceinline__ F2 zt_curvature2(F2 d64, F2 d82, F2 c, F2 s46, F2 s28
         v[1] = hi(r);
     }
     return pk(v[0], v[1]);
+}
+
+// heatLoad (internal/stencil/heatload.go:43-53): McCune and Keon's
+// regression from the gradient, in float64 with every product rounded
+// before it is added, rounded to float32 once. t: K0, A, BX, BY, E, F, CX,
+// CY; with ex, exp of the sum (CUDA's exp, within one float64 ulp of
+// Go's math.Exp: the float32 result differs only when the sum sits within
+// that of a float32 rounding boundary).
+__device__ __forceinline__ float heat_load(float gx, float gy, const double* t, bool ex) {
+    const double dx = gx, dy = gy;
+    const double g2 = __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
+    const double w = __ddiv_rn(1.0, __dsqrt_rn(__dadd_rn(1.0, g2)));
+    const double fold = fabs(__dadd_rn(__dmul_rn(t[6], dx), __dmul_rn(t[7], dy)));
+    double sum = __dadd_rn(t[1], __dmul_rn(t[2], dx));
+    sum = __dadd_rn(sum, __dmul_rn(t[3], dy));
+    sum = __dadd_rn(sum, __dmul_rn(t[4], __dsqrt_rn(g2)));
+    sum = __dadd_rn(sum, __dmul_rn(t[5], fold));
+    double v = __dadd_rn(t[0], __dmul_rn(w, sum));
+    if (ex) v = exp(v);
+    return __double2float_rn(v);
+}
+
+// orientation (internal/stencil/orientation.go:31-45): northness (gy) or
+// eastness (-gx) over sqrt(1 + g2), or over sqrt(g2) unweighted with 0
+// where flat, in float64, rounded to float32 once.
+__device__ __forceinline__ float orientation(float gx, float gy, bool east, bool unweighted) {
+    const double dx = gx, dy = gy;
+    const double c = east ? -dx : dy;
+    const double g2 = __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
+    if (!unweighted) return __double2float_rn(__ddiv_rn(c, __dsqrt_rn(__dadd_rn(1.0, g2))));
+    if (g2 == 0) return 0.0f;
+    return __double2float_rn(__ddiv_rn(c, __dsqrt_rn(g2)));
+}
+
+// The eight float64 terms of a heat-load launch, stored bit for bit in
+// 16 float slots (low word first).
+__device__ __forceinline__ void heat_terms(const float* w, double* t) {
+#pragma unroll
+    for (int i = 0; i < 8; i++) t[i] = __hiloint2double(__float_as_int(w[2 * i + 1]), __float_as_int(w[2 * i]));
 }
 
 __device__ __forceinline__ double sq64(float d) {

@@ -30,8 +30,65 @@ __global__ void __launch_bounds__(256) pointwise_kernel(const __grid_constant__ 
     }
 }
 
+// The finishing pass of Wood's fit (terrain/fit.go:121-170): the raw fit
+// sums d0..d4 (p, q, and for curvature r, s, t) at each cell, each scaled
+// by its factor (scaleRow), through the product's finisher: the gradient
+// itself, the from-gradient finishers Surface uses (SlopeFromGradientRow
+// and the rest, the same device functions as Horn's), HeatLoad and
+// Orientation's equations, or ZT's curvature formulas. Cells within the
+// fit's radius of the border get NaN; the epilogue maps NaN to itself.
+__global__ void __launch_bounds__(256) fit_finish_kernel(const __grid_constant__ LaunchParams P,
+                                                         const float* __restrict__ d0, const float* __restrict__ d1,
+                                                         const float* __restrict__ d2, const float* __restrict__ d3,
+                                                         const float* __restrict__ d4, int64_t ds) {
+    const int64_t w = P.out_x1 - P.out_x0;
+    const int64_t n = w * (P.out_y1 - P.out_y0);
+    const int r = P.radius;
+    const float nan = nanf32();
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t y = i / w, x = i - y * w;
+        const int64_t gx = P.out_x0 + x, gy = P.out_y0 + y;
+        const int64_t o = (gy - P.dst_y0) * ds + (gx - P.dst_x0);
+        float v0 = nan, v1 = nan;
+        if (gy >= r && gy < P.height - r && gx >= r && gx < P.width - r) {
+            const float p = mul(d0[o], P.k[0]), q = mul(d1[o], P.k[1]);
+            switch (P.op) {
+            case STRATA_OP_GRADIENT:
+                v0 = p;
+                v1 = q;
+                break;
+            case STRATA_OP_SLOPE:
+                v0 = P.kind == kSlopeSquareClass ? add(mul(p, p), mul(q, q)) : slope(p, q, P.k[5], P.kind != 0);
+                break;
+            case STRATA_OP_ASPECT: v0 = aspect(p, q, P.k[5], P.kind != 0); break;
+            case STRATA_OP_HILLSHADE: v0 = shade(p, q, P.k[5], P.k[6], P.k[7]); break;
+            case STRATA_OP_HEATLOAD: {
+                double t[8];
+                heat_terms(P.w, t);
+                v0 = heat_load(p, q, t, P.kind & 1);
+                break;
+            }
+            case STRATA_OP_ORIENTATION: v0 = orientation(p, q, P.kind & 1, (P.kind >> 1) & 1); break;
+            default:  // curvature: r, s and t scaled by kr, ks and kt
+                v0 = zt_finish(p, q, mul(d2[o], P.k[2]), mul(d3[o], P.k[4]), mul(d4[o], P.k[3]), P.kind);
+                break;
+            }
+        }
+        if (P.nepi) v0 = epilogue(P, v0);
+        P.dst0[(gy - P.dst_y0) * P.dst0_stride + (gx - P.dst_x0)] = v0;
+        if (P.op == STRATA_OP_GRADIENT) P.dst1[(gy - P.dst_y0) * P.dst1_stride + (gx - P.dst_x0)] = v1;
+    }
+}
+
 }  // namespace
 
+void launch_fit_finish(const LaunchParams& p, float* const d[5], int64_t ds, cudaStream_t s) {
+    const int64_t n = (p.out_x1 - p.out_x0) * (p.out_y1 - p.out_y0);
+    if (n <= 0) return;
+    int64_t blocks = (n + 255) / 256;
+    if (blocks > (int64_t)sm_count() * 16) blocks = (int64_t)sm_count() * 16;
+    fit_finish_kernel<<<(unsigned)blocks, 256, 0, s>>>(p, d[0], d[1], d[2], d[3], d[4], ds);
+}
 
 int64_t launch_data(const LaunchParams& p, cudaStream_t s, int64_t* window_cells) {
     if (p.op == STRATA_OP_LOOKUP || p.op == STRATA_OP_RECLASS) {
@@ -43,7 +100,9 @@ int64_t launch_data(const LaunchParams& p, cudaStream_t s, int64_t* window_cells
         if (window_cells) *window_cells = n;
         return blocks;
     }
-    if (p.op < STRATA_OP_GRADIENT || p.op > STRATA_OP_MAX) return -1;
+    if (p.fit || (!(p.op >= STRATA_OP_GRADIENT && p.op <= STRATA_OP_MAX) && p.op != STRATA_OP_HEATLOAD &&
+                  p.op != STRATA_OP_ORIENTATION))
+        return -1;
     if (p.out_x1 <= p.out_x0 || p.out_y1 <= p.out_y0) {
         if (window_cells) *window_cells = 0;
         return 0;

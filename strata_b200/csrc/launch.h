@@ -90,9 +90,10 @@ struct alignas(16) LaunchParams {
     // STRATA_TEST_STALL_FIRST_WAIT=1): the TMA march's first wait is on a
     // barrier nothing arrives at, with a short bound, so it runs out.
     int test_stall;
-    int pad_;
+    int fit;  // the radius of Wood's fit when the derivatives come from it (a STRATA_STAGE_FIT stage), else 0
     float k[16];
-    float w[kMaxWeights];  // CORRELATE weights (rotation applied); SEPARABLE row taps w[0..], column taps w[17..]
+    float w[kMaxWeights];  // CORRELATE weights (rotation applied); SEPARABLE row taps w[0..], column taps w[17..];
+                           // HEATLOAD the regression's eight float64 terms, bit for bit, in w[0..16)
     EpiStage epi[kMaxEpilogue];
     FusedValidity vf;  // set by launch_stage when the march writes the outputs' validity
 };
@@ -214,6 +215,13 @@ void launch_batch_validity(const ValidityClass& c, const ValidityItem* d_vitems,
 // launched, or -1 if the op / radius has no kernel; *window_cells gets the
 // input cells the tiles read (halo included, clipped to the raster).
 int64_t launch_data(const LaunchParams& p, cudaStream_t stream, int64_t* window_cells);
+
+// The finishing pass of a Wood's-fit stage (kernels.cu): p's product
+// (p.op, p.kind, p.k[5..], p.w for heat load) from the raw fit sums d[0..1]
+// (p, q) and, for curvature, d[2..4] (r, s, t) over the region (rasters
+// with dst0's geometry and stride ds), each scaled by its factor p.k[0..4],
+// then p's pointwise epilogue; cells within p.radius of the border get NaN.
+void launch_fit_finish(const LaunchParams& p, float* const d[5], int64_t ds, cudaStream_t stream);
 
 // Launches the validity kernel for one output.
 void launch_validity(const ValidityParams& v, cudaStream_t stream);

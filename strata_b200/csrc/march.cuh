@@ -40,7 +40,7 @@ struct EpiSmem<false> {
 
 template <int OP>
 constexpr bool kIsHorn = OP == STRATA_OP_GRADIENT || OP == STRATA_OP_SLOPE || OP == STRATA_OP_ASPECT ||
-                         OP == STRATA_OP_HILLSHADE;
+                         OP == STRATA_OP_HILLSHADE || OP == STRATA_OP_HEATLOAD || OP == STRATA_OP_ORIENTATION;
 
 // One output row of four cells from the window rows a (top), b, c
 // (bottom) and, for Horn ops, their horizontal differences.
@@ -91,7 +91,16 @@ __device__ __forceinline__ void row_compute(const LaunchParams& P, const EpiTabl
                 r = add_p(mul2(gx[p], gx[p]), mul2(gy[p], gy[p]));  // magnitude's radicand (horn.go:220-222)
             else if constexpr (OP == STRATA_OP_SLOPE) r = slope2(gx[p], gy[p], splat(P.k[2]), KIND != 0);
             else if constexpr (OP == STRATA_OP_ASPECT) r = aspect2(gx[p], gy[p], P.k[2], KIND != 0);
-            else r = shade2(gx[p], gy[p], P.k[2], P.k[3], P.k[4]);
+            else if constexpr (OP == STRATA_OP_HEATLOAD) {
+                // heatLoadKernel (terrain/heatload.go:147-160): Horn's gradient, then the equation
+                double t[8];
+                heat_terms(P.w, t);
+                r = pk(heat_load(lo(gx[p]), lo(gy[p]), t, P.kind & 1), heat_load(hi(gx[p]), hi(gy[p]), t, P.kind & 1));
+            } else if constexpr (OP == STRATA_OP_ORIENTATION) {
+                // orientationKernel (terrain/orientation.go:83-95)
+                const bool east = P.kind & 1, unw = (P.kind >> 1) & 1;
+                r = pk(orientation(lo(gx[p]), lo(gy[p]), east, unw), orientation(hi(gx[p]), hi(gy[p]), east, unw));
+            } else r = shade2(gx[p], gy[p], P.k[2], P.k[3], P.k[4]);
             o0[2 * p] = rowin && colin[2 * p] ? lo(r) : nan;
             o0[2 * p + 1] = rowin && colin[2 * p + 1] ? hi(r) : nan;
         }

@@ -366,6 +366,7 @@ int64_t launch_any_epi(const LaunchParams& p, cudaStream_t s) {
 }  // namespace
 
 bool march3_eligible(const LaunchParams& p) {
+    if (p.fit) return false;  // Wood's fit runs as separable folds and a finishing pass
     if (p.radius != 1 && !(p.op >= STRATA_OP_GRADIENT && p.op <= STRATA_OP_CURVATURE)) return false;
     const int64_t w = p.out_x1 - p.out_x0;
     if (w <= 0 || (w & 3) || (p.src_stride & 3) || (p.dst0_stride & 3)) return false;
@@ -379,7 +380,10 @@ bool march3_eligible(const LaunchParams& p) {
 }
 
 bool march_any_eligible(const LaunchParams& p) {
-    if (p.radius > 1 || p.op < STRATA_OP_GRADIENT || p.op > STRATA_OP_MAX) return false;
+    if (p.fit) return false;
+    const bool op_ok = (p.op >= STRATA_OP_GRADIENT && p.op <= STRATA_OP_MAX) || p.op == STRATA_OP_HEATLOAD ||
+                       p.op == STRATA_OP_ORIENTATION;
+    if (p.radius > 1 || !op_ok) return false;
     const int64_t w = p.out_x1 - p.out_x0;
     if (w <= 0) return false;
     // 32-bit block, row and column arithmetic inside the kernel.
@@ -398,6 +402,8 @@ int64_t launch_march_any(const LaunchParams& p, cudaStream_t s) {
     case STRATA_OP_ASPECT:
         return p.kind ? launch_any_epi<STRATA_OP_ASPECT, 1>(p, s) : launch_any_epi<STRATA_OP_ASPECT, 0>(p, s);
     case STRATA_OP_HILLSHADE: return launch_any_epi<STRATA_OP_HILLSHADE, 0>(p, s);
+    case STRATA_OP_HEATLOAD: return launch_any_epi<STRATA_OP_HEATLOAD, 0>(p, s);
+    case STRATA_OP_ORIENTATION: return launch_any_epi<STRATA_OP_ORIENTATION, 0>(p, s);
     case STRATA_OP_CURVATURE:
         switch (p.kind) {
         case 0: return launch_any_epi<STRATA_OP_CURVATURE, 0>(p, s);
@@ -431,6 +437,8 @@ int64_t launch_march3(const LaunchParams& p, cudaStream_t s) {
     case STRATA_OP_ASPECT:
         return p.kind ? launch_epi<STRATA_OP_ASPECT, 1>(p, s) : launch_epi<STRATA_OP_ASPECT, 0>(p, s);
     case STRATA_OP_HILLSHADE: return launch_epi<STRATA_OP_HILLSHADE, 0>(p, s);
+    case STRATA_OP_HEATLOAD: return launch_epi<STRATA_OP_HEATLOAD, 0>(p, s);
+    case STRATA_OP_ORIENTATION: return launch_epi<STRATA_OP_ORIENTATION, 0>(p, s);
     case STRATA_OP_CURVATURE:
         switch (p.kind) {
         case 0: return launch_epi<STRATA_OP_CURVATURE, 0>(p, s);

@@ -70,6 +70,33 @@ class CurvatureOptions:
     Type: int = CurvatureProfile
 
 
+# terrain.HeatLoadEquation and terrain.OrientationComponent.
+HeatLoadEquation1, HeatLoadEquation2, HeatLoadEquation3 = 0, 1, 2
+Northness, Eastness = 0, 1
+
+
+@dataclass
+class HeatLoadOptions:
+    CellSize: float = 0.0
+    CellSizeY: float = 0.0
+    ZFactor: float = 0.0
+    FitRadius: int = 0
+    Latitude: float = 0.0
+    Equation: int = HeatLoadEquation1
+    Radiation: bool = False
+    Linear: bool = False
+
+
+@dataclass
+class OrientationOptions:
+    CellSize: float = 0.0
+    CellSizeY: float = 0.0
+    ZFactor: float = 0.0
+    FitRadius: int = 0
+    Component: int = Northness
+    Unweighted: bool = False
+
+
 @dataclass
 class RuggednessOptions:
     Type: int = RuggednessTRI
@@ -108,6 +135,23 @@ def curvature_stage(o: CurvatureOptions) -> StageList:
                 _lib.CurvatureOptions(o.CellSize, o.CellSizeY, o.ZFactor, o.FitRadius, o.Type))
 
 
+def heatload_stage(o: HeatLoadOptions) -> StageList:
+    """terrain.heatLoadOp (terrain/heatload.go:144-151). The stage points at
+    the regression's terms the builder writes into its options, which the
+    StageList keeps."""
+    copts = _lib.HeatLoadOptions(o.CellSize, o.CellSizeY, o.ZFactor, o.FitRadius, o.Equation, o.Latitude,
+                                 int(bool(o.Radiation)), int(bool(o.Linear)))
+    st = _lib.Stage()
+    _lib.check(_lib.lib().strata_stage_heatload(ctypes.byref(copts), ctypes.byref(st)))
+    return StageList().add(st, copts)
+
+
+def orientation_stage(o: OrientationOptions) -> StageList:
+    return _one(_lib.lib().strata_stage_orientation,
+                _lib.OrientationOptions(o.CellSize, o.CellSizeY, o.ZFactor, o.FitRadius, o.Component,
+                                        int(bool(o.Unweighted)), 0))
+
+
 def ruggedness_stage(o: RuggednessOptions) -> StageList:
     return _one(_lib.lib().strata_stage_ruggedness, _lib.RuggednessOptions(o.Type, o.Radius))
 
@@ -119,7 +163,8 @@ def _plain(stages, dem, *outs):
 # Features (terrain/features.go): several ops over one DEM in one call.
 @dataclass
 class Feature:
-    Op: object  # SlopeOptions, AspectOptions, HillshadeOptions, CurvatureOptions or RuggednessOptions
+    Op: object  # SlopeOptions, AspectOptions, HillshadeOptions, HeatLoadOptions, OrientationOptions,
+    # CurvatureOptions or RuggednessOptions
     Dst: Float32Raster
 
 
@@ -127,6 +172,8 @@ _FEATURE_STAGES = {
     SlopeOptions: slope_stage,
     AspectOptions: aspect_stage,
     HillshadeOptions: hillshade_stage,
+    HeatLoadOptions: heatload_stage,
+    OrientationOptions: orientation_stage,
     CurvatureOptions: curvature_stage,
     RuggednessOptions: ruggedness_stage,
 }
@@ -287,3 +334,27 @@ def RuggednessTiled(ctx: Context, dst, dem, opts: RuggednessOptions, eopts: Opti
 
 def RuggednessChunked(ctx: Context, dst, dem, opts: RuggednessOptions, eopts: Options):
     return process_chunked(ruggedness_stage(opts), [dst], [dem], eopts, ctx)
+
+
+def HeatLoad(dst: Float32Raster, dem: Float32Raster, opts: HeatLoadOptions) -> None:
+    _plain(heatload_stage(opts), dem, dst)
+
+
+def HeatLoadTiled(ctx: Context, dst, dem, opts: HeatLoadOptions, eopts: Options):
+    return process(heatload_stage(opts), [dst], [dem], eopts, ctx)
+
+
+def HeatLoadChunked(ctx: Context, dst, dem, opts: HeatLoadOptions, eopts: Options):
+    return process_chunked(heatload_stage(opts), [dst], [dem], eopts, ctx)
+
+
+def Orientation(dst: Float32Raster, dem: Float32Raster, opts: OrientationOptions) -> None:
+    _plain(orientation_stage(opts), dem, dst)
+
+
+def OrientationTiled(ctx: Context, dst, dem, opts: OrientationOptions, eopts: Options):
+    return process(orientation_stage(opts), [dst], [dem], eopts, ctx)
+
+
+def OrientationChunked(ctx: Context, dst, dem, opts: OrientationOptions, eopts: Options):
+    return process_chunked(orientation_stage(opts), [dst], [dem], eopts, ctx)

@@ -79,7 +79,7 @@ def oracle_stage(st: _lib.Stage):
         tables.pop()
     if st.op == _lib.OP_CORRELATE and st.flags & _lib.STAGE_ROTATE180:
         tables[0] = tables[0][::-1].copy()
-    return orc.stage(st.op, st.radius, st.kind, list(st.k), tables)
+    return orc.stage(st.op, st.radius, st.kind, list(st.k), tables, flags=st.flags & _lib.STAGE_FIT)
 
 
 def run_oracle(stages, src: Float32Raster, dsts, nthreads=1):

@@ -61,7 +61,8 @@ def test_struct_layouts_match_header(tmp_path):
         "strata_hillshade_options": _lib.HillshadeOptions, "strata_curvature_options": _lib.CurvatureOptions,
         "strata_gradient_options": _lib.GradientOptions, "strata_ruggedness_options": _lib.RuggednessOptions,
         "strata_weights_options": _lib.WeightsOptions, "strata_separable_options": _lib.SeparableOptions,
-        "strata_box_options": _lib.BoxOptions,
+        "strata_box_options": _lib.BoxOptions, "strata_heatload_options": _lib.HeatLoadOptions,
+        "strata_orientation_options": _lib.OrientationOptions,
     }
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void){"]
     for cname, ct in structs.items():
@@ -180,9 +181,58 @@ def test_builders_panic_like_the_reference(make, msg):
     assert str(e.value).startswith(msg), str(e.value)
 
 
-def test_fit_radius_is_not_on_the_device():
-    with pytest.raises(NotSupported):
-        terrain.slope_stage(terrain.SlopeOptions(CellSize=1, FitRadius=2))
+def _k(stages, n):
+    return [np.float32(stages.stages[0].k[i]) for i in range(n)]
+
+
+@pytest.mark.parametrize("r", [1, 2, 5, 8])
+def test_fit_stages_resolve_as_the_oracle(r):
+    """FitRadius 1..8 builds Wood's fit (terrain/fit.go:38-66): the factors
+    the oracle derives, the fit flag and radius, the product's constants
+    after them."""
+    from oracle import oracle as orc
+
+    want = orc.fit_scales(r, 3.0, 5.0, 2.0)
+    g = terrain.gradient_stage(terrain.GradientOptions(CellSize=3, CellSizeY=5, ZFactor=2, FitRadius=r))
+    st = g.stages[0]
+    assert st.flags == _lib.STAGE_FIT and st.radius == r and _k(g, 5) == want
+    sl = terrain.slope_stage(terrain.SlopeOptions(CellSize=3, CellSizeY=5, ZFactor=2, FitRadius=r))
+    assert _k(sl, 6) == want + [np.float32(180 / np.pi)] and sl.stages[0].kind == 1
+    hs = terrain.hillshade_stage(terrain.HillshadeOptions(CellSize=3, CellSizeY=5, ZFactor=2, FitRadius=r))
+    assert _k(hs, 8)[5:] == [np.float32(v) for v in orc.hillshade_light(315, 45)]
+    cv = terrain.curvature_stage(terrain.CurvatureOptions(CellSize=3, CellSizeY=5, ZFactor=2, FitRadius=r, Type=2))
+    assert cv.stages[0].kind == 2 and _k(cv, 5) == want
+    with pytest.raises(StrataPanic, match="FitRadius must be 0 to 8, got 9"):
+        terrain.slope_stage(terrain.SlopeOptions(CellSize=1, FitRadius=9))
+
+
+@pytest.mark.parametrize("lat,eq,rad,lin", [(40.0, 0, False, False), (-33.5, 1, True, True), (60.0, 2, False, True),
+                                            (0.0, 0, True, False)])
+def test_heatload_stage_terms_as_the_oracle(lat, eq, rad, lin):
+    """heatLoadTerms (terrain/heatload.go:110-142): the eight float64 terms
+    the stage carries are the oracle's, and Linear takes exp but for
+    Equation 3."""
+    from oracle import oracle as orc
+
+    st = terrain.heatload_stage(terrain.HeatLoadOptions(CellSize=10, Latitude=lat, Equation=eq, Radiation=rad,
+                                                        Linear=lin))
+    s0 = st.stages[0]
+    assert s0.op == _lib.OP_HEATLOAD and s0.table_len[0] == 16
+    got = np.ctypeslib.as_array((ctypes.c_double * 8).from_address(s0.table[0]))
+    want, ex = orc.heatload_terms(lat, eq, rad, lin)
+    assert np.array_equal(got, want) and s0.kind == int(ex)
+    with pytest.raises(StrataPanic, match=r"Latitude must be in \[-90, 90\], got 91"):
+        terrain.heatload_stage(terrain.HeatLoadOptions(CellSize=1, Latitude=91))
+    with pytest.raises(StrataPanic, match="unknown HeatLoadEquation 3"):
+        terrain.heatload_stage(terrain.HeatLoadOptions(CellSize=1, Equation=3))
+
+
+def test_orientation_stage_kind():
+    st = terrain.orientation_stage(terrain.OrientationOptions(CellSize=2, Component=terrain.Eastness,
+                                                              Unweighted=True))
+    assert st.stages[0].op == _lib.OP_ORIENTATION and st.stages[0].kind == 3
+    with pytest.raises(StrataPanic, match="unknown OrientationComponent 2"):
+        terrain.orientation_stage(terrain.OrientationOptions(CellSize=1, Component=2))
 
 
 def test_context_without_a_device_fails_cleanly():

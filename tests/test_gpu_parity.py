@@ -678,3 +678,104 @@ def test_chunked_source_error_is_returned():
     from helpers import same_bits
 
     assert same_bits(got.numpy()[:16], want.numpy()[:16]).all()
+
+
+# ---------------------------------------------------------------------------
+# HeatLoad and Orientation (Horn's gradient) and Wood's quadratic fit
+# (FitRadius 1..8) for every product.
+
+HEAT_ORIENT = {
+    "heat_eq1": lambda: terrain.heatload_stage(terrain.HeatLoadOptions(CellSize=10, Latitude=40)),
+    "heat_eq2_rad_south": lambda: terrain.heatload_stage(terrain.HeatLoadOptions(CellSize=5, CellSizeY=7,
+                                                                                  Latitude=-35, Equation=1,
+                                                                                  Radiation=True)),
+    "heat_eq3": lambda: terrain.heatload_stage(terrain.HeatLoadOptions(CellSize=30, Latitude=52.5, Equation=2)),
+    "north": lambda: terrain.orientation_stage(terrain.OrientationOptions(CellSize=10)),
+    "east_unweighted": lambda: terrain.orientation_stage(terrain.OrientationOptions(CellSize=3, ZFactor=2,
+                                                                                    Component=terrain.Eastness,
+                                                                                    Unweighted=True)),
+}
+
+
+@pytest.mark.parametrize("name", sorted(HEAT_ORIENT))
+def test_heatload_orientation(name):
+    run_matrix(HEAT_ORIENT[name], dem_cells, shapes=SHAPES[:9])
+
+
+def test_heatload_linear_within_one_ulp():
+    """With Linear, Equations 1 and 2 take exp of the regression: CUDA's exp
+    and the C library's (and Go's math.Exp) agree to a float64 ulp, so the
+    float32 result may move by one ulp where the sum sits at a rounding
+    boundary; every other cell and every validity bit is exact."""
+    w, h = 257, 131
+    cells = dem_cells(w, h, 77)
+    src = host_raster(cells, synth.cell_mask(w, h, 77, 0.03))
+    st = lambda: terrain.heatload_stage(terrain.HeatLoadOptions(CellSize=10, Latitude=44, Linear=True))
+    want, got = like(src), like(src)
+    run_oracle(st(), src, [want])
+    assert engine.process(st(), [got], [src]) is None
+    g, wv = got.numpy(), want.numpy()
+    both_nan = np.isnan(g) & np.isnan(wv)
+    ulps = np.abs(g.view(np.int32).astype(np.int64) - wv.view(np.int32).astype(np.int64))
+    assert (both_nan | (ulps <= 1)).all()
+    assert (got.valid_numpy() == want.valid_numpy()).all()
+
+
+FIT_PRODUCTS = {
+    "gradient": (lambda r: terrain.gradient_stage(terrain.GradientOptions(CellSize=10, CellSizeY=12, FitRadius=r)), 2),
+    "slope_deg": (lambda r: terrain.slope_stage(terrain.SlopeOptions(CellSize=10, FitRadius=r)), 1),
+    "slope_pct": (lambda r: terrain.slope_stage(terrain.SlopeOptions(CellSize=10, Units=terrain.SlopePercent,
+                                                                     FitRadius=r)), 1),
+    "aspect": (lambda r: terrain.aspect_stage(terrain.AspectOptions(CellSize=10, Trigonometric=True, FitRadius=r)), 1),
+    "hillshade": (lambda r: terrain.hillshade_stage(terrain.HillshadeOptions(CellSize=10, Azimuth=120, FitRadius=r)),
+                  1),
+    "heatload": (lambda r: terrain.heatload_stage(terrain.HeatLoadOptions(CellSize=10, Latitude=47, Equation=2,
+                                                                          FitRadius=r)), 1),
+    "orientation": (lambda r: terrain.orientation_stage(terrain.OrientationOptions(CellSize=10, FitRadius=r)), 1),
+    "curv_profile": (lambda r: terrain.curvature_stage(terrain.CurvatureOptions(CellSize=10, Type=0, FitRadius=r)), 1),
+    "curv_plan": (lambda r: terrain.curvature_stage(terrain.CurvatureOptions(CellSize=10, Type=1, FitRadius=r)), 1),
+    "curv_mean": (lambda r: terrain.curvature_stage(terrain.CurvatureOptions(CellSize=4, CellSizeY=6, ZFactor=2,
+                                                                             Type=2, FitRadius=r)), 1),
+    "slope_classes": (lambda r: terrain.slope_stage(terrain.SlopeOptions(CellSize=10, FitRadius=r)).extend(
+        transfer.lookup_stage(SLOPE_XS, SLOPE_YS)).extend(transfer.reclass_stage(BREAKS, VALUES)), 1),
+}
+
+
+@pytest.mark.parametrize("name", sorted(FIT_PRODUCTS))
+@pytest.mark.parametrize("r", [1, 2, 5, 8])
+def test_wood_fit_products(name, r):
+    """Wood's fit (terrain/fit.go) on the device (raw sums as separable
+    correlations, then the finishing pass) against the oracle's fit, cell
+    for cell and bit for bit, over small and odd shapes and layouts."""
+    make, nout = FIT_PRODUCTS[name]
+    run_matrix(lambda: make(r), dem_cells, nout=nout, shapes=SMALL_SHAPES, seed=r)
+
+
+def test_fit_surface_and_features_equal_standalone():
+    """TestFitSurfaceIsTheStandaloneProducts (terrain/fit_test.go:134-204):
+    a Features call with FitRadius set writes what each product alone does."""
+    w, h = 96, 40
+    src = host_raster(dem_cells(w, h, 21), synth.block_mask(w, h, 21, 0.05))
+    ops = [terrain.SlopeOptions(CellSize=10, FitRadius=3), terrain.AspectOptions(CellSize=10, FitRadius=3),
+           terrain.HeatLoadOptions(CellSize=10, Latitude=30, FitRadius=2),
+           terrain.OrientationOptions(CellSize=10, Component=terrain.Eastness),
+           terrain.CurvatureOptions(CellSize=10, Type=2, FitRadius=4)]
+    singles = {terrain.SlopeOptions: terrain.Slope, terrain.AspectOptions: terrain.Aspect,
+               terrain.HeatLoadOptions: terrain.HeatLoad, terrain.OrientationOptions: terrain.Orientation,
+               terrain.CurvatureOptions: terrain.Curvature}
+    outs = [like(src) for _ in ops]
+    terrain.Features([terrain.Feature(op, d) for op, d in zip(ops, outs)], src)
+    for op, got in zip(ops, outs):
+        want = like(src)
+        singles[type(op)](want, src, op)
+        assert_same_raster(got, want, f"features {type(op).__name__}")
+
+
+def test_fit_has_no_chunked_or_batch_form():
+    from strata_b200.raster import NotSupported
+
+    w, h = 40, 30
+    src = host_raster(dem_cells(w, h, 5))
+    with pytest.raises(NotSupported):
+        engine.process_chunked(terrain.slope_stage(terrain.SlopeOptions(CellSize=1, FitRadius=2)),
+                               [engine.MemorySink(like(src))], [engine.MemorySource(src)], engine.Options())
