@@ -923,7 +923,8 @@ def _orc_of(st):
                       if st.table[i] and n > 0 else np.zeros(0, np.float32))
     while tables and tables[-1].size == 0:
         tables.pop()
-    return _orc().stage(st.op, st.radius, st.kind, list(st.k), tables, flags=st.flags & _lib.STAGE_FIT)
+    return _orc().stage(st.op, st.radius, st.kind, list(st.k), tables, flags=st.flags & _lib.STAGE_FIT,
+                        input=st.input)
 
 
 def _summary(line, keys):

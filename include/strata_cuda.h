@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define STRATA_ABI_VERSION 1
+#define STRATA_ABI_VERSION 2
 
 /* Status codes. */
 #define STRATA_OK 0
@@ -62,8 +62,40 @@ enum {
     STRATA_OP_LOOKUP = 12,    /* transfer.Lookup, pointwise */
     STRATA_OP_RECLASS = 13,   /* transfer.Reclass, pointwise */
     STRATA_OP_HEATLOAD = 14,  /* terrain.HeatLoad (McCune and Keon), radius 1 */
-    STRATA_OP_ORIENTATION = 15 /* terrain.Orientation (northness / eastness), radius 1 */
+    STRATA_OP_ORIENTATION = 15, /* terrain.Orientation (northness / eastness), radius 1 */
+    STRATA_OP_STEP = 16         /* one step of a vec.Chain (Rescale, Clamp, Normalize, algebra), pointwise */
 };
+
+/*
+ * strata_stage.kind for STRATA_OP_STEP: vec.Op (internal/vec/chain.go:
+ * 24-38). The running value acc is the step's first operand; the binary
+ * ops (ADD .. MAX) take the pipeline input named by strata_stage.input as
+ * the second, the others the immediates k[0] and k[1]:
+ *   ADD SUB MUL DIV: acc op src; MIN MAX: Go's min / max (NaN wins, -0 < +0)
+ *   ADD_SCALAR: acc + k0; MUL_SCALAR: acc * k0; AFFINE: f32(acc * k0) + k1
+ *   SUB_DIV: (acc - k0) / k1; CLAMP: min(max(acc, k0), k1)
+ *   ABS: the sign bit cleared; SQRT: f32(sqrt(f64(acc)))
+ */
+enum {
+    STRATA_VEC_ADD = 0,
+    STRATA_VEC_SUB = 1,
+    STRATA_VEC_MUL = 2,
+    STRATA_VEC_DIV = 3,
+    STRATA_VEC_MIN = 4,
+    STRATA_VEC_MAX = 5,
+    STRATA_VEC_ADD_SCALAR = 6,
+    STRATA_VEC_MUL_SCALAR = 7,
+    STRATA_VEC_AFFINE = 8,
+    STRATA_VEC_SUB_DIV = 9,
+    STRATA_VEC_CLAMP = 10,
+    STRATA_VEC_ABS = 11,
+    STRATA_VEC_SQRT = 12
+};
+
+/* vec.MaxSteps: the longest chain of pointwise stages one call takes, and
+ * the most inputs a pointwise pipeline reads. */
+#define STRATA_MAX_STEPS 16
+#define STRATA_MAX_INPUTS 4
 
 /* strata_stage.kind for STRATA_OP_CURVATURE (stencil.CurvatureKind). */
 enum { STRATA_CURV_PROFILE = 0, STRATA_CURV_PLAN = 1, STRATA_CURV_MEAN = 2 };
@@ -113,6 +145,8 @@ typedef struct {
  *   HEATLOAD   k[0]=kx k[1]=ky, table[0]=the regression's eight float64
  *              terms K0 A BX BY E F CX CY as 16 floats, kind=1 takes exp
  *   ORIENTATION k[0]=kx k[1]=ky, kind bit 0 eastness, bit 1 unweighted
+ *   STEP       kind=STRATA_VEC_*, k[0] k[1] the immediates, input the
+ *              source a binary step reads (-1 for every other op)
  * With flags STRATA_STAGE_FIT (terrain/fit.go, FitRadius > 0) a GRADIENT,
  * SLOPE, ASPECT, HILLSHADE, HEATLOAD, ORIENTATION or CURVATURE stage takes
  * its derivatives from Wood's quadratic fit: radius is the fit's,
@@ -129,6 +163,8 @@ typedef struct {
     float k[16];
     const float *table[4];
     int32_t table_len[4];
+    int32_t input;    /* STEP: see above; ignored by the other ops */
+    int32_t reserved;
 } strata_stage;
 
 /*
@@ -182,12 +218,17 @@ int strata_download(strata_ctx *ctx, void *host, const void *dev, size_t bytes);
 /*
  * exec.ProcessN (internal/exec/process.go:28) for one kernel or a
  * pipeline: stages[0] is any op, stages[1..nstages-1] pointwise ops
- * (LOOKUP / RECLASS) applied to its result in order, as exec.Pipeline
- * runs Slope -> Lookup -> Reclass (graph/run.go:390-486). src holds nsrc
- * = 1 raster; dst holds 2 rasters for GRADIENT, else 1. Edge cells (within
- * the radius of the raster's border) get NaN and invalid; interior
- * validity is the AND of the input's validity over the window
- * (internal/exec/halo.go:21-229). stats may be NULL.
+ * (LOOKUP / RECLASS / unary STEP) applied to its result in order, as
+ * exec.Pipeline runs Slope -> Lookup -> Reclass (graph/run.go:390-486);
+ * at most STRATA_MAX_STEPS pointwise stages, 4 of them LOOKUP / RECLASS.
+ * src holds nsrc = 1 raster, except for a pipeline of pointwise stages
+ * only (a vec.Chain, internal/exec/pipeline.go:432-490), which starts
+ * from src[0] and whose binary STEPs read src[input]: 1 to
+ * STRATA_MAX_INPUTS rasters of one size. dst holds 2 rasters for
+ * GRADIENT, else 1. Edge cells (within the radius of the raster's border)
+ * get NaN and invalid; interior validity is the AND of the inputs'
+ * validity over the window (internal/exec/halo.go:21-229). stats may be
+ * NULL.
  */
 int strata_process(strata_ctx *ctx, const strata_stage *stages, int nstages,
                    const strata_raster *src, int nsrc, const strata_raster *dst, int ndst,
@@ -438,6 +479,16 @@ int strata_stage_lookup(const float *xs, const float *ys, int32_t n, strata_stag
 /* transfer.newReclassKernel (transfer/transfer.go:187-195). */
 int strata_stage_reclass(const float *breaks, int32_t nbreaks, const float *values, int32_t nvalues,
                          strata_stage *out);
+/* One vec.Chain step (vec.NewChain's checks, internal/vec/chain.go:
+ * 106-132): op a STRATA_VEC_*; input the source a binary op reads (0 to
+ * STRATA_MAX_INPUTS - 1), -1 for the others; k0, k1 the immediates. */
+int strata_stage_step(int32_t op, int32_t input, float k0, float k1, strata_stage *out);
+/* transfer.Rescale's kernel (transfer/transfer.go:56-60, tiled.go:108-110):
+ * an AFFINE step with a and b. */
+int strata_stage_rescale(float a, float b, strata_stage *out);
+/* transfer.RescaleRange (transfer/transfer.go:87-92, 236-250): the AFFINE
+ * step sending [in_lo, in_hi] to [out_lo, out_hi], with its checks. */
+int strata_stage_rescale_range(float in_lo, float in_hi, float out_lo, float out_hi, strata_stage *out);
 /* terrain.heatLoadOp / heatLoadTerms (terrain/heatload.go:110-146). */
 int strata_stage_heatload(strata_heatload_options *o, strata_stage *out);
 /* terrain.orientationOp (terrain/orientation.go:55-76). */

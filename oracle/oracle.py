@@ -22,7 +22,10 @@ LIB_PATH = os.path.join(HERE, "liboracle.so")
 
 GRADIENT, SLOPE, ASPECT, HILLSHADE, CURVATURE, RUGGEDNESS = 1, 2, 3, 4, 5, 6
 CORRELATE, SEPARABLE, MEAN, MIN, MAX, LOOKUP, RECLASS = 7, 8, 9, 10, 11, 12, 13
-HEATLOAD, ORIENTATION = 14, 15
+HEATLOAD, ORIENTATION, STEP = 14, 15, 16
+# vec.Op (internal/vec/chain.go:24-38): the kind of a STEP stage
+(VEC_ADD, VEC_SUB, VEC_MUL, VEC_DIV, VEC_MIN, VEC_MAX, VEC_ADD_SCALAR, VEC_MUL_SCALAR, VEC_AFFINE, VEC_SUB_DIV,
+ VEC_CLAMP, VEC_ABS, VEC_SQRT) = range(13)
 STAGE_FIT = 2  # the derivatives from Wood's quadratic fit over the (2 radius + 1)^2 window
 
 
@@ -35,6 +38,8 @@ class Stage(ctypes.Structure):
         ("k", ctypes.c_float * 16),
         ("table", ctypes.c_void_p * 4),
         ("table_len", ctypes.c_int32 * 4),
+        ("input", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
     ]
 
 
@@ -90,6 +95,9 @@ def lib():
         L.orc_process_ex.restype = ctypes.c_int
         L.orc_process_ex.argtypes = [ctypes.POINTER(Stage), ctypes.c_int, ctypes.POINTER(Raster),
                                      ctypes.POINTER(Raster), ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.orc_process_n.restype = ctypes.c_int
+        L.orc_process_n.argtypes = [ctypes.POINTER(Stage), ctypes.c_int, ctypes.POINTER(Raster), ctypes.c_int,
+                                    ctypes.POINTER(Raster), ctypes.c_int, ctypes.c_int]
         _lib = L
     return _lib
 
@@ -160,10 +168,10 @@ def gaussian(radius, sigma):
 # ---------------------------------------------------------------------------
 # Whole-raster calls.
 
-def stage(op, radius=0, kind=0, k=(), tables=(), flags=0):
+def stage(op, radius=0, kind=0, k=(), tables=(), flags=0, input=-1):
     """Builds a Stage; returns (stage, keepalive) so table arrays outlive it."""
     st = Stage()
-    st.op, st.radius, st.kind, st.flags = op, radius, kind, flags
+    st.op, st.radius, st.kind, st.flags, st.input = op, radius, kind, flags, input
     for i, v in enumerate(k):
         st.k[i] = float(v)
     keep = []
@@ -198,6 +206,32 @@ def process(stages, src, dsts, nthreads=1, simd=False):
     rc = lib().orc_process_ex(st_arr, len(stages), ctypes.byref(s), d_arr, len(dsts), nthreads, 1 if simd else 0)
     if rc != 0:
         raise ValueError(f"oracle: invalid call (rc={rc})")
+
+
+def process_n(stages, srcs, dsts, nthreads=1):
+    """Runs a pipeline over several inputs (a pointwise chain whose binary
+    steps read srcs[input]); srcs and dsts as process() takes them."""
+    st_arr = (Stage * len(stages))(*[s for s, _ in stages])
+    s_arr = (Raster * len(srcs))(*[_raster(**x) for x in srcs])
+    d_arr = (Raster * len(dsts))(*[_raster(**d) for d in dsts])
+    rc = lib().orc_process_n(st_arr, len(stages), s_arr, len(srcs), d_arr, len(dsts), nthreads)
+    if rc != 0:
+        raise ValueError(f"oracle: invalid call (rc={rc})")
+
+
+def step_stage(op, input=-1, k0=0.0, k1=0.0):
+    """One vec.Chain step (kind = the vec.Op)."""
+    return stage(STEP, 0, op, (k0, k1), input=input)
+
+
+def rescale_range_coeffs(in_lo, in_hi, out_lo, out_hi):
+    """transfer.rescaleCoeffs (transfer/transfer.go:236-250) without its
+    checks: a = f32((outHi - outLo) / (inHi - inLo)), b = f32(outLo - a*inLo)
+    in float64."""
+    a = np.float32((float(np.float32(out_hi)) - float(np.float32(out_lo))) /
+                   (float(np.float32(in_hi)) - float(np.float32(in_lo))))
+    b = np.float32(float(np.float32(out_lo)) - float(a) * float(np.float32(in_lo)))
+    return a, b
 
 
 # ---------------------------------------------------------------------------

@@ -580,8 +580,33 @@ static inline float reclass(float v, const float *breaks, int nb, const float *v
     return values[k];
 }
 
+/* One vec.Chain step (internal/vec/chain.go:24-38, the scalar kernels
+ * of internal/vec/scalar.go:1-120): acc the running value, b the binary
+ * ops' second operand. Each operation rounds on its own (no FMA). */
+static inline float vec_step(int op, float acc, float b, float k0, float k1)
+{
+    switch (op) {
+    case 0: return acc + b;
+    case 1: return acc - b;
+    case 2: return acc * b;
+    case 3: return acc / b;
+    case 4: return orc_go_min(acc, b);
+    case 5: return orc_go_max(acc, b);
+    case 6: return acc + k0;
+    case 7: return acc * k0;
+    case 8: { float t = acc * k0; return t + k1; }   /* Affine: float32(v*a) + b */
+    case 9: { float t = acc - k0; return t / k1; }   /* SubDiv: (v - lo) / span */
+    case 10: return orc_go_min(orc_go_max(acc, k0), k1);
+    case 11: return u2f(f2u(acc) & 0x7fffffffu);      /* Abs: the sign bit cleared */
+    default: return (float)sqrt((double)acc);         /* Sqrt */
+    }
+}
+
+static inline int step_binary(const orc_stage *st) { return st->op == ORC_STEP && st->kind >= 0 && st->kind <= 5; }
+
 static inline float pointwise(const orc_stage *st, float v)
 {
+    if (st->op == ORC_STEP) return vec_step(st->kind, v, 0.0f, st->k[0], st->k[1]);
     if (st->op == ORC_LOOKUP) return lookup(v, st->table[0], st->table[1], st->table_len[0]);
     return reclass(v, st->table[0], st->table_len[0], st->table[1]);
 }
@@ -700,6 +725,8 @@ typedef struct {
     const orc_stage *stages;
     int nstages;
     const orc_raster *src;
+    const orc_raster *srcs; /* a pointwise pipeline's inputs (src is srcs[0]) */
+    int nsrc;
     const orc_raster *dst;
     int ndst;
     int r;
@@ -861,7 +888,7 @@ static void run_rows(const job_t *jb, int64_t y0, int64_t y1, unsigned char *col
     int64_t W = src->width, H = src->height, s = src->stride;
     int r = jb->r;
     const float nanf_ = u2f(0x7fc00000u);
-    int stencil = !(st->op == ORC_LOOKUP || st->op == ORC_RECLASS);
+    int stencil = !(st->op == ORC_LOOKUP || st->op == ORC_RECLASS || st->op == ORC_STEP);
     for (int64_t y = y0; y < y1; y++) {
         float *o0 = jb->dst[0].data + y * jb->dst[0].stride;
         float *o1 = jb->ndst > 1 ? jb->dst[1].data + y * jb->dst[1].stride : NULL;
@@ -870,7 +897,15 @@ static void run_rows(const job_t *jb, int64_t y0, int64_t y1, unsigned char *col
         if (!stencil) {
             for (int64_t x = 0; x < W; x++) {
                 float v = row[x];
-                for (int i = 0; i < jb->nstages; i++) v = pointwise(&jb->stages[i], v);
+                for (int i = 0; i < jb->nstages; i++) {
+                    const orc_stage *p = &jb->stages[i];
+                    if (step_binary(p)) {
+                        const orc_raster *b = &jb->srcs[p->input];
+                        v = vec_step(p->kind, v, b->data[y * b->stride + x], 0.0f, 0.0f);
+                    } else {
+                        v = pointwise(p, v);
+                    }
+                }
                 o0[x] = v;
             }
         } else {
@@ -904,8 +939,15 @@ static void run_rows(const job_t *jb, int64_t y0, int64_t y1, unsigned char *col
             }
             unsigned char *vbuf = colok + W + 1;
             if (!stencil) {
-                for (int64_t x = 0; x < W; x++)
-                    vbuf[x] = (unsigned char)(src->valid ? get_bit(src->valid, src->valid_offset + y * s + x) : 1);
+                /* halo.go:213-229 at reach 0: every masked input's bit */
+                for (int64_t x = 0; x < W; x++) {
+                    int ok = 1;
+                    for (int j = 0; j < jb->nsrc; j++) {
+                        const orc_raster *in = &jb->srcs[j];
+                        if (in->valid) ok &= get_bit(in->valid, in->valid_offset + y * in->stride + x);
+                    }
+                    vbuf[x] = (unsigned char)ok;
+                }
             } else if (!yin) {
                 memset(vbuf, 0, (size_t)W);
             } else {
@@ -985,16 +1027,47 @@ int orc_process(const orc_stage *stages, int nstages, const orc_raster *src,
     return orc_process_ex(stages, nstages, src, dst, ndst, nthreads, 0);
 }
 
+static int process_impl(const orc_stage *stages, int nstages, const orc_raster *srcs, int nsrc,
+                        const orc_raster *dst, int ndst, int nthreads, int simd);
+
 int orc_process_ex(const orc_stage *stages, int nstages, const orc_raster *src,
                    const orc_raster *dst, int ndst, int nthreads, int simd)
 {
-    if (nstages < 1 || !src || !dst) return -1;
+    return process_impl(stages, nstages, src, 1, dst, ndst, nthreads, simd);
+}
+
+int orc_process_n(const orc_stage *stages, int nstages, const orc_raster *src, int nsrc,
+                  const orc_raster *dst, int ndst, int nthreads)
+{
+    return process_impl(stages, nstages, src, nsrc, dst, ndst, nthreads, 0);
+}
+
+static int process_impl(const orc_stage *stages, int nstages, const orc_raster *srcs, int nsrc,
+                        const orc_raster *dst, int ndst, int nthreads, int simd)
+{
+    const orc_raster *src = srcs;
+    if (nstages < 1 || !src || !dst || nsrc < 1 || nsrc > 4) return -1;
     const orc_stage *st = &stages[0];
-    if (st->op < ORC_GRADIENT || st->op > ORC_ORIENTATION) return -1;
+    if (st->op < ORC_GRADIENT || st->op > ORC_STEP) return -1;
     if ((st->flags & ORC_STAGE_FIT) && (st->radius < 1 || st->radius > 8)) return -1;
     if ((st->op == ORC_HEATLOAD) && (!st->table[0] || st->table_len[0] != 16)) return -1;
+    const int lead_pointwise = st->op == ORC_LOOKUP || st->op == ORC_RECLASS || st->op == ORC_STEP;
+    if (!lead_pointwise && nsrc != 1) return -1;
     for (int i = 1; i < nstages; i++)
-        if (stages[i].op != ORC_LOOKUP && stages[i].op != ORC_RECLASS) return -1;
+        if (stages[i].op != ORC_LOOKUP && stages[i].op != ORC_RECLASS && stages[i].op != ORC_STEP) return -1;
+    /* vec.NewChain's checks (internal/vec/chain.go:106-132) */
+    for (int i = 0; i < nstages; i++) {
+        const orc_stage *p = &stages[i];
+        if (p->op != ORC_STEP) continue;
+        if (p->kind < 0 || p->kind > 12) return -1;
+        if (step_binary(p) ? (p->input < 0 || p->input >= nsrc) : p->input != -1) return -1;
+    }
+    for (int j = 0; j < nsrc; j++) {
+        if (srcs[j].width != dst[0].width || srcs[j].height != dst[0].height) return -1;
+        if (srcs[j].valid)
+            for (int d = 0; d < ndst; d++)
+                if (!dst[d].valid) return -1;
+    }
     /* Pointwise tables: Lookup's knots and values pair up (at least one);
      * Reclass has one value more than breaks (zero breaks allowed). */
     for (int i = 0; i < nstages; i++) {
@@ -1013,10 +1086,12 @@ int orc_process_ex(const orc_stage *stages, int nstages, const orc_raster *src,
     jb.stages = stages;
     jb.nstages = nstages;
     jb.src = src;
+    jb.srcs = srcs;
+    jb.nsrc = nsrc;
     jb.dst = dst;
     jb.ndst = ndst;
     jb.simd = simd;
-    jb.r = (st->op == ORC_LOOKUP || st->op == ORC_RECLASS) ? 0
+    jb.r = lead_pointwise ? 0
            : (st->flags & ORC_STAGE_FIT) ? st->radius
            : (st->op <= ORC_HILLSHADE || st->op == ORC_CURVATURE || st->op >= ORC_HEATLOAD) ? 1
            : st->radius;

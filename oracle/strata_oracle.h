@@ -33,7 +33,8 @@ enum {
     ORC_LOOKUP = 12,
     ORC_RECLASS = 13,
     ORC_HEATLOAD = 14,
-    ORC_ORIENTATION = 15
+    ORC_ORIENTATION = 15,
+    ORC_STEP = 16 /* one vec.Chain step: kind = vec.Op, k[0..1], input */
 };
 
 /* orc_stage.flags: the stage's derivatives come from Wood's quadratic fit
@@ -50,6 +51,8 @@ typedef struct {
     float k[16];
     const float *table[4];
     int32_t table_len[4];
+    int32_t input; /* ORC_STEP: the source a binary step reads, -1 for the others */
+    int32_t reserved;
 } orc_stage;
 
 typedef struct {
@@ -90,6 +93,13 @@ int orc_process(const orc_stage *stages, int nstages, const orc_raster *src,
  * results are the same bits; this is the timed CPU baseline. */
 int orc_process_ex(const orc_stage *stages, int nstages, const orc_raster *src,
                    const orc_raster *dst, int ndst, int nthreads, int simd);
+
+/* A pipeline over nsrc inputs (1 to 4): a stencil-led one takes one; a
+ * pointwise one (a vec.Chain with Lookup / Reclass stages among its
+ * steps) starts from src[0], its binary steps read src[input], and its
+ * output is valid where every masked input is. */
+int orc_process_n(const orc_stage *stages, int nstages, const orc_raster *src, int nsrc,
+                  const orc_raster *dst, int ndst, int nthreads);
 
 /* The restated AVX2 lanes of one interior row (strata_avx2.c): the first
  * multiple of eight of the n cells; returns how many it wrote. r0, r1, r2

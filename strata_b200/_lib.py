@@ -19,7 +19,12 @@ OK, EINVAL, ECUDA, ENOMEM, ECANCELED, ETIMEDOUT, EIO, ENOTSUP = 0, -1, -2, -3, -
 
 OP_GRADIENT, OP_SLOPE, OP_ASPECT, OP_HILLSHADE, OP_CURVATURE, OP_RUGGEDNESS = 1, 2, 3, 4, 5, 6
 OP_CORRELATE, OP_SEPARABLE, OP_MEAN, OP_MIN, OP_MAX, OP_LOOKUP, OP_RECLASS = 7, 8, 9, 10, 11, 12, 13
-OP_HEATLOAD, OP_ORIENTATION = 14, 15
+OP_HEATLOAD, OP_ORIENTATION, OP_STEP = 14, 15, 16
+# vec.Op (internal/vec/chain.go:24-38), strata_stage.kind of an OP_STEP stage
+(VEC_ADD, VEC_SUB, VEC_MUL, VEC_DIV, VEC_MIN, VEC_MAX, VEC_ADD_SCALAR, VEC_MUL_SCALAR, VEC_AFFINE, VEC_SUB_DIV,
+ VEC_CLAMP, VEC_ABS, VEC_SQRT) = range(13)
+MAX_STEPS = 16
+MAX_INPUTS = 4
 STAGE_ROTATE180 = 1
 STAGE_FIT = 2
 EXEC_ASYNC = 1
@@ -37,7 +42,8 @@ class Raster(ctypes.Structure):
 
 class Stage(ctypes.Structure):
     _fields_ = [("op", ctypes.c_uint32), ("radius", c_i32), ("kind", c_i32), ("flags", c_i32),
-                ("k", c_f32 * 16), ("table", c_p * 4), ("table_len", c_i32 * 4)]
+                ("k", c_f32 * 16), ("table", c_p * 4), ("table_len", c_i32 * 4), ("input", c_i32),
+                ("reserved", c_i32)]
 
 
 class ExecOpts(ctypes.Structure):
@@ -206,6 +212,9 @@ SIGNATURES = [
     ("strata_stage_reclass", ctypes.c_int, [c_p, c_i32, c_p, c_i32, ctypes.POINTER(Stage)]),
     ("strata_stage_heatload", ctypes.c_int, [ctypes.POINTER(HeatLoadOptions), ctypes.POINTER(Stage)]),
     ("strata_stage_orientation", ctypes.c_int, [ctypes.POINTER(OrientationOptions), ctypes.POINTER(Stage)]),
+    ("strata_stage_step", ctypes.c_int, [c_i32, c_i32, c_f32, c_f32, ctypes.POINTER(Stage)]),
+    ("strata_stage_rescale", ctypes.c_int, [c_f32, c_f32, ctypes.POINTER(Stage)]),
+    ("strata_stage_rescale_range", ctypes.c_int, [c_f32, c_f32, c_f32, c_f32, ctypes.POINTER(Stage)]),
     ("strata_focal_gaussian", ctypes.c_int, [c_i32, c_f64, ctypes.POINTER(c_f32)]),
 ]
 

@@ -155,9 +155,11 @@ struct strata_ctx {
 namespace {
 
 // Context buffer slots: 0 and 1 a host source's cells and mask, 2 + 2i
-// and 3 + 2i host destination i's; from kFitScratchSlot the raw sums of
-// Wood's fit.
+// and 3 + 2i host destination i's, kInputSlot + 2j and the next a further
+// host source j's; from kFitScratchSlot the raw sums of Wood's fit.
 constexpr int kFitScratchSlot = 128;
+// From kInputSlot + 2j: a host source j >= 1's cells and mask.
+constexpr int kInputSlot = 8;
 
 int ensure(strata_ctx* c, int slot, size_t bytes, void** out) {
     if ((int)c->bufs.size() <= slot) c->bufs.resize(slot + 1);
@@ -364,7 +366,28 @@ bool bit_spans(const strata_raster& a, const strata_raster& b) {
     return spans_meet(bit_addr(a), span_cells(a), bit_addr(b), span_cells(b));
 }
 
-bool is_pointwise(uint32_t op) { return op == STRATA_OP_LOOKUP || op == STRATA_OP_RECLASS; }
+// vec.Op's names (internal/vec/chain.go:45-51).
+const char* vec_name(int op) {
+    static const char* const names[] = {"Add",    "Sub",     "Mul",   "Div", "Min", "Max", "AddScalar",
+                                        "MulScalar", "Affine", "SubDiv", "Clamp", "Abs", "Sqrt"};
+    return op >= 0 && op <= STRATA_VEC_SQRT ? names[op] : "Op";
+}
+
+bool is_pointwise(uint32_t op) { return op == STRATA_OP_LOOKUP || op == STRATA_OP_RECLASS || op == STRATA_OP_STEP; }
+bool binary_step(int op) { return op >= STRATA_VEC_ADD && op <= STRATA_VEC_MAX; }
+
+// vec.NewChain's step checks (internal/vec/chain.go:106-132).
+int check_step(int op, int input) {
+    if (op < STRATA_VEC_ADD || op > STRATA_VEC_SQRT)
+        return fail(STRATA_EINVAL, "vec: chain step has unknown operation Op(%d)", op);
+    if (binary_step(op) && (input < 0 || input >= STRATA_MAX_INPUTS))
+        return fail(STRATA_EINVAL, "vec: chain step (%s) reads input %d, which is not one of its %d", vec_name(op),
+                    input, STRATA_MAX_INPUTS);
+    if (!binary_step(op) && input != -1)
+        return fail(STRATA_EINVAL, "vec: chain step (%s) reads no input, so its Src must be -1, not %d", vec_name(op),
+                    input);
+    return STRATA_OK;
+}
 
 int op_radius(const strata_stage& s) {
     if (s.flags & STRATA_STAGE_FIT) return s.radius;
@@ -389,6 +412,14 @@ bool finite32(float v) { return v - v == 0; }
 
 // A stage's tables into the launch parameters.
 int fill_stage(const strata_stage& s, LaunchParams& p, int epi_index) {
+    if (s.op == STRATA_OP_STEP) {
+        int rc = check_step(s.kind, s.input);
+        if (rc) return rc;
+        if (p.nstep >= STRATA_MAX_STEPS)
+            return fail(STRATA_EINVAL, "vec: chain has more than %d steps", STRATA_MAX_STEPS);
+        p.step[p.nstep++] = strata::ChainStep{s.kind, binary_step(s.kind) ? s.input : 0, s.k[0], s.k[1]};
+        return STRATA_OK;
+    }
     if (is_pointwise(s.op)) {
         if (epi_index >= strata::kMaxEpilogue)
             return fail(STRATA_ENOTSUP, "engine: a pipeline on the gpu backend takes at most %d pointwise stages",
@@ -596,7 +627,7 @@ bool fold_stages(const LaunchParams& p, EpiStage* out) {
 // the last few folds of the calling thread (a fold bisects the floats, a
 // cached one is a table compare).
 void fold_tail(LaunchParams& p) {
-    if (p.nepi < 2) return;
+    if (p.nepi < 2 || p.nstep) return;
     struct Entry {
         int nepi = 0;
         EpiStage in[strata::kMaxEpilogue];
@@ -672,7 +703,7 @@ float host_slope_of_square(float s, float scale, bool take_atan) {
 }
 
 void fold_slope_square(LaunchParams& p) {
-    if (p.op != STRATA_OP_SLOPE || p.nepi != 1 || p.epi[0].op != STRATA_OP_RECLASS) return;
+    if (p.op != STRATA_OP_SLOPE || p.nstep || p.nepi != 1 || p.epi[0].op != STRATA_OP_RECLASS) return;
     EpiStage& e = p.epi[0];
     const float scale = p.k[p.fit ? 5 : 2];  // a fit's product constants follow its five factors
     if (e.n > strata::kChainBreaks || !(scale > 0) || std::isinf(scale)) return;
@@ -704,27 +735,45 @@ int plan_stages(const strata_stage* stages, int nstages, LaunchParams& p, int* n
     if (!stages || nstages < 1) return fail(STRATA_EINVAL, "engine: nil kernel");
     memset(&p, 0, sizeof p);
     const strata_stage& s0 = stages[0];
-    if (s0.op < STRATA_OP_GRADIENT || s0.op > STRATA_OP_ORIENTATION)
+    if (s0.op < STRATA_OP_GRADIENT || s0.op > STRATA_OP_STEP)
         return fail(STRATA_EINVAL, "engine: unknown op %u", s0.op);
     int epi = 0;
     int rc;
-    if (is_pointwise(s0.op)) {
+    const bool pointwise = is_pointwise(s0.op);
+    if (!pointwise && (rc = fill_stage(s0, p, 0)) != STRATA_OK) return rc;
+    if (pointwise) {
         p.op = (int)s0.op;
         p.radius = 0;
-        for (int i = 0; i < nstages; i++) {
-            if (!is_pointwise(stages[i].op))
-                return fail(STRATA_ENOTSUP,
-                            "engine: a pipeline on the gpu backend is one stencil stage followed by pointwise stages");
-            if ((rc = fill_stage(stages[i], p, epi++)) != STRATA_OK) return rc;
+    }
+    // The tail: the tables in epi[], and, when it holds a chain step, the
+    // whole tail as a step sequence naming the tables by index.
+    bool seq = false;
+    for (int i = 0; i < nstages; i++) seq = seq || stages[i].op == STRATA_OP_STEP;
+    p.ninputs = 1;
+    for (int i = pointwise ? 0 : 1; i < nstages; i++) {
+        const strata_stage& s = stages[i];
+        if (!is_pointwise(s.op) || s0.op == STRATA_OP_GRADIENT)
+            return fail(STRATA_ENOTSUP,
+                        "engine: a pipeline on the gpu backend is one stencil stage followed by pointwise stages");
+        if (s.op == STRATA_OP_STEP) {
+            if ((rc = fill_stage(s, p, 0)) != STRATA_OK) return rc;
+            if (binary_step(s.kind)) {
+                if (!pointwise)
+                    return fail(STRATA_ENOTSUP,
+                                "engine: a %s step reads a second input, which a stencil's pipeline on the gpu "
+                                "backend does not take",
+                                vec_name(s.kind));
+                if (s.input + 1 > p.ninputs) p.ninputs = s.input + 1;
+            }
+            continue;
         }
-    } else {
-        if ((rc = fill_stage(s0, p, 0)) != STRATA_OK) return rc;
-        for (int i = 1; i < nstages; i++) {
-            if (!is_pointwise(stages[i].op) || s0.op == STRATA_OP_GRADIENT)
-                return fail(STRATA_ENOTSUP,
-                            "engine: a pipeline on the gpu backend is one stencil stage followed by pointwise stages");
-            if ((rc = fill_stage(stages[i], p, epi++)) != STRATA_OK) return rc;
+        if ((rc = fill_stage(s, p, epi)) != STRATA_OK) return rc;
+        if (seq) {
+            if (p.nstep >= STRATA_MAX_STEPS)
+                return fail(STRATA_EINVAL, "vec: chain has more than %d steps", STRATA_MAX_STEPS);
+            p.step[p.nstep++] = strata::ChainStep{strata::kStepTable + epi, 0, 0.0f, 0.0f};
         }
+        epi++;
     }
     p.nepi = epi;
     fold_tail(p);
@@ -733,9 +782,11 @@ int plan_stages(const strata_stage* stages, int nstages, LaunchParams& p, int* n
     return STRATA_OK;
 }
 
-int check_operands(const strata_raster* src, int nsrc, const strata_raster* dst, int ndst, int nout, int r) {
-    if (nsrc != 1 || ndst != nout || !src || !dst)
-        return fail(STRATA_EINVAL, "engine: kernel takes 1 inputs and %d outputs, got %d and %d", nout, nsrc, ndst);
+int check_operands(const strata_raster* src, int nsrc, const strata_raster* dst, int ndst, int nout, int r,
+                   int nin = 1) {
+    if (nsrc != nin || ndst != nout || !src || !dst)
+        return fail(STRATA_EINVAL, "engine: kernel takes %d inputs and %d outputs, got %d and %d", nin, nout, nsrc,
+                    ndst);
     int rc;
     for (int i = 0; i < ndst; i++) {
         if ((rc = validate("dst", i, dst[i])) != STRATA_OK) return rc;
@@ -743,16 +794,28 @@ int check_operands(const strata_raster* src, int nsrc, const strata_raster* dst,
             return fail(STRATA_EINVAL, "engine: dst[%d] is %lld×%lld, dst[0] is %lld×%lld", i, (long long)dst[i].width,
                         (long long)dst[i].height, (long long)dst[0].width, (long long)dst[0].height);
     }
-    if ((rc = validate("src", 0, src[0])) != STRATA_OK) return rc;
-    if (src[0].width != dst[0].width || src[0].height != dst[0].height)
-        return fail(STRATA_EINVAL, "engine: src[0] is %lld×%lld, dst[0] is %lld×%lld", (long long)src[0].width,
-                    (long long)src[0].height, (long long)dst[0].width, (long long)dst[0].height);
-    for (int i = 0; i < ndst; i++)
-        if (src[0].valid && !dst[i].valid)
-            return fail(STRATA_EINVAL,
-                        "engine: an input has a validity mask but dst[%d].Valid is nil; allocate it with "
-                        "raster.NewFloat32Like, or set Valid on its root raster before windowing",
-                        i);
+    for (int j = 0; j < nsrc; j++) {
+        if ((rc = validate("src", j, src[j])) != STRATA_OK) return rc;
+        if (src[j].width != dst[0].width || src[j].height != dst[0].height)
+            return fail(STRATA_EINVAL, "engine: src[%d] is %lld×%lld, dst[0] is %lld×%lld", j, (long long)src[j].width,
+                        (long long)src[j].height, (long long)dst[0].width, (long long)dst[0].height);
+        for (int i = 0; i < ndst; i++)
+            if (src[j].valid && !dst[i].valid)
+                return fail(STRATA_EINVAL,
+                            "engine: an input has a validity mask but dst[%d].Valid is nil; allocate it with "
+                            "raster.NewFloat32Like, or set Valid on its root raster before windowing",
+                            i);
+    }
+    // A pointwise kernel's other inputs: each may be dst itself (read
+    // before the cell is written), never a part of it at another offset.
+    for (int j = 1; j < nsrc; j++)
+        for (int i = 0; i < ndst; i++) {
+            if (data_rel(dst[i], src[j]) == kPartial)
+                return fail(STRATA_EINVAL, "engine: dst[%d] overlaps src[%d] at a different offset or stride", i, j);
+            if (bits_rel(dst[i], src[j]) == kPartial)
+                return fail(STRATA_EINVAL,
+                            "engine: dst[%d] validity bits overlap src[%d]'s at a different offset or stride", i, j);
+        }
     for (int i = 0; i < ndst; i++) {
         for (int j = i + 1; j < ndst; j++) {
             bool dm = r == 0 ? data_rel(dst[i], dst[j]) != kDisjoint : data_spans(dst[i], dst[j]);
@@ -973,6 +1036,7 @@ int64_t launch_fit(strata_ctx* c, const LaunchParams& p, const ValidityParams* c
         q.kind = 0;
         q.fit = 0;
         q.nepi = 0;
+        q.nstep = 0;
         memset(&q.vf, 0, sizeof q.vf);
         for (int j = 0; j <= 2 * r; j++) {
             q.w[j] = taps[i][1][j];
@@ -1012,18 +1076,30 @@ extern "C" int strata_process(strata_ctx* c, const strata_stage* stages, int nst
     int rc = plan_stages(stages, nstages, p, &nout);
     if (rc) return rc;
     if ((rc = check_opts(opts))) return rc;
-    if ((rc = check_operands(src, nsrc, dst, ndst, nout, p.radius))) return rc;
+    // A pointwise pipeline reads every input it is given (vec.Chain.Run
+    // checks the ones it never reads too), at least those its steps name.
+    const bool chain = is_pointwise((uint32_t)p.op);
+    const int nin = chain && nsrc >= p.ninputs && nsrc <= STRATA_MAX_INPUTS ? nsrc : p.ninputs;
+    if ((rc = check_operands(src, nsrc, dst, ndst, nout, p.radius, nin))) return rc;
+    p.ninputs = nin;
 
     std::lock_guard<std::mutex> lock(c->mu);
     DeviceGuard device_guard(c->device);
     cudaStream_t st = (opts && opts->stream) ? (cudaStream_t)opts->stream : c->stream;
     const int64_t W = src[0].width, H = src[0].height;
 
-    DevOperand ds, dd[2];
+    DevOperand ds, dd[2], dx[STRATA_MAX_INPUTS];
     if ((rc = stage_in(c, st, src[0], 0, true, &ds))) return rc;
+    for (int j = 1; j < nin; j++)
+        if ((rc = stage_in(c, st, src[j], kInputSlot + 2 * j, true, &dx[j]))) return rc;
+    dx[0] = ds;
     for (int i = 0; i < ndst; i++)
         if ((rc = stage_in(c, st, dst[i], 2 + 2 * i, false, &dd[i]))) return rc;
 
+    for (int j = 0; j < nin; j++) {
+        p.in[j] = dx[j].data;
+        p.in_stride[j] = dx[j].stride;
+    }
     p.src = ds.data;
     p.src_stride = ds.stride;
     p.src_x0 = p.src_y0 = 0;
@@ -1065,12 +1141,29 @@ extern "C" int strata_process(strata_ctx* c, const strata_stage* stages, int nst
         int64_t wc = 0;
         ValidityParams vp[2];
         const ValidityParams* vs[2] = {nullptr, nullptr};
-        for (int i = 0; i < ndst; i++) {
+        for (int i = 0; i < ndst && nin == 1; i++) {
             if (!dst[i].valid) continue;
             fill_validity(vp[i], ds, src[0].valid != nullptr, dd[i], span_cells(dst[i]), W, H, p.radius, y0, y1);
             vs[i] = &vp[i];
         }
         int64_t t = p.fit ? launch_fit(c, p, vs, st, &wc) : strata::launch_stage(p, vs, st, &wc);
+        if (t >= 0 && nin > 1 && dst[0].valid) {
+            strata::AndValidityParams av;
+            memset(&av, 0, sizeof av);
+            for (int j = 0; j < nin; j++) {
+                av.src_bits[j] = src[j].valid ? dx[j].bits : nullptr;
+                av.src_off[j] = dx[j].bit_off;
+                av.src_stride[j] = dx[j].stride;
+            }
+            av.nsrc = nin;
+            av.dst_bits = dd[0].bits;
+            av.dst_off = dd[0].bit_off;
+            av.dst_stride = dd[0].stride;
+            av.width = W;
+            av.y0 = y0;
+            av.y1 = y1;
+            strata::launch_and_validity(av, st);
+        }
         if (t == -2) return fail(STRATA_ENOMEM, "engine: no device memory for the fit's sums");
         if (t < 0) return fail(STRATA_ENOTSUP, "engine: op %d at radius %d has no device kernel", p.op, p.radius);
         bands += t;
@@ -1092,7 +1185,7 @@ extern "C" int strata_process(strata_ctx* c, const strata_stage* stages, int nst
     if (stats) {
         int64_t cells = done_rows * W;
         stats->cells += cells;
-        stats->ideal += cells * 4 * (1 + nout);
+        stats->ideal += cells * 4 * (nin + nout);
         stats->bands += bands;
         stats->kernel_read += window * 4;
         stats->kernel_written += cells * 4 * nout;
@@ -1451,6 +1544,41 @@ extern "C" int strata_stage_reclass(const float* breaks, int32_t nbreaks, const 
     return STRATA_OK;
 }
 
+extern "C" int strata_stage_step(int32_t op, int32_t input, float k0, float k1, strata_stage* out) {
+    if (!out) return fail(STRATA_EINVAL, "vec: nil stage");
+    int rc = check_step(op, input);
+    if (rc) return rc;
+    stage_init(out, STRATA_OP_STEP);
+    out->kind = op;
+    out->input = input;
+    out->k[0] = k0;
+    out->k[1] = k1;
+    return STRATA_OK;
+}
+
+extern "C" int strata_stage_rescale(float a, float b, strata_stage* out) {
+    return strata_stage_step(STRATA_VEC_AFFINE, -1, a, b, out);
+}
+
+// transfer.rescaleCoeffs (transfer/transfer.go:236-250).
+extern "C" int strata_stage_rescale_range(float in_lo, float in_hi, float out_lo, float out_hi, strata_stage* out) {
+    const char* op = "transfer.RescaleRange";
+    if (!out) return fail(STRATA_EINVAL, "%s: nil stage", op);
+    if (!finite32(in_lo) || !finite32(in_hi) || in_lo == in_hi)
+        return fail(STRATA_EINVAL, "%s: inLo and inHi must be finite and different, got %s and %s", op,
+                    fmt_v(in_lo, true).c_str(), fmt_v(in_hi, true).c_str());
+    if (!finite32(out_lo) || !finite32(out_hi))
+        return fail(STRATA_EINVAL, "%s: outLo and outHi must be finite, got %s and %s", op, fmt_v(out_lo, true).c_str(),
+                    fmt_v(out_hi, true).c_str());
+    const float a = (float)(((double)out_hi - (double)out_lo) / ((double)in_hi - (double)in_lo));
+    const float b = (float)((double)out_lo - (double)a * (double)in_lo);
+    if (!finite32(a) || !finite32(b))
+        return fail(STRATA_EINVAL, "%s: [%s, %s] to [%s, %s] gives a scale of %s and an offset of %s; both must be finite",
+                    op, fmt_v(in_lo, true).c_str(), fmt_v(in_hi, true).c_str(), fmt_v(out_lo, true).c_str(),
+                    fmt_v(out_hi, true).c_str(), fmt_v(a, true).c_str(), fmt_v(b, true).c_str());
+    return strata_stage_step(STRATA_VEC_AFFINE, -1, a, b, out);
+}
+
 // McCune and Keon's coefficients (terrain/heatload.go:104-108).
 static const double kHeatLoadCoef[3][6] = {
     {-1.467, 1.582, -1.500, -0.262, 0.607, 0},
@@ -1589,6 +1717,8 @@ extern "C" int strata_process_chunked(strata_ctx* c, const strata_stage* stages,
     int rc = plan_stages(stages, nstages, p, &nout);
     if (rc) return rc;
     if (p.fit) return fail(STRATA_ENOTSUP, "engine: Wood's fit (FitRadius > 0) has no chunked form on the gpu backend");
+    if (p.ninputs > 1 || nsrc > 1)
+        return fail(STRATA_ENOTSUP, "engine: a chain over several inputs has no chunked form on the gpu backend");
     if ((rc = check_opts(opts))) return rc;
     if (nsrc != 1 || ndst != nout || !src || !dst)
         return fail(STRATA_EINVAL, "engine: kernel takes 1 inputs and %d outputs, got %d and %d", nout, nsrc, ndst);
@@ -1858,6 +1988,9 @@ extern "C" int strata_process_features(strata_ctx* c, const strata_stage* stages
     for (int f = 0; f < nfeatures; f++) {
         if (counts[f] < 1) return fail(STRATA_EINVAL, "terrain: Features output %d has no Op", f);
         if ((rc = plan_stages(stages + off, counts[f], plans[(size_t)f], &nouts[(size_t)f]))) return rc;
+        if (plans[(size_t)f].ninputs > 1)
+            return fail(STRATA_EINVAL, "engine: a feature reads one input, feature %d's chain reads %d", f,
+                        plans[(size_t)f].ninputs);
         first[(size_t)f] = outs;
         outs += nouts[(size_t)f];
         off += counts[f];
@@ -2063,10 +2196,10 @@ int fill_batch_item(strata_ctx* c, const strata_batch_item& it, int i, strata::B
     LaunchParams p;
     int nout = 0, rc;
     if ((rc = plan_stages(it.stages, it.nstages, p, &nout))) return rc;
-    if ((rc = check_operands(&it.src, 1, it.dst, nout, nout, p.radius))) return rc;
+    if ((rc = check_operands(&it.src, 1, it.dst, nout, nout, p.radius, p.ninputs))) return rc;
     if (!it.src.on_device || !it.dst[0].on_device || (nout > 1 && !it.dst[1].on_device))
         return fail(STRATA_EINVAL, "engine: batch raster %d: the rasters of a batch must be on the device", i);
-    if (p.op == STRATA_OP_LOOKUP || p.op == STRATA_OP_RECLASS)
+    if (is_pointwise((uint32_t)p.op))
         return fail(STRATA_ENOTSUP, "engine: batch raster %d: a pointwise op alone has no batch kernel", i);
     if (p.fit || p.op == STRATA_OP_HEATLOAD || p.op == STRATA_OP_ORIENTATION)
         return fail(STRATA_ENOTSUP, "engine: batch raster %d: op %d has no batch kernel", i, p.op);
@@ -2671,7 +2804,7 @@ Request* prepare_request(strata_server* S, const strata_stage* stages, int nstag
                 st.table[k] = r->tables.back().data();
             }
     int rc = plan_stages(r->stages.data(), (int)r->stages.size(), r->p, &r->nout);
-    if (rc == STRATA_OK && (r->p.op == STRATA_OP_LOOKUP || r->p.op == STRATA_OP_RECLASS))
+    if (rc == STRATA_OK && is_pointwise((uint32_t)r->p.op))
         rc = fail(STRATA_ENOTSUP, "engine: a pointwise op alone has no batch kernel");
     if (rc == STRATA_OK && (r->p.fit || r->p.op == STRATA_OP_HEATLOAD || r->p.op == STRATA_OP_ORIENTATION))
         rc = fail(STRATA_ENOTSUP, "engine: op %d has no batch kernel", r->p.op);

@@ -160,7 +160,7 @@ Key key_of(const LaunchParams& p) {
         k.radius = 1;
         if (p.op == STRATA_OP_SLOPE || p.op == STRATA_OP_ASPECT) k.kind = p.kind;
         if (p.op == STRATA_OP_CURVATURE || p.op == STRATA_OP_RUGGEDNESS) k.kind = p.kind;
-        k.epi = p.nepi > 0;
+        k.epi = has_tail(p);
     } else if (p.op == STRATA_OP_CORRELATE || (p.op == STRATA_OP_RUGGEDNESS && p.kind != STRATA_RUG_ROUGHNESS)) {
         k.family = 2;
         k.kind = p.op == STRATA_OP_RUGGEDNESS ? p.kind : 0;

@@ -12,6 +12,8 @@
 
 #include <cstdint>
 
+#include "strata_cuda.h"
+
 namespace strata {
 namespace cell {
 
@@ -468,6 +470,28 @@ __device__ __forceinline__ float lookup(float v, const float* xs, const float* y
 __device__ __forceinline__ float reclass(float v, const float* breaks, int nb, const float* values) {
     const float r = values[knots_at_or_below(v, breaks, nb)];
     return v != v ? v : r;
+}
+
+// One vec.Chain step (internal/vec/chain.go:24-38, the scalar kernels of
+// internal/vec/scalar.go): acc is the running value, b the binary ops'
+// second operand, k0 and k1 the immediates. Every operation is rounded
+// on its own (Affine's multiply and add are two roundings, no FMA).
+__device__ __forceinline__ float vec_step(int op, float acc, float b, float k0, float k1) {
+    switch (op) {
+    case STRATA_VEC_ADD: return add(acc, b);
+    case STRATA_VEC_SUB: return sub(acc, b);
+    case STRATA_VEC_MUL: return mul(acc, b);
+    case STRATA_VEC_DIV: return div(acc, b);
+    case STRATA_VEC_MIN: return go_min(acc, b);
+    case STRATA_VEC_MAX: return go_max(acc, b);
+    case STRATA_VEC_ADD_SCALAR: return add(acc, k0);
+    case STRATA_VEC_MUL_SCALAR: return mul(acc, k0);
+    case STRATA_VEC_AFFINE: return add(mul(acc, k0), k1);
+    case STRATA_VEC_SUB_DIV: return div(sub(acc, k0), k1);
+    case STRATA_VEC_CLAMP: return go_min(go_max(acc, k0), k1);
+    case STRATA_VEC_ABS: return abs32(acc);
+    default: return sqrt64of32(acc);  // STRATA_VEC_SQRT
+    }
 }
 
 }  // namespace cell

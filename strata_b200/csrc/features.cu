@@ -272,7 +272,7 @@ bool aligned16_(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) ==
 }  // namespace
 
 int feature_slot(const LaunchParams& p) {
-    if (p.nepi > 1 || (p.nepi == 1 && (p.epi[0].op != STRATA_OP_RECLASS || p.epi[0].n > kChainBreaks))) return -1;
+    if (p.nstep || p.nepi > 1 || (p.nepi == 1 && (p.epi[0].op != STRATA_OP_RECLASS || p.epi[0].n > kChainBreaks))) return -1;
     int q = -1;
     if (p.op == STRATA_OP_GRADIENT) q = kFGradient;
     else if (p.op == STRATA_OP_SLOPE && p.kind == kSlopeSquareClass) q = kFSlopeClass;

@@ -18,15 +18,49 @@ namespace {
 
 using namespace cell;
 
-// Pointwise stages alone (radius 0): every cell through the epilogue.
-__global__ void __launch_bounds__(256) pointwise_kernel(const __grid_constant__ LaunchParams P) {
+// Pointwise stages alone (radius 0): every cell through the epilogue, or,
+// for a tail of chain steps, through the steps with the binary ones
+// reading their input's cell (vec.Chain over its inputs, internal/vec/
+// chain.go:133-155 and scalar.go:180-228: the running value starts at
+// input 0 and is every step's first operand). A warp takes a run of 128
+// cells of one row, 4 a lane in 4 coalesced passes; each chunk of a row
+// costs one 64-bit division.
+constexpr int kPointChunk = 1024;
+
+__device__ __forceinline__ float chain_cell(const LaunchParams& P, float v, int64_t oy, int64_t ox) {
+#pragma unroll 1
+    for (int i = 0; i < P.nstep; i++) {
+        const ChainStep& s = P.step[i];
+        if (s.op >= kStepTable) {
+            v = table_stage(P.epi[s.op - kStepTable], v);
+        } else {
+            // input 0 is the launch's own source (its window, in a tile)
+            const float* in = s.src == 0 ? P.src : P.in[s.src];
+            const int64_t st = s.src == 0 ? P.src_stride : P.in_stride[s.src];
+            const float b = s.op <= STRATA_VEC_MAX ? in[oy * st + ox] : 0.0f;
+            v = vec_step(s.op, v, b, s.k0, s.k1);
+        }
+    }
+    return v;
+}
+
+__global__ void __launch_bounds__(256) pointwise_kernel(const __grid_constant__ LaunchParams P, int64_t chunks_x,
+                                                        int64_t chunks) {
     const int64_t w = P.out_x1 - P.out_x0;
-    const int64_t n = w * (P.out_y1 - P.out_y0);
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t y = i / w, x = i - y * w;
-        const int64_t gx = P.out_x0 + x, gy = P.out_y0 + y;
-        const float v = P.src[(gy - P.src_y0) * P.src_stride + (gx - P.src_x0)];
-        P.dst0[(gy - P.dst_y0) * P.dst0_stride + (gx - P.dst_x0)] = epilogue(P, v);
+    for (int64_t c = blockIdx.x; c < chunks; c += gridDim.x) {
+        const int64_t cy = c / chunks_x, cx = c - cy * chunks_x;
+        const int64_t gy = P.out_y0 + cy, oy = gy - P.src_y0;
+        const int64_t x0 = cx * kPointChunk;
+        const float* srow = P.src + oy * P.src_stride;
+        float* drow = P.dst0 + (gy - P.dst_y0) * P.dst0_stride;
+#pragma unroll
+        for (int k = 0; k < kPointChunk / 256; k++) {
+            const int64_t x = x0 + k * 256 + threadIdx.x;
+            if (x >= w) break;
+            const int64_t gx = P.out_x0 + x;
+            const float v = srow[gx - P.src_x0];
+            drow[gx - P.dst_x0] = P.nstep ? chain_cell(P, v, oy, gx - P.src_x0) : epilogue(P, v);
+        }
     }
 }
 
@@ -74,7 +108,7 @@ __global__ void __launch_bounds__(256) fit_finish_kernel(const __grid_constant__
                 break;
             }
         }
-        if (P.nepi) v0 = epilogue(P, v0);
+        if (has_tail(P)) v0 = epilogue(P, v0);
         P.dst0[(gy - P.dst_y0) * P.dst0_stride + (gx - P.dst_x0)] = v0;
         if (P.op == STRATA_OP_GRADIENT) P.dst1[(gy - P.dst_y0) * P.dst1_stride + (gx - P.dst_x0)] = v1;
     }
@@ -91,13 +125,17 @@ void launch_fit_finish(const LaunchParams& p, float* const d[5], int64_t ds, cud
 }
 
 int64_t launch_data(const LaunchParams& p, cudaStream_t s, int64_t* window_cells) {
-    if (p.op == STRATA_OP_LOOKUP || p.op == STRATA_OP_RECLASS) {
-        const int64_t n = (p.out_x1 - p.out_x0) * (p.out_y1 - p.out_y0);
-        int64_t blocks = (n + 255) / 256;
-        if (blocks > (int64_t)sm_count() * 64) blocks = (int64_t)sm_count() * 64;
-        if (blocks < 1) blocks = 1;
-        pointwise_kernel<<<(unsigned)blocks, 256, 0, s>>>(p);
-        if (window_cells) *window_cells = n;
+    if (p.op == STRATA_OP_LOOKUP || p.op == STRATA_OP_RECLASS || p.op == STRATA_OP_STEP) {
+        const int64_t w = p.out_x1 - p.out_x0, h = p.out_y1 - p.out_y0;
+        if (w <= 0 || h <= 0) {
+            if (window_cells) *window_cells = 0;
+            return 0;
+        }
+        const int64_t chunks_x = (w + kPointChunk - 1) / kPointChunk, chunks = chunks_x * h;
+        int64_t blocks = chunks;
+        if (blocks > (int64_t)sm_count() * 16) blocks = (int64_t)sm_count() * 16;
+        pointwise_kernel<<<(unsigned)blocks, 256, 0, s>>>(p, chunks_x, chunks);
+        if (window_cells) *window_cells = w * h * (p.ninputs > 1 ? p.ninputs : 1);
         return blocks;
     }
     if (p.fit || (!(p.op >= STRATA_OP_GRADIENT && p.op <= STRATA_OP_MAX) && p.op != STRATA_OP_HEATLOAD &&

@@ -44,6 +44,17 @@ struct EpiStage {
     float b[STRATA_MAX_KNOTS + 1];
 };
 
+// One step of a pointwise tail written as a sequence (LaunchParams.nstep
+// > 0): op is a STRATA_VEC_* (a vec.Chain step, internal/vec/chain.go:
+// 24-38), or kStepTable + i to run table stage epi[i]; src is the input a
+// binary op reads; k0, k1 the immediates.
+constexpr int kStepTable = 32;
+struct ChainStep {
+    int op;
+    int src;
+    float k0, k1;
+};
+
 // The output validity a radius-1 march writes beside its cells (n > 0):
 // the source mask (null: every source cell valid), whose cell (src_x0,
 // src_y0) of the launch is bit src_off, and each output's mask (null: the
@@ -96,7 +107,18 @@ struct alignas(16) LaunchParams {
                            // HEATLOAD the regression's eight float64 terms, bit for bit, in w[0..16)
     EpiStage epi[kMaxEpilogue];
     FusedValidity vf;  // set by launch_stage when the march writes the outputs' validity
+    // The pointwise tail as a sequence, when it holds a chain step: then
+    // step[0..nstep) runs in order (the table stages by reference) and
+    // nepi only counts the tables; 0: the tail is epi[0..nepi) in order.
+    int nstep;
+    int ninputs;  // the sources a pointwise chain reads: in[0] is src
+    ChainStep step[STRATA_MAX_STEPS];
+    const float* in[STRATA_MAX_INPUTS];  // cell (src_x0, src_y0) of each input
+    int64_t in_stride[STRATA_MAX_INPUTS];
 };
+
+// A pointwise tail to run after the stencil (tables or chain steps).
+__host__ __device__ inline bool has_tail(const LaunchParams& p) { return p.nepi > 0 || p.nstep > 0; }
 
 // The fused multi-output pass (features.cu): several radius-1 ops over one
 // source in one march, terrain.Features / terrain.Surface's outputs from
@@ -225,6 +247,23 @@ void launch_fit_finish(const LaunchParams& p, float* const d[5], int64_t ds, cud
 
 // Launches the validity kernel for one output.
 void launch_validity(const ValidityParams& v, cudaStream_t stream);
+
+// The validity of a pointwise pipeline over several inputs
+// (pointwise.BinaryValidity, and halo.go:213-229 at reach 0): bit (x, y)
+// of the output, for rows [y0, y1), is the AND of every masked input's bit
+// (x, y); an unmasked input counts as valid. The output's other bits are
+// kept. Input i's cell (0, 0) is bit src_off[i] of src_bits[i] (null:
+// unmasked).
+struct AndValidityParams {
+    const uint32_t* src_bits[STRATA_MAX_INPUTS];
+    int64_t src_off[STRATA_MAX_INPUTS];
+    int64_t src_stride[STRATA_MAX_INPUTS];
+    int nsrc;
+    uint32_t* dst_bits;
+    int64_t dst_off, dst_stride;
+    int64_t width, y0, y1;
+};
+void launch_and_validity(const AndValidityParams& v, cudaStream_t stream);
 
 // Launches a stage and the validity of its masked outputs (v[i] for output
 // i, null when output i is unmasked). The radius-1 march on 16-byte aligned

@@ -321,7 +321,7 @@ int64_t launch_march(const LaunchParams& p, cudaStream_t s) {
 
 template <int OP, int KIND>
 int64_t launch_epi(const LaunchParams& p, cudaStream_t s) {
-    return p.nepi ? launch_march<OP, KIND, true>(p, s) : launch_march<OP, KIND, false>(p, s);
+    return has_tail(p) ? launch_march<OP, KIND, true>(p, s) : launch_march<OP, KIND, false>(p, s);
 }
 
 // Rasters whose rows are not 16-byte aligned where the march loads and
@@ -360,7 +360,7 @@ int64_t launch_any(const LaunchParams& p, cudaStream_t s) {
 
 template <int OP, int KIND>
 int64_t launch_any_epi(const LaunchParams& p, cudaStream_t s) {
-    return p.nepi ? launch_any<OP, KIND, true>(p, s) : launch_any<OP, KIND, false>(p, s);
+    return has_tail(p) ? launch_any<OP, KIND, true>(p, s) : launch_any<OP, KIND, false>(p, s);
 }
 
 }  // namespace

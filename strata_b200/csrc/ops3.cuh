@@ -73,11 +73,23 @@ __device__ __forceinline__ void apply3(const LaunchParams& P, const float (&z)[9
 // The pointwise stages fused after a stencil (exec.Pipeline's staged
 // Lookup / Reclass tail, internal/exec/pipeline.go:539-574), reading their
 // tables from the launch parameters.
+// A tail holding chain steps (vec.Chain, internal/vec/chain.go) runs as
+// its step sequence, the tables by reference; the host admits only the
+// unary steps after a stencil.
+__device__ __forceinline__ float table_stage(const EpiStage& e, float v) {
+    return e.op == STRATA_OP_LOOKUP ? cell::lookup(v, e.a, e.b, e.n) : cell::reclass(v, e.a, e.n, e.b);
+}
+
 __device__ __forceinline__ float epilogue(const LaunchParams& P, float v) {
-    for (int i = 0; i < P.nepi; i++) {
-        const EpiStage& e = P.epi[i];
-        v = e.op == STRATA_OP_LOOKUP ? cell::lookup(v, e.a, e.b, e.n) : cell::reclass(v, e.a, e.n, e.b);
+    if (P.nstep) {
+#pragma unroll 1
+        for (int i = 0; i < P.nstep; i++) {
+            const ChainStep& s = P.step[i];
+            v = s.op >= kStepTable ? table_stage(P.epi[s.op - kStepTable], v) : cell::vec_step(s.op, v, 0.0f, s.k0, s.k1);
+        }
+        return v;
     }
+    for (int i = 0; i < P.nepi; i++) v = table_stage(P.epi[i], v);
     return v;
 }
 
@@ -175,6 +187,20 @@ __device__ __forceinline__ void reclass_chain4(const EpiStage& e, float (&v)[4])
 
 // The epilogue over four cells, stage by stage.
 __device__ __forceinline__ void epilogue4(const LaunchParams& P, const EpiTables& T, float (&v)[4]) {
+    if (P.nstep) {
+#pragma unroll 1
+        for (int i = 0; i < P.nstep; i++) {
+            const ChainStep s = P.step[i];
+            if (s.op >= kStepTable) {
+                const int t = s.op - kStepTable;
+                epi_stage4(P.epi[t], T.a[t], T.b[t], T.p2[t], v);
+            } else {
+#pragma unroll
+                for (int c = 0; c < 4; c++) v[c] = cell::vec_step(s.op, v[c], 0.0f, s.k0, s.k1);
+            }
+        }
+        return;
+    }
     if (P.nepi == 1 && P.epi[0].op == STRATA_OP_RECLASS && P.epi[0].n <= kChainBreaks) {
         reclass_chain4(P.epi[0], v);
         return;

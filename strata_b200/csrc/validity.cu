@@ -41,7 +41,66 @@ void launch_r(const ValidityParams& v, cudaStream_t s) {
     validity_march_kernel<R><<<(unsigned)blocks, kVThreads, 0, s>>>(v, (int)strips, (int)band);
 }
 
+// n (1..32) bits of a mask from bit q on, in the low bits.
+__device__ __forceinline__ uint32_t bits_at(const uint32_t* m, int64_t q, int n) {
+    const int64_t w = q >> 5;
+    const int sh = (int)(q & 31);
+    uint32_t v = m[w] >> sh;
+    if (sh && sh + n > 32) v |= m[w + 1] << (32 - sh);
+    return n == 32 ? v : v & ((1u << n) - 1u);
+}
+
+// One thread a 32-bit output word: its bits walk the rows they fall on
+// (a row's run, or the row padding and the cells outside [y0, y1) that
+// the word keeps), each run ANDed from the inputs' words with one funnel
+// shift. No two threads share a word, so the store needs no atomic.
+__global__ void __launch_bounds__(256) and_validity_kernel(const __grid_constant__ AndValidityParams v, int64_t w0,
+                                                           int64_t nwords) {
+    const int64_t S = v.dst_stride;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nwords; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t word = w0 + i;
+        const int64_t base = word * 32 - v.dst_off;  // the cell of the word's bit 0
+        uint32_t keep = 0, val = 0;
+        int b = 0;
+        while (b < 32) {
+            const int64_t c = base + b;
+            int n;
+            if (c < 0) {
+                n = (int)(-c < 32 - b ? -c : 32 - b);
+                keep |= (n == 32 ? ~0u : ((1u << n) - 1u)) << b;
+            } else {
+                const int64_t y = c / S, x = c - y * S;
+                if (y < v.y0 || y >= v.y1 || x >= v.width) {
+                    const int64_t run = S - x;
+                    n = (int)(run < 32 - b ? run : 32 - b);
+                    keep |= (n == 32 ? ~0u : ((1u << n) - 1u)) << b;
+                } else {
+                    const int64_t run = v.width - x;
+                    n = (int)(run < 32 - b ? run : 32 - b);
+                    uint32_t ok = n == 32 ? ~0u : ((1u << n) - 1u);
+                    for (int k = 0; k < v.nsrc; k++)
+                        if (v.src_bits[k]) ok &= bits_at(v.src_bits[k], v.src_off[k] + y * v.src_stride[k] + x, n);
+                    val |= ok << b;
+                }
+            }
+            b += n;
+        }
+        uint32_t* d = v.dst_bits + word;
+        *d = keep ? (*d & keep) | val : val;
+    }
+}
+
 }  // namespace
+
+void launch_and_validity(const AndValidityParams& v, cudaStream_t s) {
+    if (!v.dst_bits || v.y1 <= v.y0 || v.width <= 0) return;
+    const int64_t first = v.dst_off + v.y0 * v.dst_stride;
+    const int64_t last = v.dst_off + (v.y1 - 1) * v.dst_stride + v.width - 1;
+    const int64_t w0 = first >> 5, nwords = (last >> 5) - w0 + 1;
+    int64_t blocks = (nwords + 255) / 256;
+    if (blocks > (int64_t)sm_count() * 16) blocks = (int64_t)sm_count() * 16;
+    and_validity_kernel<<<(unsigned)blocks, 256, 0, s>>>(v, w0, nwords);
+}
 
 void launch_validity(const ValidityParams& v, cudaStream_t s) {
     if (v.dst_words <= 0 || v.out_x1 <= v.out_x0 || v.out_y1 <= v.out_y0) return;

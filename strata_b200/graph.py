@@ -3,9 +3,9 @@ run.go), for the chains the device runs as one pass.
 
 A Graph holds named inputs, nodes and named outputs. Plan lowers every
 output whose value is one stencil op (terrain or focal) over an input,
-followed by any number of pointwise Lookup / Reclass nodes, to one device
-pass: strata_process with the stencil stage first and the pointwise stages
-fused as its epilogue, as exec.Pipeline runs Slope -> Lookup -> Reclass
+followed by pointwise Lookup / Reclass / Rescale / RescaleRange / Clamp
+nodes, to one device pass: strata_process with the stencil stage first and
+the pointwise stages fused as its epilogue, as exec.Pipeline runs Slope -> Lookup -> Reclass
 (graph/run.go:390-486, internal/exec/pipeline.go:187). A pointwise chain
 straight over an input is a pass of its own. Anything else (two stencils
 in a row, binary ops, reductions) raises NotSupported, the cue for a
@@ -168,6 +168,24 @@ def Reclass(src: Node, breaks, values) -> Node:
     transfer.reclass_stage(breaks, values)
     breaks, values = list(breaks), list(values)
     return _pointwise("transfer.Reclass", src, lambda: transfer.reclass_stage(breaks, values))
+
+
+def Rescale(src: Node, a: float, b: float) -> Node:
+    """transfer.Rescale as a chain step (vec.OpAffine) of the pass."""
+    return _pointwise("transfer.Rescale", src, lambda: transfer.rescale_stage(a, b))
+
+
+def RescaleRange(src: Node, in_lo: float, in_hi: float, out_lo: float, out_hi: float) -> Node:
+    transfer.rescale_range_stage(in_lo, in_hi, out_lo, out_hi)
+    return _pointwise("transfer.RescaleRange", src,
+                      lambda: transfer.rescale_range_stage(in_lo, in_hi, out_lo, out_hi))
+
+
+def Clamp(src: Node, lo: float, hi: float) -> Node:
+    """algebra.Clamp as a chain step (vec.OpClamp) of the pass."""
+    from . import algebra
+
+    return _pointwise("algebra.Clamp", src, lambda: algebra.clamp_stage(lo, hi))
 
 
 class Plan:

@@ -1,4 +1,4 @@
-"""transfer: Lookup and Reclass (transfer/transfer.go:21-46, tiled.go) on
+"""transfer: Lookup, Reclass and Rescale (transfer/transfer.go:21-92, tiled.go) on
 the device backend, and the stage builders a pipeline fuses as its
 pointwise tail (see graph.py).
 """
@@ -60,3 +60,46 @@ def ReclassTiled(ctx: Context, dst, src, breaks, values, eopts: Options):
 
 def ReclassChunked(ctx: Context, dst, src, breaks, values, eopts: Options):
     return process_chunked(reclass_stage(breaks, values), [dst], [src], eopts, ctx)
+
+
+def rescale_stage(a: float, b: float) -> StageList:
+    """rescaleKernel's chain step (transfer/tiled.go:108-110): vec.OpAffine,
+    float32(v*a) + b with no FMA."""
+    st = _lib.Stage()
+    _lib.check(_lib.lib().strata_stage_rescale(a, b, ctypes.byref(st)))
+    return StageList().add(st)
+
+
+def rescale_range_stage(in_lo: float, in_hi: float, out_lo: float, out_hi: float) -> StageList:
+    """RescaleRange's coefficients (transfer/transfer.go:236-250), checked,
+    as the Affine step."""
+    st = _lib.Stage()
+    _lib.check(_lib.lib().strata_stage_rescale_range(in_lo, in_hi, out_lo, out_hi, ctypes.byref(st)))
+    return StageList().add(st)
+
+
+def Rescale(dst: Float32Raster, src: Float32Raster, a: float, b: float) -> None:
+    """transfer.Rescale: float32(v*a) + b cell by cell."""
+    process(rescale_stage(a, b), [dst], [src], Options(Workers=1))
+
+
+def RescaleTiled(ctx: Context, dst, src, a, b, eopts: Options):
+    return process(rescale_stage(a, b), [dst], [src], eopts, ctx)
+
+
+def RescaleChunked(ctx: Context, dst, src, a, b, eopts: Options):
+    return process_chunked(rescale_stage(a, b), [dst], [src], eopts, ctx)
+
+
+def RescaleRange(dst: Float32Raster, src: Float32Raster, in_lo, in_hi, out_lo, out_hi) -> None:
+    """transfer.RescaleRange: the affine map sending [in_lo, in_hi] to
+    [out_lo, out_hi] (no clamp)."""
+    process(rescale_range_stage(in_lo, in_hi, out_lo, out_hi), [dst], [src], Options(Workers=1))
+
+
+def RescaleRangeTiled(ctx: Context, dst, src, in_lo, in_hi, out_lo, out_hi, eopts: Options):
+    return process(rescale_range_stage(in_lo, in_hi, out_lo, out_hi), [dst], [src], eopts, ctx)
+
+
+def RescaleRangeChunked(ctx: Context, dst, src, in_lo, in_hi, out_lo, out_hi, eopts: Options):
+    return process_chunked(rescale_range_stage(in_lo, in_hi, out_lo, out_hi), [dst], [src], eopts, ctx)

@@ -79,12 +79,16 @@ def oracle_stage(st: _lib.Stage):
         tables.pop()
     if st.op == _lib.OP_CORRELATE and st.flags & _lib.STAGE_ROTATE180:
         tables[0] = tables[0][::-1].copy()
-    return orc.stage(st.op, st.radius, st.kind, list(st.k), tables, flags=st.flags & _lib.STAGE_FIT)
+    return orc.stage(st.op, st.radius, st.kind, list(st.k), tables, flags=st.flags & _lib.STAGE_FIT, input=st.input)
 
 
-def run_oracle(stages, src: Float32Raster, dsts, nthreads=1):
-    """Runs the oracle for a product StageList into host rasters dsts."""
+def run_oracle(stages, src, dsts, nthreads=1):
+    """Runs the oracle for a product StageList into host rasters dsts; src
+    is one raster, or a list of them for a pointwise chain."""
     ost = [oracle_stage(s) for s in stages.stages]
+    if isinstance(src, (list, tuple)):
+        orc.process_n(ost, [_orc_dict(x) for x in src], [_orc_dict(d) for d in dsts], nthreads)
+        return
     orc.process(ost, _orc_dict(src), [_orc_dict(d) for d in dsts], nthreads)
 
 

@@ -16,7 +16,7 @@ import numpy as np
 import pytest
 
 from oracle import oracle as orc
-from strata_b200 import _lib, focal, terrain, transfer
+from strata_b200 import _lib, focal, terrain, transfer, vec
 from strata_b200.raster import NotSupported, StrataPanic
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -41,7 +41,7 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_abi_version():
-    assert _lib.lib().strata_abi_version() == 1
+    assert _lib.lib().strata_abi_version() == 2
 
 
 def test_op_codes_match_oracle_and_header():
@@ -174,6 +174,15 @@ def test_ruggedness_radius_default():
      "transfer.Reclass: values must hold one more element than breaks, got 2 values and 2 breaks"),
     (lambda: transfer.reclass_stage([1, float("nan")], [1, 2, 3]),
      "transfer.Reclass: breaks must not hold NaN, but breaks[1] is NaN"),
+    (lambda: transfer.rescale_range_stage(1, 1, 0, 1),
+     "transfer.RescaleRange: inLo and inHi must be finite and different, got 1 and 1"),
+    (lambda: transfer.rescale_range_stage(0, 1, float("inf"), 1),
+     "transfer.RescaleRange: outLo and outHi must be finite, got +Inf and 1"),
+    (lambda: transfer.rescale_range_stage(0, 1e-30, -3e38, 3e38),
+     "transfer.RescaleRange: [0, 1e-30] to [-3e+38, 3e+38] gives a scale of +Inf"),
+    (lambda: vec.step_stage(13), "vec: chain step has unknown operation Op(13)"),
+    (lambda: vec.step_stage(vec.OpMin, -1), "vec: chain step (Min) reads input -1, which is not one of its 4"),
+    (lambda: vec.step_stage(vec.OpClamp, 1, 0, 1), "vec: chain step (Clamp) reads no input, so its Src must be -1, not 1"),
 ])
 def test_builders_panic_like_the_reference(make, msg):
     with pytest.raises(StrataPanic) as e:
@@ -247,3 +256,18 @@ def test_context_without_a_device_fails_cleanly():
     rc = _lib.lib().strata_ctx_create(0, ctypes.byref(p))
     assert rc in (_lib.ECUDA, _lib.EINVAL)
     assert _lib.last_error()
+
+
+@pytest.mark.parametrize("lo,hi,olo,ohi", [(0, 10, 100, 200), (-3, 7, 10, 0), (0.1, 0.7, -1, 1), (1e-3, 2e5, 0, 255)])
+def test_rescale_range_coefficients_as_the_oracle(lo, hi, olo, ohi):
+    st = transfer.rescale_range_stage(lo, hi, olo, ohi).stages[0]
+    a, b = orc.rescale_range_coeffs(lo, hi, olo, ohi)
+    assert st.op == _lib.OP_STEP and st.kind == vec.OpAffine and st.input == -1
+    assert np.float32(st.k[0]) == a and np.float32(st.k[1]) == b
+
+
+def test_step_stage_fields():
+    st = vec.step_stage(vec.OpSub, 3).stages[0]
+    assert (st.op, st.kind, st.input) == (_lib.OP_STEP, vec.OpSub, 3)
+    st = transfer.rescale_stage(2.5, -1).stages[0]
+    assert (st.kind, st.input, st.k[0], st.k[1]) == (vec.OpAffine, -1, 2.5, -1.0)
