@@ -282,6 +282,38 @@ int strata_process_chunked(strata_ctx *ctx, const strata_stage *stages, int nsta
                            const strata_exec_opts *opts, strata_stats *stats);
 
 /*
+ * engine.RawSource / RawSink with RawOptions (engine/raw.go:15-191): a
+ * raster of width x height little-endian float32 cells in row-major order
+ * at byte offset `offset` of the open file fd (read with pread and written
+ * with pwrite, so the descriptor's position is not used; a write past the
+ * end extends the file). has_fill declares fill the file's NoData value:
+ * reading marks a cell invalid when it equals fill (by ==, so -0 matches
+ * 0), or, for a NaN fill, when it is any NaN; writing stores fill under
+ * invalid cells. The source or sink is then Masked.
+ */
+typedef struct {
+    int32_t fd;
+    int32_t has_fill;
+    float fill;
+    int32_t reserved;
+    int64_t width, height;
+    int64_t offset;
+} strata_raw_file;
+
+/*
+ * strata_process_chunked over raw files: the same tiles and results, each
+ * tile read with pread straight into page-locked memory (a full-width
+ * tile in one call), its validity taken from the fill value on the
+ * device, the fill stored under the invalid output cells on the device,
+ * and the tile written with pwrite. Read and write failures return
+ * STRATA_EIO with the rows in the message, as RawSource / RawSink word
+ * theirs.
+ */
+int strata_process_raw(strata_ctx *ctx, const strata_stage *stages, int nstages, const strata_raw_file *src,
+                       int nsrc, const strata_raw_file *dst, int ndst, const strata_exec_opts *opts,
+                       strata_stats *stats);
+
+/*
  * Batches (the batched form of the path; no counterpart call in strata,
  * whose plain functions take one raster each): many device-resident
  * rasters of mixed sizes and ops, each item one pipeline (stages as in

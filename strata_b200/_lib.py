@@ -61,6 +61,11 @@ READ_FN = ctypes.CFUNCTYPE(ctypes.c_int, c_p, ctypes.POINTER(Raster), c_i64, c_i
 WRITE_FN = ctypes.CFUNCTYPE(ctypes.c_int, c_p, ctypes.POINTER(Raster), c_i64, c_i64)
 
 
+class RawFile(ctypes.Structure):
+    _fields_ = [("fd", c_i32), ("has_fill", c_i32), ("fill", c_f32), ("reserved", c_i32), ("width", c_i64),
+                ("height", c_i64), ("offset", c_i64)]
+
+
 class Source(ctypes.Structure):
     _fields_ = [("width", c_i64), ("height", c_i64), ("masked", c_i32), ("reserved", c_i32),
                 ("user", c_p), ("read", READ_FN)]
@@ -177,6 +182,9 @@ SIGNATURES = [
     ("strata_process_features", ctypes.c_int, [c_p, ctypes.POINTER(Stage), ctypes.POINTER(c_i32), ctypes.c_int,
                                                ctypes.POINTER(Raster), ctypes.POINTER(Raster), ctypes.c_int,
                                                ctypes.POINTER(ExecOpts), ctypes.POINTER(Stats)]),
+    ("strata_process_raw", ctypes.c_int, [c_p, ctypes.POINTER(Stage), ctypes.c_int, ctypes.POINTER(RawFile),
+                                           ctypes.c_int, ctypes.POINTER(RawFile), ctypes.c_int,
+                                           ctypes.POINTER(ExecOpts), ctypes.POINTER(Stats)]),
     ("strata_process_chunked", ctypes.c_int, [c_p, ctypes.POINTER(Stage), ctypes.c_int, ctypes.POINTER(Source),
                                               ctypes.c_int, ctypes.POINTER(Sink), ctypes.c_int,
                                               ctypes.POINTER(ExecOpts), ctypes.POINTER(Stats)]),

@@ -7,11 +7,15 @@
 // transfer packages do.
 #include <cuda_runtime.h>
 
+#include <unistd.h>
+
+#include <cerrno>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <algorithm>
 #include <cstring>
+#include <functional>
 #include <limits>
 #include <memory>
 #include <mutex>
@@ -1706,48 +1710,42 @@ struct TileSet {
     bool pending = false;
 };
 
-}  // namespace
+// Where a chunked call's tiles come from and go to: the caller's callbacks
+// (engine.RasterSource / RasterSink), or raw float32 files whose fill
+// value becomes validity on the device (engine/raw.go).
+struct ChunkIO {
+    bool in_masked = false;  // the input tiles carry validity
+    bool in_fill = false;    // ... derived on the device from in_fill_value
+    float in_fill_value = 0;
+    bool compact = false;  // tile rows at the tile's width (else masked rows start on 64-cell boundaries)
+    // Fills the host tile buf (its cells, and its bits when the input is
+    // masked and not derived) from the window at (x, y).
+    std::function<int(const strata_raster& buf, int64_t x, int64_t y)> read;
+    bool out_masked[2] = {false, false};  // output i's tiles carry validity
+    bool out_fill[2] = {false, false};    // ... and take out_fill_value[i] under their invalid cells
+    float out_fill_value[2] = {0, 0};
+    // Takes output i's finished host tile (bits only for an output that is
+    // masked and not filled).
+    std::function<int(int i, const strata_raster& buf, int64_t x, int64_t y)> write;
+};
 
-extern "C" int strata_process_chunked(strata_ctx* c, const strata_stage* stages, int nstages,
-                                      const strata_source* src, int nsrc, const strata_sink* dst, int ndst,
-                                      const strata_exec_opts* opts, strata_stats* stats) {
-    if (!c) return fail(STRATA_EINVAL, "engine: nil context");
-    LaunchParams p;
-    int nout = 0;
-    int rc = plan_stages(stages, nstages, p, &nout);
-    if (rc) return rc;
-    if (p.fit) return fail(STRATA_ENOTSUP, "engine: Wood's fit (FitRadius > 0) has no chunked form on the gpu backend");
-    if (p.ninputs > 1 || nsrc > 1)
-        return fail(STRATA_ENOTSUP, "engine: a chain over several inputs has no chunked form on the gpu backend");
-    if ((rc = check_opts(opts))) return rc;
-    if (nsrc != 1 || ndst != nout || !src || !dst)
-        return fail(STRATA_EINVAL, "engine: kernel takes 1 inputs and %d outputs, got %d and %d", nout, nsrc, ndst);
-    for (int i = 0; i < ndst; i++)
-        if (!dst[i].write) return fail(STRATA_EINVAL, "engine: dst[%d] is a nil sink", i);
-    if (!src[0].read) return fail(STRATA_EINVAL, "engine: src[0] is a nil source");
-    const int64_t W = dst[0].width, H = dst[0].height;
-    if (W <= 0 || H <= 0)
-        return fail(STRATA_EINVAL, "engine: dst[0] is %lld×%lld; sizes must be positive", (long long)W, (long long)H);
-    if (src[0].width != W || src[0].height != H)
-        return fail(STRATA_EINVAL, "engine: src[0] is %lld×%lld, dst[0] is %lld×%lld", (long long)src[0].width,
-                    (long long)src[0].height, (long long)W, (long long)H);
-    for (int i = 0; i < ndst; i++) {
-        if (dst[i].width != W || dst[i].height != H)
-            return fail(STRATA_EINVAL, "engine: dst[%d] is %lld×%lld, dst[0] is %lld×%lld", i, (long long)dst[i].width,
-                        (long long)dst[i].height, (long long)W, (long long)H);
-        if (src[0].masked && !dst[i].masked)
-            return fail(STRATA_EINVAL, "engine: a source is Masked but dst[%d] is not; its validity would be lost", i);
-    }
-
+// exec.ProcessChunked's tile loop (internal/exec/chunked.go:33-464) over
+// two buffer sets: tile t reads with its halo, crosses to the device and
+// computes while tile t - 1 goes to the sinks. p is planned for one input.
+int run_chunked(strata_ctx* c, const LaunchParams& p, int nout, int64_t W, int64_t H, const ChunkIO& io,
+                const strata_exec_opts* opts, strata_stats* stats) {
+    const int ndst = nout;
     const int r = p.radius;
     const int64_t tw = (opts && opts->tile_width > 0) ? std::min<int64_t>(opts->tile_width, W) : W;
     const int64_t th = (opts && opts->tile_height > 0) ? std::min<int64_t>(opts->tile_height, H) : H;
     const int64_t tiles_x = (W + tw - 1) / tw;
     const int64_t ntiles = tiles_x * ((H + th - 1) / th);
     const int64_t inW = std::min(W, tw + 2 * r), inH = std::min(H, th + 2 * r);
-    const bool in_masked = src[0].masked != 0;
-    const int64_t in_stride = in_masked ? round_up64(inW) : inW;
+    const bool in_masked = io.in_masked;
+    const bool host_in_bits = in_masked && !io.in_fill;
+    const int64_t in_stride = in_masked && !io.compact ? round_up64(inW) : inW;
     const int64_t in_cells = (inH - 1) * in_stride + inW;
+    int rc;
 
     std::lock_guard<std::mutex> lock(c->mu);
     DeviceGuard device_guard(c->device);
@@ -1758,16 +1756,18 @@ extern "C" int strata_process_chunked(strata_ctx* c, const strata_stage* stages,
         if ((rc = s.in_data.get((size_t)in_cells * 4)) || (rc = s.d_in_data.get((size_t)in_cells * 4))) return rc;
         if (in_masked) {
             size_t words = (size_t)((in_cells + 63) / 64);
-            if ((rc = s.in_bits.get(words * 8)) || (rc = s.d_in_bits.get(words * 8))) return rc;
+            if ((rc = s.d_in_bits.get(words * 8))) return rc;
+            if (host_in_bits && (rc = s.in_bits.get(words * 8))) return rc;
         }
         for (int i = 0; i < ndst; i++) {
-            int64_t os = dst[i].masked ? round_up64(tw) : tw;
+            int64_t os = io.out_masked[i] && !io.compact ? round_up64(tw) : tw;
             int64_t oc = (th - 1) * os + tw;
             s.out_stride[i] = os;
             if ((rc = s.out_data[i].get((size_t)oc * 4)) || (rc = s.d_out_data[i].get((size_t)oc * 4))) return rc;
-            if (dst[i].masked) {
+            if (io.out_masked[i]) {
                 size_t words = (size_t)((oc + 63) / 64);
-                if ((rc = s.out_bits[i].get(words * 8)) || (rc = s.d_out_bits[i].get(words * 8))) return rc;
+                if ((rc = s.d_out_bits[i].get(words * 8))) return rc;
+                if (!io.out_fill[i] && (rc = s.out_bits[i].get(words * 8))) return rc;
             }
         }
         if (cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming) != cudaSuccess)
@@ -1795,10 +1795,8 @@ extern "C" int strata_process_chunked(strata_ctx* c, const strata_stage* stages,
             b.width = s.x1 - s.x0;
             b.height = s.y1 - s.y0;
             b.stride = s.out_stride[i];
-            b.valid = dst[i].masked ? (uint64_t*)s.out_bits[i].p : nullptr;
-            if (dst[i].write(dst[i].user, &b, s.x0, s.y0) != 0)
-                return fail(STRATA_EIO, "engine: writing dst[%d] at (%lld, %lld) failed", i, (long long)s.x0,
-                            (long long)s.y0);
+            b.valid = io.out_masked[i] && !io.out_fill[i] ? (uint64_t*)s.out_bits[i].p : nullptr;
+            if ((rc = io.write(i, b, s.x0, s.y0)) != STRATA_OK) return rc;
         }
         int64_t cells = (s.x1 - s.x0) * (s.y1 - s.y0);
         local.sink_written += cells * 4 * ndst;
@@ -1824,26 +1822,26 @@ extern "C" int strata_process_chunked(strata_ctx* c, const strata_stage* stages,
         const int64_t rx0 = std::max<int64_t>(0, x0 - r), ry0 = std::max<int64_t>(0, y0 - r);
         const int64_t rx1 = std::min(W, x1 + r), ry1 = std::min(H, y1 + r);
         const int64_t ww = rx1 - rx0, wh = ry1 - ry0;
-        const int64_t ws = in_masked ? round_up64(ww) : ww;
+        const int64_t ws = in_masked && !io.compact ? round_up64(ww) : ww;
+        const int64_t wcells = (wh - 1) * ws + ww;
         strata_raster b = {};
         b.data = (float*)s.in_data.p;
         b.width = ww;
         b.height = wh;
         b.stride = ws;
-        b.valid = in_masked ? (uint64_t*)s.in_bits.p : nullptr;
-        if (in_masked) memset(s.in_bits.p, 0, (size_t)(((wh - 1) * ws + ww + 63) / 64) * 8);
-        if (src[0].read(src[0].user, &b, rx0, ry0) != 0) {
-            status = fail(STRATA_EIO, "engine: reading src[0] at (%lld, %lld) failed", (long long)rx0, (long long)ry0);
-            break;
-        }
+        b.valid = host_in_bits ? (uint64_t*)s.in_bits.p : nullptr;
+        if (host_in_bits) memset(s.in_bits.p, 0, (size_t)((wcells + 63) / 64) * 8);
+        if ((status = io.read(b, rx0, ry0)) != STRATA_OK) break;
         local.source_read += ww * wh * 4;
-        const int64_t wcells = (wh - 1) * ws + ww;
         cudaError_t e = cudaMemcpyAsync(s.d_in_data.p, s.in_data.p, (size_t)wcells * 4, cudaMemcpyHostToDevice, st);
-        if (e == cudaSuccess && in_masked)
+        if (e == cudaSuccess && host_in_bits)
             e = cudaMemcpyAsync(s.d_in_bits.p, s.in_bits.p, (size_t)((wcells + 63) / 64) * 8, cudaMemcpyHostToDevice,
                                 st);
+        if (e == cudaSuccess && in_masked && io.in_fill)
+            strata::launch_fill_bits((const float*)s.d_in_data.p, wcells, io.in_fill_value, (uint32_t*)s.d_in_bits.p,
+                                     st);
         for (int i = 0; i < ndst && e == cudaSuccess; i++)
-            if (dst[i].masked) {
+            if (io.out_masked[i]) {
                 int64_t oc = (y1 - y0 - 1) * s.out_stride[i] + (x1 - x0);
                 e = cudaMemsetAsync(s.d_out_bits[i].p, 0, (size_t)((oc + 63) / 64) * 8, st);
             }
@@ -1877,7 +1875,7 @@ extern "C" int strata_process_chunked(strata_ctx* c, const strata_stage* stages,
         ValidityParams vp[2];
         const ValidityParams* vs[2] = {nullptr, nullptr};
         for (int i = 0; i < ndst; i++) {
-            if (!dst[i].masked) continue;
+            if (!io.out_masked[i]) continue;
             ValidityParams& v = vp[i];
             vs[i] = &v;
             memset(&v, 0, sizeof v);
@@ -1913,10 +1911,14 @@ extern "C" int strata_process_chunked(strata_ctx* c, const strata_stage* stages,
         }
         local.bands += nt;
         local.kernel_read += wc * 4;
+        for (int i = 0; i < ndst; i++)
+            if (io.out_fill[i])
+                strata::launch_fill_invalid((float*)s.d_out_data[i].p, s.out_stride[i], x1 - x0, y1 - y0,
+                                            (const uint32_t*)s.d_out_bits[i].p, io.out_fill_value[i], st);
         for (int i = 0; i < ndst && e == cudaSuccess; i++) {
             int64_t oc = (y1 - y0 - 1) * s.out_stride[i] + (x1 - x0);
             e = cudaMemcpyAsync(s.out_data[i].p, s.d_out_data[i].p, (size_t)oc * 4, cudaMemcpyDeviceToHost, st);
-            if (e == cudaSuccess && dst[i].masked)
+            if (e == cudaSuccess && io.out_masked[i] && !io.out_fill[i])
                 e = cudaMemcpyAsync(s.out_bits[i].p, s.d_out_bits[i].p, (size_t)((oc + 63) / 64) * 8,
                                     cudaMemcpyDeviceToHost, st);
         }
@@ -1965,6 +1967,155 @@ extern "C" int strata_process_chunked(strata_ctx* c, const strata_stage* stages,
     if (status == STRATA_OK) status = take_status(c, st);
     if (status == STRATA_ECANCELED) return fail(STRATA_ECANCELED, "context canceled");
     return status;
+}
+
+// Reads or writes n bytes at off of fd, retrying short transfers; returns
+// the bytes moved (less than n at the end of the file or on an error, with
+// errno set for an error).
+int64_t raw_io(bool write, int fd, char* p, int64_t n, int64_t off) {
+    int64_t done = 0;
+    while (done < n) {
+        const size_t k = (size_t)std::min<int64_t>(n - done, (int64_t)1 << 30);
+        const ssize_t got = write ? pwrite(fd, p + done, k, (off_t)(off + done)) : pread(fd, p + done, k, (off_t)(off + done));
+        if (got < 0 && errno == EINTR) continue;
+        if (got <= 0) {
+            if (got == 0) errno = 0;
+            break;
+        }
+        done += got;
+    }
+    return done;
+}
+
+std::string rows_name(int64_t y, int64_t k) {
+    char b[64];
+    if (k == 1) snprintf(b, sizeof b, "row %lld", (long long)y);
+    else snprintf(b, sizeof b, "rows %lld to %lld", (long long)y, (long long)(y + k - 1));
+    return b;
+}
+
+// The rows of tile buf at (x, y) of a raw file: one call for rows that are
+// consecutive both in the file and in buf (a window as wide as the file
+// into a buffer without row padding), else a call per row
+// (engine/raw.go:74-111, 195-239).
+int raw_rows(bool write, const strata_raw_file& f, const strata_raster& buf, int64_t x, int64_t y) {
+    const bool whole = buf.width == f.width && buf.stride == buf.width;
+    const int64_t per = whole ? buf.height : 1;
+    for (int64_t row = 0; row < buf.height; row += per) {
+        const int64_t k = std::min(per, buf.height - row);
+        const int64_t n = ((k - 1) * buf.stride + buf.width) * 4;
+        const int64_t off = f.offset + 4 * ((y + row) * f.width + x);
+        const int64_t got = raw_io(write, f.fd, (char*)(buf.data + row * buf.stride), n, off);
+        if (got < n) {
+            const int err = errno;
+            if (write)
+                return fail(STRATA_EIO, "engine: raw sink: writing %s: %s", rows_name(y + row, k).c_str(),
+                            err ? strerror(err) : "short write");
+            return fail(STRATA_EIO, "engine: raw source: reading %s: %s", rows_name(y + row, k).c_str(),
+                        err ? strerror(err) : "unexpected EOF");
+        }
+    }
+    return STRATA_OK;
+}
+
+// NewRawSource / NewRawSink's checks (engine/raw.go:278-289).
+int check_raw(const char* fn, const strata_raw_file& f) {
+    if (f.fd < 0) return fail(STRATA_EINVAL, "engine: %s: nil file", fn);
+    if (f.width <= 0 || f.height <= 0)
+        return fail(STRATA_EINVAL, "engine: %s: dimensions must be positive, got %lld×%lld", fn, (long long)f.width,
+                    (long long)f.height);
+    if ((uint64_t)f.width > (uint64_t)INT64_MAX / 4 / (uint64_t)f.height)
+        return fail(STRATA_EINVAL, "engine: %s: %lld×%lld cells do not fit in a file", fn, (long long)f.width,
+                    (long long)f.height);
+    if (f.offset < 0) return fail(STRATA_EINVAL, "engine: %s: negative offset %lld", fn, (long long)f.offset);
+    return STRATA_OK;
+}
+
+static_assert(__BYTE_ORDER__ == __ORDER_LITTLE_ENDIAN__, "raw files are read in place: a little-endian host");
+
+}  // namespace
+
+extern "C" int strata_process_chunked(strata_ctx* c, const strata_stage* stages, int nstages,
+                                      const strata_source* src, int nsrc, const strata_sink* dst, int ndst,
+                                      const strata_exec_opts* opts, strata_stats* stats) {
+    if (!c) return fail(STRATA_EINVAL, "engine: nil context");
+    LaunchParams p;
+    int nout = 0;
+    int rc = plan_stages(stages, nstages, p, &nout);
+    if (rc) return rc;
+    if (p.fit) return fail(STRATA_ENOTSUP, "engine: Wood's fit (FitRadius > 0) has no chunked form on the gpu backend");
+    if (p.ninputs > 1 || nsrc > 1)
+        return fail(STRATA_ENOTSUP, "engine: a chain over several inputs has no chunked form on the gpu backend");
+    if ((rc = check_opts(opts))) return rc;
+    if (nsrc != 1 || ndst != nout || !src || !dst)
+        return fail(STRATA_EINVAL, "engine: kernel takes 1 inputs and %d outputs, got %d and %d", nout, nsrc, ndst);
+    for (int i = 0; i < ndst; i++)
+        if (!dst[i].write) return fail(STRATA_EINVAL, "engine: dst[%d] is a nil sink", i);
+    if (!src[0].read) return fail(STRATA_EINVAL, "engine: src[0] is a nil source");
+    const int64_t W = dst[0].width, H = dst[0].height;
+    if (W <= 0 || H <= 0)
+        return fail(STRATA_EINVAL, "engine: dst[0] is %lld×%lld; sizes must be positive", (long long)W, (long long)H);
+    if (src[0].width != W || src[0].height != H)
+        return fail(STRATA_EINVAL, "engine: src[0] is %lld×%lld, dst[0] is %lld×%lld", (long long)src[0].width,
+                    (long long)src[0].height, (long long)W, (long long)H);
+    for (int i = 0; i < ndst; i++) {
+        if (dst[i].width != W || dst[i].height != H)
+            return fail(STRATA_EINVAL, "engine: dst[%d] is %lld×%lld, dst[0] is %lld×%lld", i, (long long)dst[i].width,
+                        (long long)dst[i].height, (long long)W, (long long)H);
+        if (src[0].masked && !dst[i].masked)
+            return fail(STRATA_EINVAL, "engine: a source is Masked but dst[%d] is not; its validity would be lost", i);
+    }
+    ChunkIO io;
+    io.in_masked = src[0].masked != 0;
+    io.read = [&](const strata_raster& b, int64_t x, int64_t y) -> int {
+        if (src[0].read(src[0].user, &b, x, y) != 0)
+            return fail(STRATA_EIO, "engine: reading src[0] at (%lld, %lld) failed", (long long)x, (long long)y);
+        return STRATA_OK;
+    };
+    for (int i = 0; i < ndst; i++) io.out_masked[i] = dst[i].masked != 0;
+    io.write = [&](int i, const strata_raster& b, int64_t x, int64_t y) -> int {
+        if (dst[i].write(dst[i].user, &b, x, y) != 0)
+            return fail(STRATA_EIO, "engine: writing dst[%d] at (%lld, %lld) failed", i, (long long)x, (long long)y);
+        return STRATA_OK;
+    };
+    return run_chunked(c, p, nout, W, H, io, opts, stats);
+}
+
+extern "C" int strata_process_raw(strata_ctx* c, const strata_stage* stages, int nstages, const strata_raw_file* src,
+                                  int nsrc, const strata_raw_file* dst, int ndst, const strata_exec_opts* opts,
+                                  strata_stats* stats) {
+    if (!c) return fail(STRATA_EINVAL, "engine: nil context");
+    LaunchParams p;
+    int nout = 0;
+    int rc = plan_stages(stages, nstages, p, &nout);
+    if (rc) return rc;
+    if (p.fit) return fail(STRATA_ENOTSUP, "engine: Wood's fit (FitRadius > 0) has no chunked form on the gpu backend");
+    if (p.ninputs > 1 || nsrc > 1)
+        return fail(STRATA_ENOTSUP, "engine: a chain over several inputs has no chunked form on the gpu backend");
+    if ((rc = check_opts(opts))) return rc;
+    if (nsrc != 1 || ndst != nout || !src || !dst)
+        return fail(STRATA_EINVAL, "engine: kernel takes 1 inputs and %d outputs, got %d and %d", nout, nsrc, ndst);
+    if ((rc = check_raw("NewRawSource", src[0]))) return rc;
+    const int64_t W = src[0].width, H = src[0].height;
+    for (int i = 0; i < ndst; i++) {
+        if ((rc = check_raw("NewRawSink", dst[i]))) return rc;
+        if (dst[i].width != W || dst[i].height != H)
+            return fail(STRATA_EINVAL, "engine: dst[%d] is %lld×%lld, src[0] is %lld×%lld", i, (long long)dst[i].width,
+                        (long long)dst[i].height, (long long)W, (long long)H);
+        if (src[0].has_fill && !dst[i].has_fill)
+            return fail(STRATA_EINVAL, "engine: a source is Masked but dst[%d] is not; its validity would be lost", i);
+    }
+    ChunkIO io;
+    io.compact = true;
+    io.in_masked = io.in_fill = src[0].has_fill != 0;
+    io.in_fill_value = src[0].fill;
+    io.read = [&](const strata_raster& b, int64_t x, int64_t y) { return raw_rows(false, src[0], b, x, y); };
+    for (int i = 0; i < ndst; i++) {
+        io.out_masked[i] = io.out_fill[i] = dst[i].has_fill != 0;
+        io.out_fill_value[i] = dst[i].fill;
+    }
+    io.write = [&](int i, const strata_raster& b, int64_t x, int64_t y) { return raw_rows(true, dst[i], b, x, y); };
+    return run_chunked(c, p, nout, W, H, io, opts, stats);
 }
 
 // ---------------------------------------------------------------------------

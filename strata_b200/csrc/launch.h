@@ -265,6 +265,15 @@ struct AndValidityParams {
 };
 void launch_and_validity(const AndValidityParams& v, cudaStream_t stream);
 
+// A raw file's fill value as validity (raw.cu): bits[k] holds the
+// validity of cells [32k, 32k + 32) of the run cells[0, n) (a cell equal
+// to fill, or any NaN for a NaN fill, is invalid; bits past n are 0); and
+// fill stored under the invalid cells of a w x h tile whose cell (x, y) is
+// data[y * stride + x] with its bit at the same index of bits.
+void launch_fill_bits(const float* cells, int64_t n, float fill, uint32_t* bits, cudaStream_t stream);
+void launch_fill_invalid(float* data, int64_t stride, int64_t w, int64_t h, const uint32_t* bits, float fill,
+                         cudaStream_t stream);
+
 // Launches a stage and the validity of its masked outputs (v[i] for output
 // i, null when output i is unmasked). The radius-1 march on 16-byte aligned
 // rows writes the validity itself when every v[i] describes the launch's

@@ -357,7 +357,10 @@ def _buffer_view(b: _lib.Raster) -> Float32Raster:
 def process_chunked(stages: StageList, dst: Sequence[RasterSink], src: Sequence[RasterSource],
                     opts: Optional[Options] = None, ctx: Optional[Context] = None):
     """exec.ProcessChunked on the device. Returns None, Canceled, or the
-    first source / sink error (a SourceSinkError wrapping it)."""
+    first source / sink error (a SourceSinkError wrapping it). With raw
+    files on every side it runs process_raw."""
+    if src and dst and all(isinstance(s, RawSource) for s in src) and all(isinstance(d, RawSink) for d in dst):
+        return process_raw(stages, dst, src, opts, ctx)
     dev = opts.Device if opts is not None else 0
     c = device_context(dev)
     errors: list = []
@@ -414,5 +417,146 @@ def process_chunked(stages: StageList, dst: Sequence[RasterSink], src: Sequence[
         return Canceled("context canceled")
     if rc == _lib.EIO:
         return errors[0] if errors else SourceSinkError(_lib.last_error())
+    _lib.check(rc)
+    return None
+
+
+# ---------------------------------------------------------------------------
+# Raw float32 files (engine/raw.go): little-endian cells, row-major, no
+# header, at a byte offset of an open file. A chunked call whose sources
+# and sinks are all raw files runs strata_process_raw: the tiles are read
+# with pread into page-locked memory, their validity is taken from the fill
+# value on the device, the fill goes under the invalid output cells on the
+# device, and the tiles are written with pwrite. Mixed with other sources
+# or sinks, the raw ones serve windows through ReadWindow / WriteWindow
+# on the host (the same bits).
+
+@dataclass
+class RawOptions:
+    """engine.RawOptions: Fill is the file's NoData value when HasFill."""
+    Fill: float = 0.0
+    HasFill: bool = False
+
+
+def _raw_size_check(fn: str, f, width: int, height: int) -> None:
+    if f is None:
+        raise StrataPanic(f"engine: {fn}: nil file")
+    if width <= 0 or height <= 0:
+        raise StrataPanic(f"engine: {fn}: dimensions must be positive, got {width}×{height}")
+    if width > ((1 << 63) - 1) // 4 // height:
+        raise StrataPanic(f"engine: {fn}: {width}×{height} cells do not fit in a file")
+
+
+def _fd(f) -> int:
+    return f if isinstance(f, int) else f.fileno()
+
+
+def _rows(r: Float32Raster, width: int):
+    """(first row, rows) groups of r one call moves: all rows at once when
+    they are consecutive in the file and in r, else one a call."""
+    per = r.height if (r.width == width and r.stride == r.width) else 1
+    for row in range(0, r.height, per):
+        yield row, min(per, r.height - row)
+
+
+def _rows_name(y: int, k: int) -> str:
+    return f"row {y}" if k == 1 else f"rows {y} to {y + k - 1}"
+
+
+class RawSource(RasterSource):
+    """engine.RawSource: a width×height raw float32 raster read from f (an
+    open binary file or a descriptor) at byte offset offset."""
+
+    def __init__(self, f, width: int, height: int, opts: RawOptions = RawOptions(), offset: int = 0):
+        _raw_size_check("NewRawSource", f, width, height)
+        self.f, self.w, self.h, self.opts, self.offset = f, width, height, opts, offset
+
+    def Size(self):
+        return self.w, self.h
+
+    def Masked(self) -> bool:
+        return bool(self.opts.HasFill)
+
+    def ReadWindow(self, dst: Float32Raster, x: int, y: int):
+        import os
+
+        if self.opts.HasFill and dst.valid is None:
+            raise StrataPanic("engine: RawSource.ReadWindow: the source has a fill value and dst has no validity mask")
+        fill = np.float32(self.opts.Fill)
+        for row, k in _rows(dst, self.w):
+            n = 4 * ((k - 1) * dst.stride + dst.width)
+            b = os.pread(_fd(self.f), n, self.offset + 4 * ((y + row) * self.w + x))
+            if len(b) < n:
+                return SourceSinkError(f"engine: raw source: reading {_rows_name(y + row, k)}: unexpected EOF")
+            cells = np.frombuffer(b, np.float32)
+            s = row * dst.stride
+            dst.data[s:s + cells.size] = cells
+        if dst.valid is not None:
+            for yy in range(dst.height):
+                c = np.asarray(dst.data[yy * dst.stride:yy * dst.stride + dst.width])
+                ok = ~np.isnan(c) if np.isnan(fill) else (c != fill) if self.opts.HasFill else np.ones(c.size, bool)
+                _put_bits(dst.valid, dst.valid_offset + yy * dst.stride, ok.astype(np.uint8))
+        return None
+
+
+class RawSink(RasterSink):
+    """engine.RawSink: writes a width×height raw float32 raster to f at
+    byte offset offset, the fill value under invalid cells."""
+
+    def __init__(self, f, width: int, height: int, opts: RawOptions = RawOptions(), offset: int = 0):
+        _raw_size_check("NewRawSink", f, width, height)
+        self.f, self.w, self.h, self.opts, self.offset = f, width, height, opts, offset
+
+    def Size(self):
+        return self.w, self.h
+
+    def Masked(self) -> bool:
+        return bool(self.opts.HasFill)
+
+    def WriteWindow(self, src: Float32Raster, x: int, y: int):
+        import os
+
+        if src.valid is not None and not self.opts.HasFill:
+            raise StrataPanic("engine: RawSink.WriteWindow: src has a validity mask and the sink has no fill value")
+        fill = np.float32(self.opts.Fill)
+        for row, k in _rows(src, self.w):
+            n = (k - 1) * src.stride + src.width
+            s = row * src.stride
+            cells = np.array(src.data[s:s + n], np.float32)
+            if src.valid is not None:
+                for j in range(k):
+                    bits = _bits(src.valid, src.valid_offset + (row + j) * src.stride, src.width)
+                    seg = cells[j * src.stride:j * src.stride + src.width]
+                    seg[bits == 0] = fill
+            b = cells.tobytes()
+            if os.pwrite(_fd(self.f), b, self.offset + 4 * ((y + row) * self.w + x)) < len(b):
+                return SourceSinkError(f"engine: raw sink: writing {_rows_name(y + row, k)}: short write")
+        return None
+
+
+def process_raw(stages: StageList, dst: Sequence[RawSink], src: Sequence[RawSource],
+                opts: Optional[Options] = None, ctx: Optional[Context] = None):
+    """exec.ProcessChunked over raw files on the device (strata_process_raw).
+    Returns None, Canceled, or a SourceSinkError."""
+    dev = opts.Device if opts is not None else 0
+    c = device_context(dev)
+
+    def raw(r):
+        f = _lib.RawFile()
+        f.fd, f.has_fill, f.fill = _fd(r.f), 1 if r.opts.HasFill else 0, r.opts.Fill
+        f.width, f.height, f.offset = r.w, r.h, r.offset
+        return f
+
+    srcs = (_lib.RawFile * len(src))(*[raw(s) for s in src])
+    dsts = (_lib.RawFile * len(dst))(*[raw(d) for d in dst])
+    o = c_opts(opts, ctx)
+    cst = _lib.Stats()
+    rc = _lib.lib().strata_process_raw(c, stages.c_array(), len(stages.stages), srcs, len(src), dsts, len(dst),
+                                       ctypes.byref(o), ctypes.byref(cst))
+    _stats_out(opts, cst)
+    if rc == _lib.ECANCELED:
+        return Canceled("context canceled")
+    if rc == _lib.EIO:
+        return SourceSinkError(_lib.last_error())
     _lib.check(rc)
     return None

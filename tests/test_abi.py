@@ -62,7 +62,7 @@ def test_struct_layouts_match_header(tmp_path):
         "strata_gradient_options": _lib.GradientOptions, "strata_ruggedness_options": _lib.RuggednessOptions,
         "strata_weights_options": _lib.WeightsOptions, "strata_separable_options": _lib.SeparableOptions,
         "strata_box_options": _lib.BoxOptions, "strata_heatload_options": _lib.HeatLoadOptions,
-        "strata_orientation_options": _lib.OrientationOptions,
+        "strata_orientation_options": _lib.OrientationOptions, "strata_raw_file": _lib.RawFile,
     }
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void){"]
     for cname, ct in structs.items():
