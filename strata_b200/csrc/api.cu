@@ -16,6 +16,8 @@
 #include <algorithm>
 #include <cstring>
 #include <functional>
+#include <future>
+#include <thread>
 #include <limits>
 #include <memory>
 #include <mutex>
@@ -154,6 +156,9 @@ struct strata_ctx {
     // page-locked host copy.
     int* d_status = nullptr;
     int* h_status = nullptr;
+    // The chunked calls' two tile buffer sets (page-locked and device),
+    // grown on demand and reused.
+    std::shared_ptr<void> chunk_sets;
 };
 
 namespace {
@@ -1708,6 +1713,9 @@ struct TileSet {
     int64_t x0 = 0, y0 = 0, x1 = 0, y1 = 0;
     int64_t out_stride[2] = {0, 0};
     bool pending = false;
+    ~TileSet() {
+        if (done) cudaEventDestroy(done);
+    }
 };
 
 // Where a chunked call's tiles come from and go to: the caller's callbacks
@@ -1727,6 +1735,7 @@ struct ChunkIO {
     // Takes output i's finished host tile (bits only for an output that is
     // masked and not filled).
     std::function<int(int i, const strata_raster& buf, int64_t x, int64_t y)> write;
+    bool async_write = false;  // write a tile on a second thread while the next is read
 };
 
 // exec.ProcessChunked's tile loop (internal/exec/chunked.go:33-464) over
@@ -1751,8 +1760,12 @@ int run_chunked(strata_ctx* c, const LaunchParams& p, int nout, int64_t W, int64
     DeviceGuard device_guard(c->device);
     cudaStream_t st = (opts && opts->stream) ? (cudaStream_t)opts->stream : c->stream;
 
-    TileSet sets[2];
-    for (auto& s : sets) {
+    if (!c->chunk_sets)
+        c->chunk_sets = std::shared_ptr<void>(new TileSet[2], [](void* q) { delete[] static_cast<TileSet*>(q); });
+    TileSet* sets = static_cast<TileSet*>(c->chunk_sets.get());
+    for (int k = 0; k < 2; k++) {
+        TileSet& s = sets[k];
+        s.pending = false;
         if ((rc = s.in_data.get((size_t)in_cells * 4)) || (rc = s.d_in_data.get((size_t)in_cells * 4))) return rc;
         if (in_masked) {
             size_t words = (size_t)((in_cells + 63) / 64);
@@ -1770,23 +1783,16 @@ int run_chunked(strata_ctx* c, const LaunchParams& p, int nout, int64_t W, int64
                 if (!io.out_fill[i] && (rc = s.out_bits[i].get(words * 8))) return rc;
             }
         }
-        if (cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming) != cudaSuccess)
+        if (!s.done && cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming) != cudaSuccess) {
+            s.done = nullptr;
             return fail(STRATA_ECUDA, "strata_cuda: cudaEventCreate");
-    }
-    struct EventGuard {
-        TileSet* s;
-        ~EventGuard() {
-            for (int i = 0; i < 2; i++)
-                if (s[i].done) cudaEventDestroy(s[i].done);
         }
-    } guard{sets};
+    }
 
     strata_stats local = {};
     int status = STRATA_OK;
     // Hands a finished tile to the sinks.
-    auto flush = [&](TileSet& s) -> int {
-        if (!s.pending) return STRATA_OK;
-        s.pending = false;
+    auto write_tile = [&](TileSet& s) -> int {
         cudaError_t e = cudaEventSynchronize(s.done);
         if (e != cudaSuccess) return cuda_fail(e, "tile");
         for (int i = 0; i < ndst; i++) {
@@ -1796,7 +1802,8 @@ int run_chunked(strata_ctx* c, const LaunchParams& p, int nout, int64_t W, int64
             b.height = s.y1 - s.y0;
             b.stride = s.out_stride[i];
             b.valid = io.out_masked[i] && !io.out_fill[i] ? (uint64_t*)s.out_bits[i].p : nullptr;
-            if ((rc = io.write(i, b, s.x0, s.y0)) != STRATA_OK) return rc;
+            const int wrc = io.write(i, b, s.x0, s.y0);
+            if (wrc != STRATA_OK) return wrc;
         }
         int64_t cells = (s.x1 - s.x0) * (s.y1 - s.y0);
         local.sink_written += cells * 4 * ndst;
@@ -1806,13 +1813,47 @@ int run_chunked(strata_ctx* c, const LaunchParams& p, int nout, int64_t W, int64
         local.tiles++;
         return STRATA_OK;
     };
+    auto flush = [&](TileSet& s) -> int {
+        if (!s.pending) return STRATA_OK;
+        s.pending = false;
+        return write_tile(s);
+    };
+    // With io.async_write a tile goes to the sinks on a second thread while
+    // the next tile is read: its status, and its message (set on that
+    // thread), come back when it is joined, before the set's output
+    // buffers take another tile and before the call returns.
+    std::future<std::pair<int, std::string>> writing;
+    auto flush_async = [&](TileSet& s) {
+        if (!s.pending) return;
+        s.pending = false;
+        TileSet* sp = &s;
+        writing = std::async(std::launch::async, [&write_tile, sp]() {
+            const int wrc = write_tile(*sp);
+            return std::make_pair(wrc, wrc == STRATA_OK ? std::string() : g_err);
+        });
+    };
+    auto join_write = [&]() -> int {
+        if (!writing.valid()) return STRATA_OK;
+        auto r = writing.get();
+        if (r.first != STRATA_OK) g_err = r.second;
+        return r.first;
+    };
 
     const volatile int32_t* cancel = opts ? opts->cancel : nullptr;
     for (int64_t t = 0; t < ntiles && status == STRATA_OK; t++) {
         TileSet& s = sets[t & 1];
         // The set's previous tile (t - 2) must be with the sinks before its
-        // buffers are reused; tile t - 1 is written while t computes.
+        // buffers are reused; tile t - 1 is written while t computes. A
+        // background write of tile t - 2 needs only its input copied in
+        // before this read reuses the input buffers.
         if ((status = flush(s))) break;
+        if (io.async_write) {
+            const cudaError_t e = cudaEventSynchronize(s.done);
+            if (e != cudaSuccess) {
+                status = cuda_fail(e, "tile");
+                break;
+            }
+        }
         if (cancel && *cancel) {
             status = STRATA_ECANCELED;
             break;
@@ -1915,6 +1956,9 @@ int run_chunked(strata_ctx* c, const LaunchParams& p, int nout, int64_t W, int64
             if (io.out_fill[i])
                 strata::launch_fill_invalid((float*)s.d_out_data[i].p, s.out_stride[i], x1 - x0, y1 - y0,
                                             (const uint32_t*)s.d_out_bits[i].p, io.out_fill_value[i], st);
+        // The set's output buffers still hold tile t - 2 while its
+        // background write runs.
+        if (io.async_write && (status = join_write())) break;
         for (int i = 0; i < ndst && e == cudaSuccess; i++) {
             int64_t oc = (y1 - y0 - 1) * s.out_stride[i] + (x1 - x0);
             e = cudaMemcpyAsync(s.out_data[i].p, s.d_out_data[i].p, (size_t)oc * 4, cudaMemcpyDeviceToHost, st);
@@ -1934,7 +1978,13 @@ int run_chunked(strata_ctx* c, const LaunchParams& p, int nout, int64_t W, int64
         s.y1 = y1;
         s.pending = true;
         // Write the other set's tile (t - 1) while this one runs.
-        if ((status = flush(sets[(t + 1) & 1]))) break;
+        if (io.async_write) flush_async(sets[(t + 1) & 1]);
+        else if ((status = flush(sets[(t + 1) & 1]))) break;
+    }
+    // A tile still being written is the oldest.
+    {
+        const int wrc = join_write();
+        if (status == STRATA_OK || status == STRATA_ECANCELED) status = wrc ? wrc : status;
     }
     // Tiles already computed are written in plan order, after a cancel too;
     // after a failure nothing more is written.
@@ -1987,6 +2037,41 @@ int64_t raw_io(bool write, int fd, char* p, int64_t n, int64_t off) {
     return done;
 }
 
+// raw_io over large spans in parts of at least 2 MiB on up to 8 threads
+// (a page-cache copy runs at one core's memory bandwidth). Returns whether
+// every byte moved, with the first failing part's errno in *err.
+bool raw_io_parallel(bool write, int fd, char* p, int64_t n, int64_t off, int* err) {
+    constexpr int64_t kPart = (int64_t)2 << 20;
+    const int parts = (int)std::min<int64_t>(8, std::max<int64_t>(1, n / kPart));
+    *err = 0;
+    if (parts == 1) {
+        const bool ok = raw_io(write, fd, p, n, off) == n;
+        if (!ok) *err = errno;
+        return ok;
+    }
+    const int64_t step = (n / parts + 4095) / 4096 * 4096;
+    std::vector<std::thread> threads;
+    std::vector<int> errs((size_t)parts, 0);
+    std::vector<char> oks((size_t)parts, 1);
+    for (int k = 0; k < parts; k++) {
+        const int64_t a = k * step, b = std::min(n, a + step);
+        if (a >= b) break;
+        threads.emplace_back([=, &errs, &oks]() {
+            if (raw_io(write, fd, p + a, b - a, off + a) != b - a) {
+                oks[(size_t)k] = 0;
+                errs[(size_t)k] = errno;
+            }
+        });
+    }
+    for (auto& t : threads) t.join();
+    for (int k = 0; k < parts; k++)
+        if (!oks[(size_t)k]) {
+            *err = errs[(size_t)k];
+            return false;
+        }
+    return true;
+}
+
 std::string rows_name(int64_t y, int64_t k) {
     char b[64];
     if (k == 1) snprintf(b, sizeof b, "row %lld", (long long)y);
@@ -2005,9 +2090,8 @@ int raw_rows(bool write, const strata_raw_file& f, const strata_raster& buf, int
         const int64_t k = std::min(per, buf.height - row);
         const int64_t n = ((k - 1) * buf.stride + buf.width) * 4;
         const int64_t off = f.offset + 4 * ((y + row) * f.width + x);
-        const int64_t got = raw_io(write, f.fd, (char*)(buf.data + row * buf.stride), n, off);
-        if (got < n) {
-            const int err = errno;
+        int err = 0;
+        if (!raw_io_parallel(write, f.fd, (char*)(buf.data + row * buf.stride), n, off, &err)) {
             if (write)
                 return fail(STRATA_EIO, "engine: raw sink: writing %s: %s", rows_name(y + row, k).c_str(),
                             err ? strerror(err) : "short write");
@@ -2115,6 +2199,7 @@ extern "C" int strata_process_raw(strata_ctx* c, const strata_stage* stages, int
         io.out_fill_value[i] = dst[i].fill;
     }
     io.write = [&](int i, const strata_raster& b, int64_t x, int64_t y) { return raw_rows(true, dst[i], b, x, y); };
+    io.async_write = true;
     return run_chunked(c, p, nout, W, H, io, opts, stats);
 }
 
