@@ -235,6 +235,37 @@ int strata_process(strata_ctx *ctx, const strata_stage *stages, int nstages,
                    const strata_exec_opts *opts, strata_stats *stats);
 
 /*
+ * A row strip of a raster `height` rows tall (the multi-GPU split:
+ * internal/exec/worker.go:83-181 splits a raster into bands the same way):
+ * src holds input rows [src_row, src_row + src->height) and dst output rows
+ * [dst_row, dst_row + dst->height). The source rows must cover every row
+ * the outputs read, [dst_row - radius, dst_row + dst->height + radius)
+ * clipped to the raster. The outputs are the rows strata_process writes
+ * for them over the whole raster: the edge ring lies at the whole
+ * raster's border only. One input; the rest as strata_process.
+ */
+typedef struct {
+    int64_t height;
+    int64_t src_row;
+    int64_t dst_row;
+} strata_strip;
+int strata_process_strip(strata_ctx *ctx, const strata_stage *stages, int nstages, const strata_raster *src,
+                         const strata_raster *dst, int ndst, const strata_strip *strip, const strata_exec_opts *opts,
+                         strata_stats *stats);
+
+/*
+ * strata_process over several devices, one context each: the raster is
+ * cut into nctx row strips as equal as can be, each strip with its halo
+ * rows read from the host by its own device and computed there
+ * (strata_process_strip) on a thread of its own, the strips' rows written
+ * back in place. Host rasters, one input; no stream or cancel flag. The
+ * result is strata_process's, bit for bit.
+ */
+int strata_process_multi(strata_ctx *const *ctxs, int nctx, const strata_stage *stages, int nstages,
+                         const strata_raster *src, int nsrc, const strata_raster *dst, int ndst,
+                         const strata_exec_opts *opts, strata_stats *stats);
+
+/*
  * terrain.Features / terrain.Surface (terrain/features.go:60-92,
  * terrain/surface.go:57-98): several pipelines over one input in one call.
  * Feature f is stages[s_f .. s_f + counts[f]) (s_f the sum of the earlier

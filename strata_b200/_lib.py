@@ -61,6 +61,10 @@ READ_FN = ctypes.CFUNCTYPE(ctypes.c_int, c_p, ctypes.POINTER(Raster), c_i64, c_i
 WRITE_FN = ctypes.CFUNCTYPE(ctypes.c_int, c_p, ctypes.POINTER(Raster), c_i64, c_i64)
 
 
+class Strip(ctypes.Structure):
+    _fields_ = [("height", c_i64), ("src_row", c_i64), ("dst_row", c_i64)]
+
+
 class RawFile(ctypes.Structure):
     _fields_ = [("fd", c_i32), ("has_fill", c_i32), ("fill", c_f32), ("reserved", c_i32), ("width", c_i64),
                 ("height", c_i64), ("offset", c_i64)]
@@ -182,6 +186,12 @@ SIGNATURES = [
     ("strata_process_features", ctypes.c_int, [c_p, ctypes.POINTER(Stage), ctypes.POINTER(c_i32), ctypes.c_int,
                                                ctypes.POINTER(Raster), ctypes.POINTER(Raster), ctypes.c_int,
                                                ctypes.POINTER(ExecOpts), ctypes.POINTER(Stats)]),
+    ("strata_process_strip", ctypes.c_int, [c_p, ctypes.POINTER(Stage), ctypes.c_int, ctypes.POINTER(Raster),
+                                             ctypes.POINTER(Raster), ctypes.c_int, ctypes.POINTER(Strip),
+                                             ctypes.POINTER(ExecOpts), ctypes.POINTER(Stats)]),
+    ("strata_process_multi", ctypes.c_int, [ctypes.POINTER(c_p), ctypes.c_int, ctypes.POINTER(Stage), ctypes.c_int,
+                                             ctypes.POINTER(Raster), ctypes.c_int, ctypes.POINTER(Raster), ctypes.c_int,
+                                             ctypes.POINTER(ExecOpts), ctypes.POINTER(Stats)]),
     ("strata_process_raw", ctypes.c_int, [c_p, ctypes.POINTER(Stage), ctypes.c_int, ctypes.POINTER(RawFile),
                                            ctypes.c_int, ctypes.POINTER(RawFile), ctypes.c_int,
                                            ctypes.POINTER(ExecOpts), ctypes.POINTER(Stats)]),

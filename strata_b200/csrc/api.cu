@@ -16,6 +16,7 @@
 #include <algorithm>
 #include <cstring>
 #include <functional>
+#include <thread>
 #include <future>
 #include <thread>
 #include <limits>
@@ -900,7 +901,12 @@ cudaError_t mask_back(const strata_raster& r, const DevOperand& d, uint64_t* edg
 
 // Merges the edge words mask_back fetched: only the raster's own bits of
 // them change.
+// Strips of one raster computed at once on several devices share their
+// edge words, so the merges take turns.
+std::mutex g_edge_mu;
+
 void merge_edges(const strata_raster& r, const DevOperand& d, const uint64_t* edge) {
+    std::lock_guard<std::mutex> lock(g_edge_mu);
     const int64_t lo = r.valid_offset, hi = r.valid_offset + span_cells(r);
     auto merge = [&](int64_t k, uint64_t v) {
         const int64_t w = d.host_w0 + k;
@@ -1200,6 +1206,209 @@ extern "C" int strata_process(strata_ctx* c, const strata_stage* stages, int nst
         stats->kernel_written += cells * 4 * nout;
     }
     if (canceled) return fail(STRATA_ECANCELED, "context canceled");
+    return STRATA_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Row strips of one raster (the multi-GPU split): a strip's outputs are
+// the rows strata_process writes for them over the whole raster.
+
+extern "C" int strata_process_strip(strata_ctx* c, const strata_stage* stages, int nstages, const strata_raster* src,
+                                    const strata_raster* dst, int ndst, const strata_strip* strip,
+                                    const strata_exec_opts* opts, strata_stats* stats) {
+    if (!c) return fail(STRATA_EINVAL, "engine: nil context");
+    if (!strip || !src || !dst) return fail(STRATA_EINVAL, "engine: nil strip operands");
+    LaunchParams p;
+    int nout = 0;
+    int rc = plan_stages(stages, nstages, p, &nout);
+    if (rc) return rc;
+    if ((rc = check_opts(opts))) return rc;
+    if (p.ninputs > 1) return fail(STRATA_ENOTSUP, "engine: a chain over several inputs has no strip form");
+    if (ndst != nout)
+        return fail(STRATA_EINVAL, "engine: kernel takes 1 inputs and %d outputs, got 1 and %d", nout, ndst);
+    if ((rc = validate("src", 0, src[0]))) return rc;
+    for (int i = 0; i < ndst; i++) {
+        if ((rc = validate("dst", i, dst[i]))) return rc;
+        if (dst[i].width != src[0].width || dst[i].height != dst[0].height)
+            return fail(STRATA_EINVAL, "engine: dst[%d] is %lld×%lld, the strip is %lld×%lld", i,
+                        (long long)dst[i].width, (long long)dst[i].height, (long long)src[0].width,
+                        (long long)dst[0].height);
+        if (src[0].valid && !dst[i].valid)
+            return fail(STRATA_EINVAL,
+                        "engine: an input has a validity mask but dst[%d].Valid is nil; allocate it with "
+                        "raster.NewFloat32Like, or set Valid on its root raster before windowing",
+                        i);
+        if (p.radius > 0 && (data_spans(dst[i], src[0]) || bit_spans(dst[i], src[0])))
+            return fail(STRATA_EINVAL, "engine: dst[%d] and src[0] share memory; a kernel with radius %d would read "
+                                       "neighbours it has already overwritten", i, p.radius);
+        for (int j = 0; j < i; j++)
+            if (data_spans(dst[i], dst[j]) || bit_spans(dst[i], dst[j]))
+                return fail(STRATA_EINVAL, "engine: dst[%d] and dst[%d] share memory", j, i);
+    }
+    const int64_t H = strip->height, W = src[0].width;
+    const int64_t s0 = strip->src_row, s1 = s0 + src[0].height;
+    const int64_t y0 = strip->dst_row, y1 = y0 + dst[0].height;
+    const int r = p.radius;
+    if (y0 < 0 || y1 > H || s0 < 0 || s1 > H)
+        return fail(STRATA_EINVAL, "engine: strip rows [%lld, %lld) and source rows [%lld, %lld) must lie in the "
+                                   "raster's %lld rows",
+                    (long long)y0, (long long)y1, (long long)s0, (long long)s1, (long long)H);
+    if (s0 > std::max<int64_t>(0, y0 - r) || s1 < std::min<int64_t>(H, y1 + r))
+        return fail(STRATA_EINVAL, "engine: source rows [%lld, %lld) do not cover rows [%lld, %lld) that output rows "
+                                   "[%lld, %lld) read at radius %d",
+                    (long long)s0, (long long)s1, (long long)std::max<int64_t>(0, y0 - r),
+                    (long long)std::min<int64_t>(H, y1 + r), (long long)y0, (long long)y1, r);
+
+    std::lock_guard<std::mutex> lock(c->mu);
+    DeviceGuard device_guard(c->device);
+    cudaStream_t st = (opts && opts->stream) ? (cudaStream_t)opts->stream : c->stream;
+    DevOperand ds, dd[2];
+    if ((rc = stage_in(c, st, src[0], 0, true, &ds))) return rc;
+    for (int i = 0; i < ndst; i++)
+        if ((rc = stage_in(c, st, dst[i], 2 + 2 * i, false, &dd[i]))) return rc;
+    p.src = ds.data;
+    p.src_stride = ds.stride;
+    p.src_x0 = 0;
+    p.src_y0 = s0;
+    p.src_w = W;
+    p.src_h = s1 - s0;
+    p.in[0] = ds.data;
+    p.in_stride[0] = ds.stride;
+    p.dst0 = dd[0].data;
+    p.dst0_stride = dd[0].stride;
+    if (ndst > 1) {
+        p.dst1 = dd[1].data;
+        p.dst1_stride = dd[1].stride;
+    }
+    p.dst_x0 = 0;
+    p.dst_y0 = y0;
+    p.width = W;
+    p.height = H;
+    p.out_x0 = 0;
+    p.out_x1 = W;
+    p.out_y0 = y0;
+    p.out_y1 = y1;
+    p.status = c->d_status;
+    p.test_stall = test_stall_requested();
+    ValidityParams vp[2];
+    const ValidityParams* vs[2] = {nullptr, nullptr};
+    for (int i = 0; i < ndst; i++) {
+        if (!dst[i].valid) continue;
+        ValidityParams& v = vp[i];
+        memset(&v, 0, sizeof v);
+        if (src[0].valid) {
+            v.src_bits = ds.bits;
+            v.src_off = ds.bit_off;
+            v.src_stride = ds.stride;
+            v.src_lo_word = ds.lo_word;
+            v.src_hi_word = ds.hi_word;
+        }
+        v.src_y0 = s0;
+        v.dst_bits = dd[i].bits;
+        v.dst_off = dd[i].bit_off;
+        v.dst_stride = dd[i].stride;
+        v.dst_y0 = y0;
+        v.out_x1 = W;
+        v.out_y0 = y0;
+        v.out_y1 = y1;
+        v.width = W;
+        v.height = H;
+        v.radius = r;
+        const int64_t b0 = dd[i].bit_off, b1 = dd[i].bit_off + (y1 - y0 - 1) * dd[i].stride + W;
+        v.dst_lo_word = b0 >> 5;
+        v.dst_words = ((b1 + 31) >> 5) - v.dst_lo_word;
+        vs[i] = &v;
+    }
+    int64_t wc = 0;
+    const int64_t t = p.fit ? launch_fit(c, p, vs, st, &wc) : strata::launch_stage(p, vs, st, &wc);
+    if (t == -2) return fail(STRATA_ENOMEM, "engine: no device memory for the fit's sums");
+    if (t < 0) return fail(STRATA_ENOTSUP, "engine: op %d at radius %d has no device kernel", p.op, p.radius);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
+    for (int i = 0; i < ndst; i++)
+        if ((rc = stage_out(c, st, dst[i], dd[i]))) return rc;
+    const bool all_device = src[0].on_device && dst[0].on_device && (ndst < 2 || dst[1].on_device);
+    if (!(all_device && opts && (opts->flags & STRATA_EXEC_ASYNC)))
+        if ((rc = take_status(c, st))) return rc;
+    if (stats) {
+        const int64_t cells = (y1 - y0) * W;
+        stats->cells += cells;
+        stats->ideal += cells * 4 * (1 + nout);
+        stats->bands += t;
+        stats->kernel_read += wc * 4;
+        stats->kernel_written += cells * 4 * nout;
+    }
+    return STRATA_OK;
+}
+
+// A view of rows [y0, y1) of r.
+static strata_raster rows_of(const strata_raster& r, int64_t y0, int64_t y1) {
+    strata_raster v = r;
+    v.data = r.data + y0 * r.stride;
+    v.height = y1 - y0;
+    if (r.valid) v.valid_offset = r.valid_offset + y0 * r.stride;
+    return v;
+}
+
+extern "C" int strata_process_multi(strata_ctx* const* ctxs, int nctx, const strata_stage* stages, int nstages,
+                                    const strata_raster* src, int nsrc, const strata_raster* dst, int ndst,
+                                    const strata_exec_opts* opts, strata_stats* stats) {
+    if (!ctxs || nctx < 1) return fail(STRATA_EINVAL, "engine: no devices");
+    for (int i = 0; i < nctx; i++)
+        if (!ctxs[i]) return fail(STRATA_EINVAL, "engine: nil context %d", i);
+    if (nctx == 1) return strata_process(ctxs[0], stages, nstages, src, nsrc, dst, ndst, opts, stats);
+    LaunchParams p;
+    int nout = 0;
+    int rc = plan_stages(stages, nstages, p, &nout);
+    if (rc) return rc;
+    if ((rc = check_opts(opts))) return rc;
+    if (p.ninputs > 1 || nsrc > 1)
+        return fail(STRATA_ENOTSUP, "engine: a chain over several inputs has no multi-device form");
+    if ((rc = check_operands(src, nsrc, dst, ndst, nout, p.radius))) return rc;
+    if (opts && (opts->stream || opts->cancel))
+        return fail(STRATA_EINVAL, "engine: a multi-device call takes no stream or cancel flag");
+    if (src[0].on_device || dst[0].on_device || (ndst > 1 && dst[1].on_device))
+        return fail(STRATA_ENOTSUP, "engine: a multi-device call takes host rasters");
+    // shard.strips: contiguous output rows, as equal as can be, each with
+    // its halo rows read from the host by its own device.
+    const int64_t H = src[0].height, r = p.radius;
+    const int64_t base = H / nctx, extra = H % nctx;
+    std::vector<int> codes((size_t)nctx, STRATA_OK);
+    std::vector<std::string> errs((size_t)nctx);
+    std::vector<strata_stats> part((size_t)nctx);
+    std::vector<std::thread> threads;
+    int64_t y = 0;
+    for (int i = 0; i < nctx; i++) {
+        const int64_t n = base + (i < extra ? 1 : 0);
+        const int64_t y0 = y, y1 = y + n;
+        y = y1;
+        if (n == 0) continue;
+        threads.emplace_back([&, i, y0, y1]() {
+            const int64_t s0 = std::max<int64_t>(0, y0 - r), s1 = std::min<int64_t>(H, y1 + r);
+            const strata_raster sv = rows_of(src[0], s0, s1);
+            strata_raster dv[2];
+            for (int k = 0; k < ndst; k++) dv[k] = rows_of(dst[k], y0, y1);
+            const strata_strip strip = {H, s0, y0};
+            memset(&part[(size_t)i], 0, sizeof(strata_stats));
+            codes[(size_t)i] = strata_process_strip(ctxs[i], stages, nstages, &sv, dv, ndst, &strip, opts,
+                                                    &part[(size_t)i]);
+            if (codes[(size_t)i] != STRATA_OK) errs[(size_t)i] = g_err;
+        });
+    }
+    for (auto& t : threads) t.join();
+    for (int i = 0; i < nctx; i++)
+        if (codes[(size_t)i] != STRATA_OK) {
+            g_err = errs[(size_t)i];
+            return codes[(size_t)i];
+        }
+    if (stats)
+        for (const strata_stats& q : part) {
+            stats->cells += q.cells;
+            stats->ideal += q.ideal;
+            stats->bands += q.bands;
+            stats->kernel_read += q.kernel_read;
+            stats->kernel_written += q.kernel_written;
+        }
     return STRATA_OK;
 }
 

@@ -27,7 +27,9 @@ class Options:
     the chunked tiles (0 = the whole raster); Workers is accepted for
     parity. Stats, when set, is added to by the call. Stream is an optional
     torch.cuda.Stream for device-resident operands; Async skips the final
-    synchronisation when every operand is on the device."""
+    synchronisation when every operand is on the device. Device picks the
+    GPU; Devices, with more than one entry, splits a plain call's raster
+    into row strips over those GPUs (strata_process_multi)."""
     TileWidth: int = 0
     TileHeight: int = 0
     Workers: int = 0
@@ -35,6 +37,7 @@ class Options:
     Stream: object = None
     Async: bool = False
     Device: int = 0
+    Devices: Optional[List[int]] = None
 
 
 @dataclass
@@ -188,6 +191,8 @@ def process(stages: StageList, dst: Sequence[Float32Raster], src: Sequence[Float
             opts: Optional[Options] = None, ctx: Optional[Context] = None):
     """exec.ProcessN on the device. Returns None, or Canceled if ctx was
     cancelled first; raises StrataPanic on programming errors."""
+    if opts is not None and opts.Devices and len(opts.Devices) > 1:
+        return process_multi(stages, dst, src, opts, ctx)
     dev = opts.Device if opts is not None else 0
     c = device_context(dev)
     srcs = (_lib.Raster * len(src))(*[c_raster(s) for s in src])
@@ -199,6 +204,44 @@ def process(stages: StageList, dst: Sequence[Float32Raster], src: Sequence[Float
     _stats_out(opts, cst)
     if rc == _lib.ECANCELED:
         return Canceled("context canceled")
+    _lib.check(rc)
+    return None
+
+
+def process_multi(stages: StageList, dst: Sequence[Float32Raster], src: Sequence[Float32Raster],
+                  opts: Options, ctx: Optional[Context] = None):
+    """A plain call split into row strips over opts.Devices, each strip with
+    its halo rows computed on its own GPU (strata_process_multi); the same
+    bits as one device. Host rasters."""
+    if ctx is not None:
+        raise StrataPanic("engine: a multi-device call takes no cancellable context")
+    ctxs = (ctypes.c_void_p * len(opts.Devices))(*[device_context(d) for d in opts.Devices])
+    srcs = (_lib.Raster * len(src))(*[c_raster(s) for s in src])
+    dsts = (_lib.Raster * len(dst))(*[c_raster(d) for d in dst])
+    o = c_opts(Options(TileWidth=opts.TileWidth, TileHeight=opts.TileHeight, Workers=opts.Workers))
+    cst = _lib.Stats()
+    rc = _lib.lib().strata_process_multi(ctxs, len(opts.Devices), stages.c_array(), len(stages.stages), srcs,
+                                         len(src), dsts, len(dst), ctypes.byref(o), ctypes.byref(cst))
+    _stats_out(opts, cst)
+    _lib.check(rc)
+    return None
+
+
+def process_strip(stages: StageList, dst: Sequence[Float32Raster], src: Float32Raster, height: int, src_row: int,
+                  dst_row: int, opts: Optional[Options] = None):
+    """Rows [dst_row, dst_row + dst[0].height) of a height-row raster's
+    outputs from its input rows [src_row, src_row + src.height), as
+    strata_process writes them over the whole raster (strata_process_strip)."""
+    dev = opts.Device if opts is not None else 0
+    c = device_context(dev)
+    s = c_raster(src)
+    dsts = (_lib.Raster * len(dst))(*[c_raster(d) for d in dst])
+    strip = _lib.Strip(height, src_row, dst_row)
+    o = c_opts(opts)
+    cst = _lib.Stats()
+    rc = _lib.lib().strata_process_strip(c, stages.c_array(), len(stages.stages), ctypes.byref(s), dsts, len(dst),
+                                         ctypes.byref(strip), ctypes.byref(o), ctypes.byref(cst))
+    _stats_out(opts, cst)
     _lib.check(rc)
     return None
 

@@ -8,11 +8,14 @@ keeps the rows that are not its own edge ring. Rows a strip's own edge ring
 covers are either the whole raster's edge ring (kept, they are NaN and
 invalid there too) or rows another rank owns (dropped). No data moves
 between ranks while computing: there is no collective on the data path.
-The only collective a multi-GPU run needs is the max of the ranks' times.
+The only collective a multi-GPU run needs is the max of the ranks' times,
+and, when every rank wants the whole result, the exchange of the strips
+(process_sharded). In one process, engine.Options(Devices=[...]) runs the
+same split over several GPUs (strata_process_multi).
 """
 from __future__ import annotations
 
-from typing import List, Tuple
+from typing import Callable, List, Optional, Tuple
 
 
 def strips(height: int, world: int) -> List[Tuple[int, int]]:
@@ -65,3 +68,65 @@ def max_over_ranks(value: float, device=None) -> float:
     t = torch.tensor([value], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def stage_radius(stages) -> int:
+    """How far the pipeline's first stage reads (its tail is pointwise): the
+    fit's radius, 1 for the Horn and Zevenbergen-Thorne products, 0 for a
+    pointwise pipeline, else the stage's radius."""
+    from . import _lib
+
+    st = stages.stages[0]
+    if st.flags & _lib.STAGE_FIT:
+        return int(st.radius)
+    if st.op in (_lib.OP_GRADIENT, _lib.OP_SLOPE, _lib.OP_ASPECT, _lib.OP_HILLSHADE, _lib.OP_CURVATURE,
+                 _lib.OP_HEATLOAD, _lib.OP_ORIENTATION):
+        return 1
+    if st.op in (_lib.OP_LOOKUP, _lib.OP_RECLASS, _lib.OP_STEP):
+        return 0
+    return int(st.radius)
+
+
+def process_sharded(stages, dst, src, rank: Optional[int] = None, world: Optional[int] = None, opts=None,
+                    compute: Optional[Callable] = None, group=None) -> None:
+    """One raster over the ranks of a process group, one rank a GPU: every
+    rank holds the host input src and outputs dst; rank i computes output
+    rows strips(H, world)[i] from their halo rows on its own device
+    (engine.process_strip, the same rows strata_process writes), then the
+    strips are exchanged so that every rank's dst holds the whole result.
+    No data moves between ranks while computing; the exchange is the
+    reassembly. compute replaces the device call (same arguments as
+    engine.process_strip) where a rank has no GPU."""
+    import numpy as np
+
+    from . import engine
+    from .raster import Float32Raster, mask_from_bool
+
+    if rank is None or world is None:
+        import torch.distributed as dist
+
+        rank, world = dist.get_rank(group), dist.get_world_size(group)
+    H, W = src.height, src.width
+    r = stage_radius(stages)
+    y0, y1 = strips(H, world)[rank]
+    if y1 > y0:
+        s0, s1 = halo_rows(H, r, y0, y1)
+        (compute or engine.process_strip)(stages, [d.Window(0, y0, W, y1 - y0) for d in dst],
+                                          src.Window(0, s0, W, s1 - s0), H, s0, y0, opts)
+    if world == 1:
+        return None
+    import torch.distributed as dist
+
+    mine = [(d.Window(0, y0, W, y1 - y0).numpy(), d.Window(0, y0, W, y1 - y0).valid_numpy()) if y1 > y0 else None
+            for d in dst]
+    got = [None] * world
+    dist.all_gather_object(got, (y0, y1, mine), group=group)
+    for k, (a0, a1, parts) in enumerate(got):
+        if k == rank or a1 <= a0:
+            continue
+        for d, (cells, valid) in zip(dst, parts):
+            win = d.Window(0, a0, W, a1 - a0)
+            part = Float32Raster(np.ascontiguousarray(cells).reshape(-1), W, a1 - a0, W,
+                                 None if valid is None else mask_from_bool(valid, W, 0), 0)
+            engine._copy_cells(win, part, valid is not None and win.valid is not None)
+    return None
