@@ -993,6 +993,34 @@ def run_raw(args, rank, world, local_rank):
             "parity": {"rows_checked": rows - 1, "cells": int(w2.size), "mismatches": int(bad.sum())}}
 
 
+def run_stats(args, local_rank):
+    """engine.Stats of each op of the workload, one plain call each over the
+    device-resident raster, as JSON lines (op, cells, ideal, kernel_read,
+    kernel_written in bytes): the byte counts an ncu capture of the same
+    command sets beside dram__bytes_read.sum / dram__bytes_write.sum of the
+    op's launches. No timing."""
+    import torch
+
+    from strata_b200 import engine
+    from strata_b200.raster import Float32Raster, mask_from_bool
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    wl = workload(args.workload, args.side, args.ops)
+    W, H = wl["width"], wl["height"]
+    n, words = W * H, (W * H + 63) // 64
+    src = Float32Raster(torch.from_numpy(wl["cells"].reshape(-1)).to(dev), W, H, W,
+                        torch.from_numpy(mask_from_bool(wl["valid"]).view(np.int64)).to(dev), 0)
+    outs = [Float32Raster(torch.empty(n, dtype=torch.float32, device=dev), W, H, W,
+                          torch.empty(words, dtype=torch.int64, device=dev), 0) for _ in range(2)]
+    for name, make, _mk, nout in wl["ops"]:
+        st = engine.Stats()
+        assert engine.process(make(), outs[:nout], [src], engine.Options(Device=local_rank, Stats=st)) is None
+        torch.cuda.synchronize()
+        print(json.dumps({"op": name, "cells": st.Cells, "ideal": st.Ideal, "kernel_read": st.KernelRead,
+                          "kernel_written": st.KernelWritten, "bands": st.Bands}), flush=True)
+
+
 def _summary(line, keys):
     return {k: line[k] for k in keys if k in line}
 
@@ -1071,6 +1099,8 @@ def main():
     ap.add_argument("--side", type=int, default=None, help="raster side override (profiling captures)")
     ap.add_argument("--band", type=int, default=None, help="serving: rows per unit of the radius-1 batch kernels")
     ap.add_argument("--ops", default=None, help="comma-separated ops of the workload to keep (profiling captures)")
+    ap.add_argument("--stats", action="store_true",
+                    help="print each op's engine.Stats from one plain call (for an ncu DRAM-bytes capture) and exit")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -1078,6 +1108,9 @@ def main():
     if args.impl == "reference":
         if rank == 0:
             run_reference(args)
+        return
+    if args.stats:
+        run_stats(args, local_rank)
         return
     if world > 1:
         import datetime
