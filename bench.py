@@ -423,14 +423,20 @@ def run_ours(args, rank, world, local_rank):
 
     per_op = [[torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)] for _ in ops]
     op_ms = [0.0] * len(ops)
-    # Per-op durations, each op run alone (engine.process), from a separate
-    # pass of K steps with events between ops.
+    # Per-op durations, each op run alone (engine.process): K back-to-back
+    # calls of the op between two events, after one untimed call that keeps
+    # the stream busy while the host issues the timed ones (so no host issue
+    # time lands inside the events).
     with torch.cuda.stream(stream):
-        for _ in range(args.steps):
-            separate(per_op)
-            torch.cuda.synchronize()
-            for i in range(len(ops)):
-                op_ms[i] += per_op[i][0].elapsed_time(per_op[i][1]) / args.steps
+        for i, (name, stages, nout) in enumerate(ops):
+            assert engine.process(stages, outs[:nout], [src], opts) is None
+            per_op[i][0].record(stream)
+            for _ in range(args.steps):
+                assert engine.process(stages, outs[:nout], [src], opts) is None
+            per_op[i][1].record(stream)
+        torch.cuda.synchronize()
+        for i in range(len(ops)):
+            op_ms[i] = per_op[i][0].elapsed_time(per_op[i][1]) / args.steps
 
     barrier()
     torch.cuda.synchronize()

@@ -8,6 +8,7 @@
 // of the raster's border NaN (internal/exec/halo.go:61-92); the validity of
 // the outputs is written by validity.cu.
 #include <cstring>
+#include <memory>
 
 #include "cellops.cuh"
 #include "launch.h"
@@ -160,6 +161,41 @@ int64_t launch_data(const LaunchParams& p, cudaStream_t s, int64_t* window_cells
     return -1;  // beyond the kernels' 32-bit index limits: the caller falls back to the CPU
 }
 
+namespace {
+
+// A host thread's second stream on the current device, with the two
+// events that fork it from and join it back to the caller's stream; made
+// on first use, released when the thread ends.
+struct SideStream {
+    cudaStream_t s = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+    ~SideStream() {
+        if (s) cudaStreamDestroy(s);
+        if (fork) cudaEventDestroy(fork);
+        if (join) cudaEventDestroy(join);
+    }
+};
+
+SideStream* side_stream() {
+    thread_local std::unique_ptr<SideStream> per_device[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    auto& q = per_device[dev];
+    if (!q) {
+        auto n = std::make_unique<SideStream>();
+        if (cudaStreamCreateWithFlags(&n->s, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&n->fork, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&n->join, cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;  // the validity then runs on the caller's stream
+        }
+        q = std::move(n);
+    }
+    return q.get();
+}
+
+}  // namespace
+
 int64_t launch_stage(LaunchParams p, const ValidityParams* const v[2], cudaStream_t s, int64_t* window_cells) {
     memset(&p.vf, 0, sizeof p.vf);
     const ValidityParams* any = v[0] ? v[0] : v[1];
@@ -187,10 +223,24 @@ int64_t launch_stage(LaunchParams p, const ValidityParams* const v[2], cudaStrea
         }
         return launch_data(p, s, window_cells);
     }
+    // The output validity reads only the source mask and writes only the
+    // output masks, the data kernel only the cells: on a region large
+    // enough for the overlap to outweigh the fork and join, the validity
+    // runs on a second stream beside it, forked from and joined back to s.
+    const int64_t cells = (p.out_x1 - p.out_x0) * (p.out_y1 - p.out_y0);
+    SideStream* side = (v[0] || v[1]) && cells >= ((int64_t)1 << 22) ? side_stream() : nullptr;
+    if (side) {
+        cudaEventRecord(side->fork, s);
+        cudaStreamWaitEvent(side->s, side->fork, 0);
+        for (int i = 0; i < 2; i++)
+            if (v[i]) launch_validity(*v[i], side->s);
+        cudaEventRecord(side->join, side->s);
+    }
     const int64_t t = launch_data(p, s, window_cells);
-    if (t < 0) return t;
-    for (int i = 0; i < 2; i++)
-        if (v[i]) launch_validity(*v[i], s);
+    if (side) cudaStreamWaitEvent(s, side->join, 0);
+    else
+        for (int i = 0; i < 2; i++)
+            if (v[i]) launch_validity(*v[i], s);
     return t;
 }
 
