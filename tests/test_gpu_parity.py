@@ -609,6 +609,49 @@ def test_fused_features_equal_separate_calls_and_oracle(w, h):
             k += n
 
 
+CARRIERS = {
+    "slope_deg": lambda: terrain.slope_stage(terrain.SlopeOptions(CellSize=10)),
+    "slope_rad_reclass": lambda: terrain.slope_stage(terrain.SlopeOptions(CellSize=3, Units=terrain.SlopeRadians)).extend(
+        transfer.reclass_stage([0.1, 0.5, 1.0], [1, 2, 3, 4])),
+    "aspect_trig": lambda: terrain.aspect_stage(terrain.AspectOptions(CellSize=5, Trigonometric=True)),
+    "hillshade": lambda: terrain.hillshade_stage(terrain.HillshadeOptions(CellSize=10, Azimuth=200, Altitude=30)),
+    "curv_profile": lambda: terrain.curvature_stage(terrain.CurvatureOptions(CellSize=10, Type=0)),
+    "curv_plan": lambda: terrain.curvature_stage(terrain.CurvatureOptions(CellSize=10, Type=1)),
+    "curv_mean_reclass": lambda: terrain.curvature_stage(terrain.CurvatureOptions(CellSize=10, Type=2)).extend(
+        transfer.reclass_stage([-0.01, 0, 0.01], [1, 2, 3, 4])),
+    "tri_riley": lambda: terrain.ruggedness_stage(terrain.RuggednessOptions(Type=0)),
+}
+
+
+@pytest.mark.parametrize("name", sorted(CARRIERS))
+def test_fused_pass_carried_by_each_product(name):
+    """The memory-bound features carried by one arithmetic-bound product
+    in the fused pass: every output equals its op run alone and the oracle,
+    masked and unmasked, compact and strided outputs."""
+    w, h = 388, 53
+    cells = dem_cells(w, h, len(name))
+    for masked, strided in itertools.product((False, True), (False, True)):
+        src = host_raster(cells, synth.block_mask(w, h, w, 0.05) if masked else None)
+        feats = lambda: [terrain.gradient_stage(terrain.GradientOptions(CellSize=10)), CARRIERS[name](),
+                         terrain.ruggedness_stage(terrain.RuggednessOptions(Type=2)),
+                         terrain.ruggedness_stage(terrain.RuggednessOptions(Type=3))]
+        nouts = [2, 1, 1, 1]
+        st, off = (w + 8, 40) if strided else (None, 0)
+        outs = [like(src, st, off) for _ in range(sum(nouts))]
+        assert engine.process_features(feats(), outs, src) is None
+        k = 0
+        for f, n in zip(feats(), nouts):
+            alone = [like(src, st, off) for _ in range(n)]
+            assert engine.process(f, alone, [src]) is None
+            want = [like(src, st, off) for _ in range(n)]
+            run_oracle(f, src, want)
+            for i in range(n):
+                what = f"{name} masked={masked} strided={strided} op {f.stages[0].op} out{i}"
+                assert_same_raster(outs[k + i], alone[i], what + " vs alone")
+                assert_same_raster(outs[k + i], want[i], what + " vs oracle")
+            k += n
+
+
 def test_surface_equals_separate_calls():
     w, h = 128, 40
     src = host_raster(dem_cells(w, h, 13), synth.cell_mask(w, h, 13))
