@@ -160,6 +160,12 @@ struct strata_ctx {
     // The chunked calls' two tile buffer sets (page-locked and device),
     // grown on demand and reused.
     std::shared_ptr<void> chunk_sets;
+    // A second compute stream for the features of one Features call that
+    // run as their own launches (one kernel's tail overlaps the next's
+    // start), with the events that fork it from and join it back to the
+    // call's stream; made on first use.
+    cudaStream_t aux_stream = nullptr;
+    cudaEvent_t aux_fork = nullptr, aux_join = nullptr;
 };
 
 namespace {
@@ -233,6 +239,9 @@ extern "C" void strata_ctx_destroy(strata_ctx* c) {
     if (c->h_edges) cudaFreeHost(c->h_edges);
     if (c->stream) cudaStreamDestroy(c->stream);
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+    if (c->aux_stream) cudaStreamDestroy(c->aux_stream);
+    if (c->aux_fork) cudaEventDestroy(c->aux_fork);
+    if (c->aux_join) cudaEventDestroy(c->aux_join);
     delete c;
 }
 
@@ -2465,7 +2474,7 @@ extern "C" int strata_process_features(strata_ctx* c, const strata_stage* stages
     int64_t bands = 0, window = 0;
     // Starts the copies back of outputs [o, o + n) once the work queued on st
     // so far is done, on the copy stream, so they overlap the next kernels.
-    auto copy_back = [&](int o, int n) -> int {
+    auto copy_back = [&](int o, int n, cudaStream_t from) -> int {
         bool any_host = false;
         for (int i = o; i < o + n; i++) any_host = any_host || !dst[i].on_device;
         if (!any_host) return STRATA_OK;
@@ -2473,7 +2482,7 @@ extern "C" int strata_process_features(strata_ctx* c, const strata_stage* stages
         cudaError_t e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
         if (e != cudaSuccess) return cuda_fail(e, "event");
         events.push_back(ev);
-        cudaEventRecord(ev, st);
+        cudaEventRecord(ev, from);
         cudaStreamWaitEvent(cs, ev, 0);
         for (int i = o; i < o + n; i++) {
             if (dst[i].on_device) continue;
@@ -2566,7 +2575,7 @@ extern "C" int strata_process_features(strata_ctx* c, const strata_stage* stages
                 }
                 for (int f : group) {
                     done[(size_t)f] = 1;
-                    if ((rc = copy_back(first[(size_t)f], nouts[(size_t)f]))) {
+                    if ((rc = copy_back(first[(size_t)f], nouts[(size_t)f], st))) {
                         cleanup();
                         return rc;
                     }
@@ -2574,10 +2583,36 @@ extern "C" int strata_process_features(strata_ctx* c, const strata_stage* stages
             }
         }
     }
+    // The features that run as their own launches alternate between the
+    // call's stream and a second one, so that one kernel's last wave
+    // overlaps the next kernel's first; Wood's fit keeps to the call's
+    // stream (its sums share the context's scratch).
+    int own = 0;
+    for (int f = 0; f < nfeatures; f++) own += !done[(size_t)f] && !plans[(size_t)f].fit;
+    cudaStream_t lanes[2] = {st, st};
+    if (own >= 2) {
+        if (!c->aux_stream && (cudaStreamCreateWithFlags(&c->aux_stream, cudaStreamNonBlocking) != cudaSuccess ||
+                               cudaEventCreateWithFlags(&c->aux_fork, cudaEventDisableTiming) != cudaSuccess ||
+                               cudaEventCreateWithFlags(&c->aux_join, cudaEventDisableTiming) != cudaSuccess)) {
+            cudaGetLastError();
+            if (c->aux_stream) cudaStreamDestroy(c->aux_stream);
+            if (c->aux_fork) cudaEventDestroy(c->aux_fork);
+            c->aux_stream = nullptr;
+            c->aux_fork = nullptr;
+        }
+        if (c->aux_stream && c->aux_join) {
+            lanes[1] = c->aux_stream;
+            cudaEventRecord(c->aux_fork, st);
+            cudaStreamWaitEvent(c->aux_stream, c->aux_fork, 0);
+        }
+    }
+    int lane = 0;
     for (int f = 0; f < nfeatures; f++) {
         if (done[(size_t)f]) continue;
         LaunchParams& p = plans[(size_t)f];
         const int o = first[(size_t)f];
+        const cudaStream_t fs = p.fit ? st : lanes[lane];
+        if (!p.fit) lane ^= 1;
         int64_t wc = 0;
         ValidityParams vp[2];
         const ValidityParams* vs[2] = {nullptr, nullptr};
@@ -2587,8 +2622,12 @@ extern "C" int strata_process_features(strata_ctx* c, const strata_stage* stages
                           0, H);
             vs[i - o] = &vp[i - o];
         }
-        int64_t t = p.fit ? launch_fit(c, p, vs, st, &wc) : strata::launch_stage(p, vs, st, &wc);
+        int64_t t = p.fit ? launch_fit(c, p, vs, st, &wc) : strata::launch_stage(p, vs, fs, &wc);
         if (t < 0) {
+            if (lanes[1] != st) {
+                cudaEventRecord(c->aux_join, lanes[1]);
+                cudaStreamWaitEvent(st, c->aux_join, 0);
+            }
             cleanup();
             if (t == -2) return fail(STRATA_ENOMEM, "engine: no device memory for the fit's sums");
             return fail(STRATA_ENOTSUP, "engine: op %d at radius %d has no device kernel", p.op, p.radius);
@@ -2601,10 +2640,14 @@ extern "C" int strata_process_features(strata_ctx* c, const strata_stage* stages
             return cuda_fail(e, "kernel launch");
         }
         // The outputs' copies back overlap the next feature's kernels.
-        if ((rc = copy_back(o, nouts[(size_t)f]))) {
+        if ((rc = copy_back(o, nouts[(size_t)f], fs))) {
             cleanup();
             return rc;
         }
+    }
+    if (lanes[1] != st) {
+        cudaEventRecord(c->aux_join, lanes[1]);
+        cudaStreamWaitEvent(st, c->aux_join, 0);
     }
     cudaError_t e = cudaStreamSynchronize(cs);
     cleanup();
