@@ -652,6 +652,30 @@ def test_fused_pass_carried_by_each_product(name):
             k += n
 
 
+def test_features_over_many_units_two_streams():
+    """A Features call on a raster of thousands of strip units, the ops that
+    run as their own launches alternating over two streams, twice on the
+    same context: every output equals its op run alone."""
+    w, h = 1032, 3001
+    src = to_device(host_raster(dem_cells(w, h, 77), synth.block_mask(w, h, 77, 0.03)))
+    feats = lambda: [terrain.gradient_stage(terrain.GradientOptions(CellSize=10)),
+                     terrain.aspect_stage(terrain.AspectOptions(CellSize=10)),
+                     terrain.ruggedness_stage(terrain.RuggednessOptions(Type=2)),
+                     terrain.curvature_stage(terrain.CurvatureOptions(CellSize=10, Type=1)),
+                     terrain.ruggedness_stage(terrain.RuggednessOptions(Type=3))]
+    nouts = [2, 1, 1, 1, 1]
+    outs = [to_device(like(to_host(src))) for _ in range(sum(nouts))]
+    for _ in range(2):  # the second call reuses the context's streams
+        assert engine.process_features(feats(), outs, src) is None
+    k = 0
+    for f, n in zip(feats(), nouts):
+        alone = [to_device(like(to_host(src))) for _ in range(n)]
+        assert engine.process(f, alone, [src]) is None
+        for i in range(n):
+            assert_same_raster(to_host(outs[k + i]), to_host(alone[i]), f"op {f.stages[0].op} out{i}")
+        k += n
+
+
 def test_surface_equals_separate_calls():
     w, h = 128, 40
     src = host_raster(dem_cells(w, h, 13), synth.cell_mask(w, h, 13))
