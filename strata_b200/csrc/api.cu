@@ -2163,7 +2163,11 @@ int run_chunked(strata_ctx* c, const LaunchParams& p, int nout, int64_t W, int64
             v.dst_lo_word = 0;
             v.dst_words = (oc + 31) >> 5;
         }
-        int64_t nt = strata::launch_stage(q, vs, st, &wc);
+        int64_t nt = q.fit ? launch_fit(c, q, vs, st, &wc) : strata::launch_stage(q, vs, st, &wc);
+        if (nt == -2) {
+            status = fail(STRATA_ENOMEM, "engine: no device memory for the fit's sums");
+            break;
+        }
         if (nt < 0) {
             status = fail(STRATA_ENOTSUP, "engine: op %d at radius %d has no device kernel", p.op, p.radius);
             break;
@@ -2345,7 +2349,6 @@ extern "C" int strata_process_chunked(strata_ctx* c, const strata_stage* stages,
     int nout = 0;
     int rc = plan_stages(stages, nstages, p, &nout);
     if (rc) return rc;
-    if (p.fit) return fail(STRATA_ENOTSUP, "engine: Wood's fit (FitRadius > 0) has no chunked form on the gpu backend");
     if (p.ninputs > 1 || nsrc > 1)
         return fail(STRATA_ENOTSUP, "engine: a chain over several inputs has no chunked form on the gpu backend");
     if ((rc = check_opts(opts))) return rc;
@@ -2391,7 +2394,6 @@ extern "C" int strata_process_raw(strata_ctx* c, const strata_stage* stages, int
     int nout = 0;
     int rc = plan_stages(stages, nstages, p, &nout);
     if (rc) return rc;
-    if (p.fit) return fail(STRATA_ENOTSUP, "engine: Wood's fit (FitRadius > 0) has no chunked form on the gpu backend");
     if (p.ninputs > 1 || nsrc > 1)
         return fail(STRATA_ENOTSUP, "engine: a chain over several inputs has no chunked form on the gpu backend");
     if ((rc = check_opts(opts))) return rc;
@@ -2689,8 +2691,8 @@ int fill_batch_item(strata_ctx* c, const strata_batch_item& it, int i, strata::B
         return fail(STRATA_EINVAL, "engine: batch raster %d: the rasters of a batch must be on the device", i);
     if (is_pointwise((uint32_t)p.op))
         return fail(STRATA_ENOTSUP, "engine: batch raster %d: a pointwise op alone has no batch kernel", i);
-    if (p.fit || p.op == STRATA_OP_HEATLOAD || p.op == STRATA_OP_ORIENTATION)
-        return fail(STRATA_ENOTSUP, "engine: batch raster %d: op %d has no batch kernel", i, p.op);
+    if (p.fit)
+        return fail(STRATA_ENOTSUP, "engine: batch raster %d: Wood's fit (FitRadius > 0) has no batch kernel", i);
     if (it.tile_height < 0 || it.tile_height > 1024)
         return fail(STRATA_EINVAL, "engine: batch raster %d: band of %d rows (0 to 1024)", i, it.tile_height);
     DevOperand ds, dd[2];
@@ -3294,8 +3296,8 @@ Request* prepare_request(strata_server* S, const strata_stage* stages, int nstag
     int rc = plan_stages(r->stages.data(), (int)r->stages.size(), r->p, &r->nout);
     if (rc == STRATA_OK && is_pointwise((uint32_t)r->p.op))
         rc = fail(STRATA_ENOTSUP, "engine: a pointwise op alone has no batch kernel");
-    if (rc == STRATA_OK && (r->p.fit || r->p.op == STRATA_OP_HEATLOAD || r->p.op == STRATA_OP_ORIENTATION))
-        rc = fail(STRATA_ENOTSUP, "engine: op %d has no batch kernel", r->p.op);
+    if (rc == STRATA_OK && r->p.fit)
+        rc = fail(STRATA_ENOTSUP, "engine: Wood's fit (FitRadius > 0) has no batch kernel");
     if (rc) {
         delete r;
         *rc_out = rc;

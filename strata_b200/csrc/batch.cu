@@ -295,6 +295,8 @@ bool launch_batch_class(const BatchClass& c, const BatchItem* d, cudaStream_t s)
     case STRATA_OP_ASPECT:
         return c.kind ? launch_march_epi<STRATA_OP_ASPECT, 1>(c, d, s) : launch_march_epi<STRATA_OP_ASPECT, 0>(c, d, s);
     case STRATA_OP_HILLSHADE: return launch_march_epi<STRATA_OP_HILLSHADE, 0>(c, d, s);
+    case STRATA_OP_HEATLOAD: return launch_march_epi<STRATA_OP_HEATLOAD, 0>(c, d, s);
+    case STRATA_OP_ORIENTATION: return launch_march_epi<STRATA_OP_ORIENTATION, 0>(c, d, s);
     case STRATA_OP_CURVATURE:
         switch (c.kind) {
         case 0: return launch_march_epi<STRATA_OP_CURVATURE, 0>(c, d, s);

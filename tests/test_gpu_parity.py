@@ -838,11 +838,55 @@ def test_fit_surface_and_features_equal_standalone():
         assert_same_raster(got, want, f"features {type(op).__name__}")
 
 
-def test_fit_has_no_chunked_or_batch_form():
+@pytest.mark.parametrize("r", [1, 3, 8])
+def test_fit_chunked_equals_plain(r):
+    """Wood's fit through the chunked form (tiles with the fit's halo, the
+    sums in context scratch per tile) writes the plain call's bits."""
+    w, h = 517, 203
+    src = host_raster(dem_cells(w, h, 5 + r), synth.block_mask(w, h, r, 0.03))
+    st = lambda: terrain.curvature_stage(terrain.CurvatureOptions(CellSize=10, Type=2, FitRadius=r))
+    plain, chunked = like(src), like(src)
+    assert engine.process(st(), [plain], [src]) is None
+    assert engine.process_chunked(st(), [engine.MemorySink(chunked)], [engine.MemorySource(src)],
+                                  engine.Options(TileWidth=200, TileHeight=64)) is None
+    assert_same_raster(chunked, plain, f"fit r={r} chunked")
+
+
+def test_fit_has_no_batch_form():
+    from strata_b200 import batch
     from strata_b200.raster import NotSupported
 
     w, h = 40, 30
-    src = host_raster(dem_cells(w, h, 5))
+    src = to_device(host_raster(dem_cells(w, h, 5)))
     with pytest.raises(NotSupported):
-        engine.process_chunked(terrain.slope_stage(terrain.SlopeOptions(CellSize=1, FitRadius=2)),
-                               [engine.MemorySink(like(src))], [engine.MemorySource(src)], engine.Options())
+        batch.Batch([batch.Item(terrain.slope_stage(terrain.SlopeOptions(CellSize=1, FitRadius=2)), src,
+                                [to_device(like(to_host(src)))])])
+
+
+def test_heatload_orientation_in_a_batch():
+    """HeatLoad and Orientation run in the batched form: every raster equals
+    its plain call."""
+    from strata_b200 import batch
+
+    rng = np.random.default_rng(3)
+    items, outs, wants = [], [], []
+    makers = [lambda: terrain.heatload_stage(terrain.HeatLoadOptions(CellSize=10, Latitude=40, Equation=1)),
+              lambda: terrain.heatload_stage(terrain.HeatLoadOptions(CellSize=30, Latitude=-20, Linear=True)),
+              lambda: terrain.orientation_stage(terrain.OrientationOptions(CellSize=10)),
+              lambda: terrain.orientation_stage(terrain.OrientationOptions(CellSize=5, Component=terrain.Eastness,
+                                                                           Unweighted=True))]
+    for i in range(8):
+        w, h = int(rng.integers(30, 600)), int(rng.integers(10, 300))
+        hsrc = host_raster(dem_cells(w, h, i), synth.block_mask(w, h, i, 0.03))
+        st = makers[i % 4]
+        want = like(hsrc)
+        assert engine.process(st(), [want], [hsrc]) is None
+        out = to_device(like(hsrc))
+        items.append(batch.Item(st(), to_device(hsrc), [out]))
+        outs.append(out)
+        wants.append(want)
+    b = batch.Batch(items)
+    b.run()
+    b.close()
+    for i, (o, w_) in enumerate(zip(outs, wants)):
+        assert_same_raster(to_host(o), w_, f"batch item {i}")
