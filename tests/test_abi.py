@@ -271,3 +271,29 @@ def test_step_stage_fields():
     assert (st.op, st.kind, st.input) == (_lib.OP_STEP, vec.OpSub, 3)
     st = transfer.rescale_stage(2.5, -1).stages[0]
     assert (st.kind, st.input, st.k[0], st.k[1]) == (vec.OpAffine, -1, 2.5, -1.0)
+
+
+def test_builder_constants_over_random_options():
+    """The stage builders' resolved constants (Horn and ZT scales, the
+    hillshade light vector, Gaussian taps) equal the oracle's own
+    resolution bit for bit over a seeded sweep of options: cell sizes over
+    nine decades, anisotropic cells, negative and fractional z factors,
+    azimuths past a full turn and altitudes over the whole range."""
+    rng = np.random.default_rng(20261204)
+    for _ in range(400):
+        cs = float(np.float32(10 ** rng.uniform(-4, 5)))
+        csy = 0.0 if rng.random() < 0.4 else float(np.float32(10 ** rng.uniform(-4, 5)))
+        z = 0.0 if rng.random() < 0.3 else float(np.float32(rng.uniform(-10, 10)))
+        kx, ky = orc.horn_scales(cs, csy or cs, z or 1.0)
+        got = k_of(terrain.slope_stage(terrain.SlopeOptions(CellSize=cs, CellSizeY=csy, ZFactor=z)))
+        assert (got[0], got[1]) == (kx, ky), (cs, csy, z)
+        got = k_of(terrain.curvature_stage(terrain.CurvatureOptions(CellSize=cs, CellSizeY=csy, ZFactor=z, Type=1)))
+        assert got[:5] == orc.zt_scales(cs, csy or cs, z or 1.0), (cs, csy, z)
+        az, alt = float(np.float32(rng.uniform(-720, 720))), float(np.float32(rng.uniform(0, 90)))
+        got = k_of(terrain.hillshade_stage(terrain.HillshadeOptions(CellSize=cs, CellSizeY=csy, ZFactor=z,
+                                                                    Azimuth=az, Altitude=alt)))
+        assert (got[0], got[1]) == (kx, ky) and got[2:5] == orc.hillshade_light(az, alt), (cs, csy, z, az, alt)
+    for r in range(1, 9):
+        for sigma in rng.uniform(0.05, 20, 6):
+            sigma = float(np.float32(sigma))
+            assert (focal.Gaussian(r, sigma).view(np.uint32) == orc.gaussian(r, sigma).view(np.uint32)).all(), (r, sigma)
