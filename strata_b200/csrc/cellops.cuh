@@ -364,7 +364,7 @@ __device__ __forceinline__ F2 zt_curvature2(F2 d64, F2 d82, F2 c, F2 s46, F2 s28
 // that of a float32 rounding boundary).
 __device__ __forceinline__ float heat_load(float gx, float gy, const double* t, bool ex) {
     const double dx = gx, dy = gy;
-    const double g2 = __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
+    const double g2 = __fma_rn(dx, dx, __dmul_rn(dy, dy));  // dx * dx exact (add_sq64)
     const double w = __ddiv_rn(1.0, __dsqrt_rn(__dadd_rn(1.0, g2)));
     const double fold = fabs(__dadd_rn(__dmul_rn(t[6], dx), __dmul_rn(t[7], dy)));
     double sum = __dadd_rn(t[1], __dmul_rn(t[2], dx));
@@ -382,7 +382,7 @@ __device__ __forceinline__ float heat_load(float gx, float gy, const double* t, 
 __device__ __forceinline__ float orientation(float gx, float gy, bool east, bool unweighted) {
     const double dx = gx, dy = gy;
     const double c = east ? -dx : dy;
-    const double g2 = __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
+    const double g2 = __fma_rn(dx, dx, __dmul_rn(dy, dy));  // dx * dx exact (add_sq64)
     if (!unweighted) return __double2float_rn(__ddiv_rn(c, __dsqrt_rn(__dadd_rn(1.0, g2))));
     if (g2 == 0) return 0.0f;
     return __double2float_rn(__ddiv_rn(c, __dsqrt_rn(g2)));
@@ -400,18 +400,28 @@ __device__ __forceinline__ double sq64(float d) {
     return __dmul_rn(x, x);
 }
 
+// a + float64(d) * float64(d), each step rounded as the reference rounds
+// it, in one fused multiply-add: the square of a float32 in float64 is
+// exact (48 significant bits of 53; the float32 range squared stays within
+// float64's normal range), so rounding the product first changes nothing
+// and the one rounding of the sum is the reference's.
+__device__ __forceinline__ double add_sq64(double a, float d) {
+    const double x = (double)d;
+    return __fma_rn(x, x, a);
+}
+
 // RuggednessRow at radius 1 (internal/stencil/rugged.go:70-103).
 __device__ __forceinline__ float rugged3(float v1, float v2, float v3, float v4, float v5, float v6,
                                          float v7, float v8, float v9, int kind) {
     float c = v5;
     if (kind == 0) {
-        double a = __dadd_rn(sq64(sub(v1, c)), sq64(sub(v2, c)));
-        a = __dadd_rn(a, sq64(sub(v3, c)));
-        a = __dadd_rn(a, sq64(sub(v4, c)));
-        a = __dadd_rn(a, sq64(sub(v6, c)));
-        a = __dadd_rn(a, sq64(sub(v7, c)));
-        a = __dadd_rn(a, sq64(sub(v8, c)));
-        a = __dadd_rn(a, sq64(sub(v9, c)));
+        double a = add_sq64(sq64(sub(v1, c)), sub(v2, c));
+        a = add_sq64(a, sub(v3, c));
+        a = add_sq64(a, sub(v4, c));
+        a = add_sq64(a, sub(v6, c));
+        a = add_sq64(a, sub(v7, c));
+        a = add_sq64(a, sub(v8, c));
+        a = add_sq64(a, sub(v9, c));
         return __double2float_rn(__dsqrt_rn(a));
     }
     if (kind == 1) {

@@ -545,7 +545,7 @@ __device__ __forceinline__ void window_body(const LaunchParams& P, int64_t x0, i
                     if constexpr (OP == STRATA_OP_CORRELATE) {
                         acc[m][i] = add(acc[m][i], mul(w[k], v));
                     } else if (k != R || !centre_row) {
-                        if constexpr (RILEY) dacc[m][i] = __dadd_rn(dacc[m][i], sq64(sub(v, ctr[m][i])));
+                        if constexpr (RILEY) dacc[m][i] = add_sq64(dacc[m][i], sub(v, ctr[m][i]));
                         else if constexpr (WILSON) acc[m][i] = add(acc[m][i], abs32(sub(v, ctr[m][i])));
                         else acc[m][i] = add(acc[m][i], v);
                     }
