@@ -231,26 +231,41 @@ __device__ __forceinline__ F2 add_p(F2 a, F2 b) { return pk(add(lo(a), lo(b)), a
 __device__ __forceinline__ F2 sub_p(F2 a, F2 b) { return pk(sub(lo(a), lo(b)), sub(hi(a), hi(b))); }
 
 // atan32 over a pair: the same steps, the halves apart only for the
-// argument reduction and the division.
+// argument reduction and the division. SKIP_SMALL: when no active lane of
+// the warp holds an argument above tan(pi/8), every reduction is the
+// identity, whose quotient x / 1 is x itself, so the warp skips the
+// divisions (Slope's magnitudes on gentle terrain); the bits are the same.
+template <bool SKIP_SMALL = false>
 __device__ __forceinline__ F2 atan32x2(F2 x) {
-    const F2 xm = sub2(x, splat(1.0f)), xp = add2(x, splat(1.0f));
-    const float xs[2] = {lo(x), hi(x)}, xms[2] = {lo(xm), hi(xm)}, xps[2] = {lo(xp), hi(xp)};
+    const float xs[2] = {lo(x), hi(x)};
     float t[2], y0[2];
+    bool small = false;
+    if constexpr (SKIP_SMALL) small = !__any_sync(__activemask(), xs[0] > kTanPi8 || xs[1] > kTanPi8);
+    if (small) {
 #pragma unroll
-    for (int h = 0; h < 2; h++) {
-        float num = xs[h], den = 1.0f;
-        y0[h] = 0.0f;
-        if (xs[h] > kTanPi8) {
-            num = xms[h];
-            den = xps[h];
-            y0[h] = kPi4;
+        for (int h = 0; h < 2; h++) {
+            t[h] = xs[h];
+            y0[h] = 0.0f;
         }
-        if (xs[h] > kTan3Pi8) {
-            num = -1.0f;
-            den = xs[h];
-            y0[h] = kPi2;
+    } else {
+        const F2 xm = sub2(x, splat(1.0f)), xp = add2(x, splat(1.0f));
+        const float xms[2] = {lo(xm), hi(xm)}, xps[2] = {lo(xp), hi(xp)};
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            float num = xs[h], den = 1.0f;
+            y0[h] = 0.0f;
+            if (xs[h] > kTanPi8) {
+                num = xms[h];
+                den = xps[h];
+                y0[h] = kPi4;
+            }
+            if (xs[h] > kTan3Pi8) {
+                num = -1.0f;
+                den = xs[h];
+                y0[h] = kPi2;
+            }
+            t[h] = div(num, den);
         }
-        t[h] = div(num, den);
     }
     const F2 tt = pk(t[0], t[1]);
     const F2 z = mul2(tt, tt);
@@ -264,7 +279,7 @@ __device__ __forceinline__ F2 atan32x2(F2 x) {
 __device__ __forceinline__ F2 slope2(F2 gx, F2 gy, F2 scale, bool take_atan) {
     const F2 s = add_p(mul2(gx, gx), mul2(gy, gy));
     const F2 m = pk(sqrt64of32(lo(s)), sqrt64of32(hi(s)));
-    return mul2(take_atan ? atan32x2(m) : m, scale);
+    return mul2(take_atan ? atan32x2<true>(m) : m, scale);
 }
 
 // aspect over a pair of gradients, atan2f32's steps inline. Its fix-up

@@ -93,6 +93,29 @@ def test_terrain_ops(name):
     run_matrix(TERRAIN[name], dem_cells)
 
 
+def gentle_cells(w, h, seed):
+    """Gentle terrain (slopes mostly below 22.5 degrees, where whole warps
+    skip the arctangent's division) with a few steep ridges and scattered
+    special values, so warps that skip and warps that divide both occur,
+    and some warps mix both kinds of lanes."""
+    cells = synth.fbm_dem(w, h, seed, lo=0, hi=3000) * np.float32(0.01)
+    rng = np.random.default_rng(seed)
+    for _ in range(max(1, w * h // 4000)):
+        y, x = int(rng.integers(0, h)), int(rng.integers(0, w))
+        cells[y, x:x + int(rng.integers(1, 40))] += np.float32(rng.uniform(5, 400))
+    return poison(cells.astype(np.float32), seed, 0.001)
+
+
+@pytest.mark.parametrize("units", ["deg", "rad"])
+def test_slope_on_gentle_terrain(units):
+    """Slope with the arctangent over gentle terrain: the warps whose
+    magnitudes all lie below tan(pi/8) take the arctangent without its
+    division, the others with it; every cell matches the oracle."""
+    u = terrain.SlopeDegrees if units == "deg" else terrain.SlopeRadians
+    run_matrix(lambda: terrain.slope_stage(terrain.SlopeOptions(CellSize=10, Units=u)), gentle_cells,
+               shapes=[(257, 131), (516, 70), (1028, 33), (2052, 40)], seed=7)
+
+
 def test_gradient_two_outputs():
     run_matrix(lambda: terrain.gradient_stage(terrain.GradientOptions(CellSize=30, CellSizeY=25)), dem_cells, nout=2)
 
