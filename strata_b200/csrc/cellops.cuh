@@ -464,6 +464,24 @@ __device__ __forceinline__ float rugged3(float v1, float v2, float v3, float v4,
     return sub(hi, lo);
 }
 
+// rugged3's roughness for four adjacent cells from their window rows a, b,
+// c (six columns each): the maximum and minimum of each column over the
+// three rows first, then of three adjacent columns per cell. Go's min and
+// max (min.NaN / max.NaN) are exactly associative and commutative, so the
+// regrouping keeps rugged3's bits, in 44 operations instead of 68.
+__device__ __forceinline__ void roughness4(const float (&a)[6], const float (&b)[6], const float (&c)[6],
+                                           float (&o)[4]) {
+    float hi[6], lo[6];
+#pragma unroll
+    for (int j = 0; j < 6; j++) {
+        hi[j] = go_max(go_max(a[j], b[j]), c[j]);
+        lo[j] = go_min(go_min(a[j], b[j]), c[j]);
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+        o[i] = sub(go_max(go_max(hi[i], hi[i + 1]), hi[i + 2]), go_min(go_min(lo[i], lo[i + 1]), lo[i + 2]));
+}
+
 // The reference's table index, k = the first j with v < xs[j] (or n):
 // for strictly increasing, NaN-free knots and a non-NaN v that is the
 // number of knots at or below v, which this counts without branches. The

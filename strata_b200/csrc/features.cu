@@ -142,10 +142,7 @@ __device__ __forceinline__ void features_row(const FeaturesParams& F, const Stri
         }
         if (F.f[kFRoughness].on) {
             float o[4];
-#pragma unroll
-            for (int i = 0; i < 4; i++)
-                o[i] = rugged3(a.v[i], a.v[i + 1], a.v[i + 2], b.v[i], b.v[i + 1], b.v[i + 2], c.v[i], c.v[i + 1],
-                               c.v[i + 2], STRATA_RUG_ROUGHNESS);
+            roughness4(a.v, b.v, c.v, o);
             feature_store(F.f[kFRoughness], 0, S, in, rowoff, coloff, o);
         }
         if (F.f[kFWilson].on) {

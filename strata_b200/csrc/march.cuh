@@ -125,6 +125,13 @@ __device__ __forceinline__ void row_compute(const LaunchParams& P, const EpiTabl
             o0[j] = rowin && colin[j] ? hi(r) : nan;
         }
         if constexpr (EPI) epilogue4(P, *T, o0);
+    } else if constexpr (OP == STRATA_OP_RUGGEDNESS && KIND == STRATA_RUG_ROUGHNESS) {
+        // the window's column maxima and minima shared by the lane's four cells
+        float r[4];
+        roughness4(a.v, b.v, c.v, r);
+#pragma unroll
+        for (int i = 0; i < 4; i++) o0[i] = (rowin && colin[i]) ? r[i] : nan;
+        if constexpr (EPI) epilogue4(P, *T, o0);
     } else {
 #pragma unroll
         for (int i = 0; i < 4; i++) {
